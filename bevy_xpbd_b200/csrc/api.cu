@@ -1,0 +1,1074 @@
+// Host runtime behind include/xpbd_cuda.h: batch packing, device buffers, per-frame schedule, CUDA-graph capture,
+// autotuning, state readback and device error reporting.
+//
+// Reference counterparts: init_cloth_sim_jacobi (buffer creation, cloth_jacobi.rs:213-569),
+// prepare_cloth_bind_groups_jacobi (per-frame uniform upload, :571-649), run_cloth_sim_jacobi /
+// run_cloth_sim_gauss_seidel (per-frame dispatch schedule, cloth_jacobi.rs:675-916, cloth_compute.rs:1271-1522),
+// reset_cloth_sim_state_jacobi (:918-944).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/xpbd_cuda.h"
+#include "mesh_prep.h"
+#include "xpbd_internal.h"
+#include "xpbd_kernels.h"
+
+using namespace xpbd;
+
+namespace {
+
+struct ClothHost {
+    uint32_t n = 0, e = 0;
+    std::vector<float> pos, vel, w, rest_pos;
+    std::vector<uint32_t> ci, cj, ctype;
+    std::vector<float> rest, comp;
+    uint32_t order = XPBD_ORDER_COLOR_REFERENCE;
+    std::vector<uint32_t> given_offsets;
+    // derived at commit
+    std::vector<uint32_t> perm, colors, batch_off;
+    uint32_t vtx_off = 0, con_off = 0;
+    std::vector<uint32_t> lambda_inc;  // per input constraint: incidence holding its λ (Jacobi), or UINT32_MAX
+    std::vector<uint32_t> lambda_gs;   // per input constraint: position in the color-major table
+};
+
+struct DeviceBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct xpbd_ctx {
+    int device = 0;
+    int sms = 148;
+    bool coop_supported = false;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::vector<ClothHost> cloths;
+    bool committed = false;
+    XpbdWorld W{};
+    std::vector<void*> allocs;
+    XpbdDevParams hp{};
+    XpbdDevParams* dparams = nullptr;
+    xpbd_time_step_params tsp{};
+    xpbd_solver_opts opts{};
+    bool params_set = false;
+    CollisionBuffers cb{};
+    bool coll_ready = false;
+    uint32_t coll_ring_depth_built = 0;
+    // schedule
+    uint32_t block = 256, grid = 0;
+    bool coop = false;
+    // graph
+    cudaGraphExec_t exec = nullptr;
+    std::string graph_key;
+    uint64_t graph_nodes = 0;
+    // staging
+    float* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    float* d_xyz = nullptr;
+    unsigned* d_resid = nullptr;
+    int* d_status_copy = nullptr;
+    xpbd_stats stats{};
+    std::string last_error;
+    float forced_timeout_ms = 0.f;
+};
+
+// ------------------------------------------------------------------------------------------------- helpers
+static int fail(xpbd_ctx* c, int code, const std::string& msg) {
+    if (c) c->last_error = msg;
+    return code;
+}
+static int cuda_fail(xpbd_ctx* c, cudaError_t e, const char* what) {
+    int code = (e == cudaErrorMemoryAllocation) ? XPBD_ERR_OUT_OF_MEMORY : XPBD_ERR_CUDA;
+    return fail(c, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(call, what)                                   \
+    do {                                                 \
+        cudaError_t _e = (call);                         \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
+    } while (0)
+
+template <typename T>
+static T* dev_alloc(xpbd_ctx* ctx, size_t count, cudaError_t* err) {
+    void* p = nullptr;
+    size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    *err = cudaMalloc(&p, bytes);
+    if (*err == cudaSuccess) ctx->allocs.push_back(p);
+    return (T*)p;
+}
+
+static void free_device(xpbd_ctx* ctx) {
+    if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
+    ctx->exec = nullptr;
+    ctx->graph_key.clear();
+    for (void* p : ctx->allocs) cudaFree(p);
+    ctx->allocs.clear();
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+}
+
+static void fill_dev_params(xpbd_ctx* ctx) {
+    const xpbd_time_step_params& t = ctx->tsp;
+    const xpbd_solver_opts& o = ctx->opts;
+    XpbdDevParams& p = ctx->hp;
+    p.dt = t.dt;
+    p.inv_dt = t.inv_dt;
+    p.inv_dt_sq = t.inv_dt * t.inv_dt;  // ClothSimParamsGpu::pack (cloth_compute.rs:325)
+    p.omega = t.jacobi_omega;
+    p.iterations = t.inner_iterations;
+    p.relaxation = o.relaxation;
+    p.lambda_mode = o.lambda_mode;
+    p.solver = o.solver;
+    for (int k = 0; k < 3; ++k) {
+        p.gravity[k] = t.gravity[k];
+        p.grab_target[k] = t.grab_target[k];
+    }
+    p.damp = expf(-t.linear_drag_per_sec * t.dt);  // xpbd_cpu.rs:402, one libm evaluation per upload
+    p.grab_idx = t.grab_idx;
+    p.grab_active = t.grab_active;
+    p.grab_stiffness = t.grab_stiffness;
+    p.thickness = o.thickness;
+    p.coll_scale = o.coll_scale;
+    p.inv_cell = 1.0f / std::max(o.hash_cell, o.thickness);
+    p.ground_y = o.ground_y;
+    p.ground_enabled = o.ground_enabled;
+    p.collision = o.collision;
+    p.table_bits = o.hash_table_bits;
+    p.warm_start = o.warm_start;
+    float tmo = ctx->forced_timeout_ms > 0.f ? ctx->forced_timeout_ms
+                                             : (o.barrier_timeout_ms > 0.f ? o.barrier_timeout_ms : 2000.f);
+    p.barrier_timeout_ns = (unsigned long long)((double)tmo * 1e6);
+}
+
+extern "C" void xpbd_default_opts(xpbd_solver_opts* o) {
+    memset(o, 0, sizeof(*o));
+    o->solver = XPBD_SOLVER_JACOBI;
+    o->relaxation = XPBD_RELAX_OMEGA;
+    o->lambda_mode = XPBD_LAMBDA_RESET_PER_ITERATION;
+    o->substeps = 36;  // SUBSTEPS, cloth_compute.rs:59
+    o->collision = XPBD_COLLISION_NONE;
+    o->collision_every_n_substeps = 1;
+    o->thickness = 0.04f;   // THICKNESS
+    o->coll_scale = 0.38f;  // DEFAULT_COLL_SCALE
+    o->hash_cell = 0.04f;
+    o->hash_table_bits = 20;
+    o->ring_depth = 2;
+    o->use_graphs = 1;
+    o->barrier_timeout_ms = 2000.f;
+}
+
+// ------------------------------------------------------------------------------------------------- lifetime
+extern "C" int xpbd_create(xpbd_ctx** out, int device) {
+    if (!out) return XPBD_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return XPBD_ERR_NO_DEVICE;
+    if (device < 0 || device >= count) return XPBD_ERR_INVALID_ARGUMENT;
+    auto* ctx = new xpbd_ctx;
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+    int coop = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return XPBD_ERR_CUDA;
+    }
+    ctx->coop_supported = coop != 0;
+    ctx->stream = ctx->own_stream;
+    xpbd_default_opts(&ctx->opts);
+    *out = ctx;
+    return XPBD_OK;
+}
+
+extern "C" void xpbd_destroy(xpbd_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_device(ctx);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+}
+
+extern "C" int xpbd_set_stream(xpbd_ctx* ctx, void* stream) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return XPBD_OK;
+}
+
+// ------------------------------------------------------------------------------------------------- building
+extern "C" int xpbd_add_cloth(xpbd_ctx* ctx, const xpbd_cloth_desc* d, uint32_t* cloth_id) {
+    if (!ctx || !d) return XPBD_ERR_INVALID_ARGUMENT;
+    if (ctx->committed) return fail(ctx, XPBD_ERR_STATE, "xpbd_add_cloth after xpbd_commit");
+    if (d->num_particles == 0 || !d->positions || !d->inv_mass)
+        return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "cloth needs particles, positions and inv_mass");
+    if (d->num_constraints > 0 && (!d->constraint_i || !d->constraint_j || !d->rest_len || !d->compliance))
+        return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "constraint arrays missing");
+    if (d->order > XPBD_ORDER_PRESORTED) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad constraint order mode");
+    ClothHost c;
+    c.n = d->num_particles;
+    c.e = d->num_constraints;
+    c.pos.assign(d->positions, d->positions + 3 * (size_t)c.n);
+    c.vel.assign(3 * (size_t)c.n, 0.f);
+    if (d->velocities) c.vel.assign(d->velocities, d->velocities + 3 * (size_t)c.n);
+    c.w.assign(d->inv_mass, d->inv_mass + c.n);
+    c.rest_pos = d->rest_positions ? std::vector<float>(d->rest_positions, d->rest_positions + 3 * (size_t)c.n)
+                                   : c.pos;
+    for (uint32_t i = 0; i < c.n; ++i) {
+        if (!std::isfinite(c.w[i]) || c.w[i] < 0.f)
+            return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "inv_mass must be finite and >= 0");
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(c.pos[3 * i + k])) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "non-finite position");
+    }
+    if (c.e) {
+        c.ci.assign(d->constraint_i, d->constraint_i + c.e);
+        c.cj.assign(d->constraint_j, d->constraint_j + c.e);
+        c.rest.assign(d->rest_len, d->rest_len + c.e);
+        c.comp.assign(d->compliance, d->compliance + c.e);
+        c.ctype.assign(c.e, XPBD_CONSTRAINT_STRETCH);
+        if (d->constraint_type) c.ctype.assign(d->constraint_type, d->constraint_type + c.e);
+        for (uint32_t e = 0; e < c.e; ++e) {
+            if (c.ci[e] >= c.n || c.cj[e] >= c.n)
+                return fail(ctx, XPBD_ERR_INDEX_RANGE, "constraint endpoint out of range");
+            if (c.ci[e] == c.cj[e]) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "constraint joins a particle to itself");
+            if (!(c.rest[e] >= 0.f) || !std::isfinite(c.rest[e]) || !(c.comp[e] >= 0.f) || !std::isfinite(c.comp[e]))
+                return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "rest length / compliance must be finite and >= 0");
+        }
+    }
+    c.order = d->order;
+    if (d->order == XPBD_ORDER_PRESORTED) {
+        if (!d->batch_offsets) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "presorted order needs batch_offsets");
+        c.given_offsets.assign(d->batch_offsets, d->batch_offsets + d->batch_count + 1);
+        if (c.given_offsets.front() != 0 || c.given_offsets.back() != c.e ||
+            !std::is_sorted(c.given_offsets.begin(), c.given_offsets.end()))
+            return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "batch_offsets must rise from 0 to num_constraints");
+    }
+    uint64_t total = (uint64_t)c.n;
+    for (auto& o : ctx->cloths) total += o.n;
+    if (total >= XPBD_MAX_PARTICLES) return fail(ctx, XPBD_ERR_CAPACITY, "more than 2^28 particles per context");
+    if (ctx->cloths.size() >= 65535) return fail(ctx, XPBD_ERR_CAPACITY, "more than 65535 cloths per context");
+    if (cloth_id) *cloth_id = (uint32_t)ctx->cloths.size();
+    ctx->cloths.push_back(std::move(c));
+    return XPBD_OK;
+}
+
+static void ensure_pinned(xpbd_ctx* ctx, size_t bytes) {
+    if (ctx->pinned_bytes >= bytes) return;
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    if (cudaHostAlloc((void**)&ctx->pinned, bytes, cudaHostAllocDefault) == cudaSuccess) ctx->pinned_bytes = bytes;
+}
+
+extern "C" int xpbd_commit(xpbd_ctx* ctx) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    if (ctx->committed) return fail(ctx, XPBD_ERR_STATE, "already committed");
+    if (ctx->cloths.empty()) return fail(ctx, XPBD_ERR_STATE, "no cloth added");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const uint32_t C = (uint32_t)ctx->cloths.size();
+    uint32_t N = 0, E = 0, max_colors = 0;
+    // ---- coloring + per-cloth offsets
+    for (auto& c : ctx->cloths) {
+        c.vtx_off = N;
+        c.con_off = E;
+        N += c.n;
+        E += c.e;
+        if (c.order == XPBD_ORDER_PRESORTED) {
+            c.perm.resize(c.e);
+            for (uint32_t k = 0; k < c.e; ++k) c.perm[k] = k;
+            c.batch_off = c.given_offsets;
+            c.colors.assign(c.e, 0);
+            for (size_t b = 0; b + 1 < c.batch_off.size(); ++b)
+                for (uint32_t k = c.batch_off[b]; k < c.batch_off[b + 1]; ++k) c.colors[k] = (uint32_t)b;
+        } else {
+            color_constraints(c.n, c.e, c.ci.data(), c.cj.data(), c.order == XPBD_ORDER_COLOR_INDEX, c.perm,
+                              c.colors, c.batch_off);
+        }
+        max_colors = std::max<uint32_t>(max_colors, (uint32_t)c.batch_off.size() - 1);
+    }
+    // ---- host tables
+    std::vector<float4> hx(N), hv(N), hrest(N);
+    std::vector<uint32_t> row_off(N + 1, 0);
+    std::vector<uint2> inc;
+    std::vector<XpbdTile> tiles;
+    std::vector<float> palette((size_t)C * XPBD_PALETTE, 0.f);
+    std::vector<uint4> con_in(E);
+    inc.reserve(2 * (size_t)E);
+    for (uint32_t ci_ = 0; ci_ < C; ++ci_) {
+        ClothHost& c = ctx->cloths[ci_];
+        for (uint32_t i = 0; i < c.n; ++i) {
+            hx[c.vtx_off + i] = make_float4(c.pos[3 * i], c.pos[3 * i + 1], c.pos[3 * i + 2], c.w[i]);
+            hv[c.vtx_off + i] = make_float4(c.vel[3 * i], c.vel[3 * i + 1], c.vel[3 * i + 2], 0.f);
+            hrest[c.vtx_off + i] =
+                make_float4(c.rest_pos[3 * i], c.rest_pos[3 * i + 1], c.rest_pos[3 * i + 2], 0.f);
+        }
+        // compliance palette
+        std::vector<float> pal;
+        std::vector<uint32_t> pidx(c.e);
+        for (uint32_t e = 0; e < c.e; ++e) {
+            uint32_t bits;
+            memcpy(&bits, &c.comp[e], 4);
+            size_t k = 0;
+            for (; k < pal.size(); ++k) {
+                uint32_t pb;
+                memcpy(&pb, &pal[k], 4);
+                if (pb == bits) break;
+            }
+            if (k == pal.size()) {
+                if (pal.size() == XPBD_PALETTE)
+                    return fail(ctx, XPBD_ERR_UNSUPPORTED, "more than 16 distinct compliance values in one cloth");
+                pal.push_back(c.comp[e]);
+            }
+            pidx[e] = (uint32_t)k;
+        }
+        for (size_t k = 0; k < pal.size(); ++k) palette[(size_t)ci_ * XPBD_PALETTE + k] = pal[k];
+        // batch-sorted constraints and the neighbour table in reference order
+        std::vector<uint32_t> si(c.e), sj(c.e);
+        for (uint32_t k = 0; k < c.e; ++k) {
+            si[k] = c.ci[c.perm[k]];
+            sj[k] = c.cj[c.perm[k]];
+        }
+        std::vector<uint32_t> roff, other, eid;
+        neighbor_csr(c.n, c.e, si.data(), sj.data(), roff, other, eid);
+        c.lambda_inc.assign(c.e, 0xFFFFFFFFu);
+        for (uint32_t i = 0; i < c.n; ++i) {
+            const uint32_t g = c.vtx_off + i;
+            row_off[g] = (uint32_t)inc.size();
+            if (c.w[i] <= 0.f) continue;  // pinned rows stay empty: jacobi_gather returns jac_in for them
+            for (uint32_t k = roff[i]; k < roff[i + 1]; ++k) {
+                const uint32_t e_in = c.perm[eid[k]];
+                uint32_t rb;
+                memcpy(&rb, &c.rest[e_in], 4);
+                if (c.lambda_inc[e_in] == 0xFFFFFFFFu) c.lambda_inc[e_in] = (uint32_t)inc.size();
+                inc.push_back(make_uint2((other[k] + c.vtx_off) | (pidx[e_in] << 28), rb));
+            }
+        }
+        for (uint32_t first = 0; first < c.n; first += 32) {
+            XpbdTile t;
+            t.first = c.vtx_off + first;
+            t.count = (uint16_t)std::min<uint32_t>(32, c.n - first);
+            t.cloth = (uint16_t)ci_;
+            tiles.push_back(t);
+        }
+        for (uint32_t e = 0; e < c.e; ++e) {
+            uint32_t rb, cb;
+            memcpy(&rb, &c.rest[e], 4);
+            memcpy(&cb, &c.comp[e], 4);
+            con_in[c.con_off + e] = make_uint4(c.ci[e] + c.vtx_off, c.cj[e] + c.vtx_off, rb, cb);
+        }
+    }
+    row_off[N] = (uint32_t)inc.size();
+    // ---- Gauss–Seidel table, color-major across cloths
+    std::vector<uint4> con(E);
+    std::vector<uint32_t> color_off(max_colors + 1, 0);
+    {
+        uint32_t pos = 0;
+        for (uint32_t col = 0; col < max_colors; ++col) {
+            color_off[col] = pos;
+            for (auto& c : ctx->cloths) {
+                if (col + 1 >= c.batch_off.size()) continue;
+                if (c.lambda_gs.empty()) c.lambda_gs.assign(c.e, 0);
+                for (uint32_t k = c.batch_off[col]; k < c.batch_off[col + 1]; ++k) {
+                    const uint32_t e_in = c.perm[k];
+                    con[pos] = con_in[c.con_off + e_in];
+                    c.lambda_gs[e_in] = pos;
+                    ++pos;
+                }
+            }
+        }
+        color_off[max_colors] = pos;
+    }
+    // ---- device buffers
+    cudaError_t err = cudaSuccess;
+    XpbdWorld& W = ctx->W;
+    W.n = N;
+    W.e = E;
+    W.n_inc = (uint32_t)inc.size();
+    W.n_tiles = (uint32_t)tiles.size();
+    W.n_colors = max_colors;
+    W.n_cloths = C;
+#define ALLOC(ptr, T, count)                                                         \
+    do {                                                                             \
+        ptr = dev_alloc<T>(ctx, (count), &err);                                      \
+        if (err != cudaSuccess) { free_device(ctx); return cuda_fail(ctx, err, "cudaMalloc"); } \
+    } while (0)
+    float4 *x, *v, *j0, *j1, *rest;
+    uint32_t *roff_d, *color_d;
+    uint2* inc_d;
+    float *lam_inc, *pal_d, *lam_con;
+    XpbdTile* tiles_d;
+    uint4 *con_d, *con_in_d;
+    int* status;
+    XpbdGridSync* sync;
+    ALLOC(x, float4, N);
+    ALLOC(v, float4, N);
+    ALLOC(j0, float4, N);
+    ALLOC(j1, float4, N);
+    ALLOC(rest, float4, N);
+    ALLOC(roff_d, uint32_t, N + 1);
+    ALLOC(inc_d, uint2, inc.size());
+    ALLOC(lam_inc, float, inc.size());
+    ALLOC(tiles_d, XpbdTile, tiles.size());
+    ALLOC(pal_d, float, palette.size());
+    ALLOC(con_d, uint4, E);
+    ALLOC(lam_con, float, E);
+    ALLOC(color_d, uint32_t, max_colors + 1);
+    ALLOC(con_in_d, uint4, E);
+    ALLOC(ctx->dparams, XpbdDevParams, 1);
+    ALLOC(status, int, 4);
+    ALLOC(sync, XpbdGridSync, 1);
+    ALLOC(ctx->d_xyz, float, 3 * (size_t)N);
+    ALLOC(ctx->d_resid, unsigned, 4);
+    cudaStream_t st = ctx->stream;
+#define H2D(dst, src, bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), "upload")
+    H2D(x, hx.data(), N * sizeof(float4));
+    H2D(v, hv.data(), N * sizeof(float4));
+    H2D(j0, hx.data(), N * sizeof(float4));
+    H2D(j1, hx.data(), N * sizeof(float4));
+    H2D(rest, hrest.data(), N * sizeof(float4));
+    H2D(roff_d, row_off.data(), (N + 1) * sizeof(uint32_t));
+    if (!inc.empty()) H2D(inc_d, inc.data(), inc.size() * sizeof(uint2));
+    CK(cudaMemsetAsync(lam_inc, 0, std::max<size_t>(inc.size(), 1) * sizeof(float), st), "memset");
+    H2D(tiles_d, tiles.data(), tiles.size() * sizeof(XpbdTile));
+    H2D(pal_d, palette.data(), palette.size() * sizeof(float));
+    if (E) {
+        H2D(con_d, con.data(), E * sizeof(uint4));
+        H2D(con_in_d, con_in.data(), E * sizeof(uint4));
+    }
+    CK(cudaMemsetAsync(lam_con, 0, std::max<size_t>(E, 1) * sizeof(float), st), "memset");
+    H2D(color_d, color_off.data(), color_off.size() * sizeof(uint32_t));
+    CK(cudaMemsetAsync(status, 0, 4 * sizeof(int), st), "memset");
+    CK(cudaMemsetAsync(sync, 0, sizeof(XpbdGridSync), st), "memset");
+    CK(cudaStreamSynchronize(st), "commit sync");
+    W.x = x;
+    W.v = v;
+    W.jac[0] = j0;
+    W.jac[1] = j1;
+    W.rest = rest;
+    W.row_off = roff_d;
+    W.inc = inc_d;
+    W.inc_lambda = lam_inc;
+    W.tiles = tiles_d;
+    W.palette_comp = pal_d;
+    W.con = con_d;
+    W.con_lambda = lam_con;
+    W.color_off = color_d;
+    W.con_in = con_in_d;
+    W.params = ctx->dparams;
+    W.status = status;
+    W.sync = sync;
+    ensure_pinned(ctx, 16 * (size_t)N);
+    ctx->committed = true;
+    ctx->stats.num_particles = N;
+    ctx->stats.num_constraints = E;
+    ctx->stats.num_cloths = C;
+    ctx->stats.num_colors = max_colors;
+    return XPBD_OK;
+}
+
+// ------------------------------------------------------------------------------------------------- schedule
+static void choose_schedule(xpbd_ctx* ctx) {
+    uint32_t block = ctx->opts.block_threads ? ctx->opts.block_threads : 256;
+    if (block != 128 && block != 256 && block != 512 && block != 1024) block = 256;
+    int maxb = max_blocks_per_sm(ctx->opts.solver, block);
+    if (maxb < 1) maxb = 1;
+    int bps = ctx->opts.blocks_per_sm ? (int)ctx->opts.blocks_per_sm : maxb;
+    if (bps > maxb) bps = maxb;
+    // never more blocks than useful work
+    uint64_t work = ctx->opts.solver == XPBD_SOLVER_JACOBI ? (uint64_t)ctx->W.n_tiles * 32 : ctx->W.n;
+    uint32_t grid = (uint32_t)ctx->sms * (uint32_t)bps;
+    uint32_t need = (uint32_t)std::max<uint64_t>(1, (work + block - 1) / block);
+    if (grid > need) grid = need;
+    ctx->block = block;
+    ctx->grid = grid;
+    ctx->coop = ctx->coop_supported;
+    ctx->stats.grid_blocks = grid;
+    ctx->stats.block_threads = block;
+}
+
+static int ensure_collision_buffers(xpbd_ctx* ctx) {
+    const xpbd_solver_opts& o = ctx->opts;
+    const uint32_t N = ctx->W.n;
+    cudaError_t err = cudaSuccess;
+    if (!ctx->coll_ready || ctx->cb.table_bits != o.hash_table_bits) {
+        if (o.hash_table_bits < 4 || o.hash_table_bits > 28)
+            return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "hash_table_bits must be in [4, 28]");
+        CollisionBuffers& B = ctx->cb;
+        B.table_bits = o.hash_table_bits;
+        B.keys = dev_alloc<uint32_t>(ctx, N, &err);
+        if (err == cudaSuccess) B.vals = dev_alloc<uint32_t>(ctx, N, &err);
+        if (err == cudaSuccess) B.keys_sorted = dev_alloc<uint32_t>(ctx, N, &err);
+        if (err == cudaSuccess) B.vals_sorted = dev_alloc<uint32_t>(ctx, N, &err);
+        if (err == cudaSuccess) B.table_start = dev_alloc<uint32_t>(ctx, (size_t)1 << B.table_bits, &err);
+        if (err == cudaSuccess) B.pair_count = dev_alloc<uint32_t>(ctx, N + 1, &err);
+        B.sort_scratch_bytes = radix_sort_scratch_bytes(N);
+        if (err == cudaSuccess) B.sort_scratch = dev_alloc<char>(ctx, B.sort_scratch_bytes, &err);
+        if (err != cudaSuccess) return cuda_fail(ctx, err, "collision buffers");
+        // table entries are validated on use; any initial content is safe
+        CK(cudaMemsetAsync(B.table_start, 0xFF, ((size_t)1 << B.table_bits) * 4, ctx->stream), "memset");
+        ctx->coll_ready = true;
+    }
+    if (o.collision == XPBD_COLLISION_RING_FILTER && ctx->coll_ring_depth_built != o.ring_depth) {
+        std::vector<uint32_t> off, idx;
+        for (auto& c : ctx->cloths)
+            topology_rings(c.n, c.e, c.ci.data(), c.cj.data(), c.ctype.data(), o.ring_depth, c.vtx_off, off, idx);
+        uint32_t* doff = dev_alloc<uint32_t>(ctx, off.size(), &err);
+        uint32_t* didx = nullptr;
+        if (err == cudaSuccess) didx = dev_alloc<uint32_t>(ctx, idx.size(), &err);
+        if (err != cudaSuccess) return cuda_fail(ctx, err, "ring buffers");
+        CK(cudaMemcpyAsync(doff, off.data(), off.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "upload");
+        if (!idx.empty())
+            CK(cudaMemcpyAsync(didx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "upload");
+        CK(cudaStreamSynchronize(ctx->stream), "sync");
+        ctx->cb.ring_off = doff;
+        ctx->cb.ring_idx = didx;
+        ctx->coll_ring_depth_built = o.ring_depth;
+    }
+    return XPBD_OK;
+}
+
+// Enqueues one frame (opts.substeps substeps) on `st`. Returns the number of kernel launches.
+static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launches) {
+    const xpbd_solver_opts& o = ctx->opts;
+    const uint32_t S = std::max<uint32_t>(1, o.substeps);
+    const uint32_t I = ctx->tsp.inner_iterations;
+    const uint32_t solver = o.solver;
+    const bool coll = o.collision != XPBD_COLLISION_NONE && o.coll_scale > 1e-12f;
+    const uint32_t every = std::max<uint32_t>(1, o.collision_every_n_substeps);
+    const float inv_cell = ctx->hp.inv_cell;
+    cudaError_t e;
+    if (!coll) {
+        e = launch_solver(solver, ctx->block, ctx->grid, ctx->coop, ctx->W, kEndFinalize, S, 0, 0, st);
+        *launches += 1;
+        return e;
+    }
+    bool pending = false;
+    uint32_t pend = 0;
+    for (uint32_t s = 0; s < S; ++s) {
+        const bool run_coll = (s % every) == every - 1;
+        const bool last = s + 1 == S;
+        uint32_t flags = pending ? kBeginFinalize : 0u;
+        if (last && !run_coll) flags |= kEndFinalize;
+        const uint32_t start = (solver == XPBD_SOLVER_JACOBI) ? pend : 0u;
+        e = launch_solver(solver, ctx->block, ctx->grid, ctx->coop, ctx->W, flags, 1, pend, start, st);
+        *launches += 1;
+        if (e != cudaSuccess) return e;
+        if (last && !run_coll) return cudaSuccess;
+        const uint32_t fin = (solver == XPBD_SOLVER_JACOBI) ? ((start + I) & 1u) : 0u;
+        if (run_coll) {
+            e = collision_build(ctx->W, ctx->W.jac[fin], ctx->cb, inv_cell, ctx->sms, st, launches);
+            if (e != cudaSuccess) return e;
+            e = collision_resolve(ctx->W, ctx->W.jac[fin], ctx->W.jac[fin ^ 1u], ctx->cb, inv_cell, o.collision,
+                                  ctx->sms, st, launches);
+            if (e != cudaSuccess) return e;
+            pend = fin ^ 1u;
+        } else {
+            pend = fin;
+        }
+        pending = true;
+    }
+    e = launch_finalize(ctx->W, pend, ctx->sms, st);
+    *launches += 1;
+    return e;
+}
+
+static std::string schedule_key(xpbd_ctx* ctx) {
+    const xpbd_solver_opts& o = ctx->opts;
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%u/%u/%u/%u/%u/%u/%u/%u/%d/%p/%u/%u", o.solver, o.substeps, o.collision,
+             o.collision_every_n_substeps, ctx->tsp.inner_iterations, ctx->block, ctx->grid, (int)ctx->coop,
+             (int)(o.coll_scale > 1e-12f), (void*)ctx->stream, o.hash_table_bits, o.ring_depth);
+    return buf;
+}
+
+static int check_ready(xpbd_ctx* ctx) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "xpbd_commit has not been called");
+    if (!ctx->params_set) return fail(ctx, XPBD_ERR_STATE, "xpbd_set_params has not been called");
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_set_params(xpbd_ctx* ctx, const xpbd_time_step_params* params, const xpbd_solver_opts* opts) {
+    if (!ctx || !params) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "xpbd_commit has not been called");
+    if (!(params->dt > 0.f) || !std::isfinite(params->inv_dt))
+        return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "dt must be positive");
+    if (opts) {
+        if (opts->solver > XPBD_SOLVER_GAUSS_SEIDEL || opts->relaxation > XPBD_RELAX_AVERAGE ||
+            opts->lambda_mode > XPBD_LAMBDA_PER_SUBSTEP || opts->collision > XPBD_COLLISION_RING_FILTER)
+            return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "unknown solver option value");
+        if (opts->collision != XPBD_COLLISION_NONE && !(opts->hash_cell >= opts->thickness))
+            return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "hash_cell must be >= thickness");
+        if (opts->warm_start) return fail(ctx, XPBD_ERR_UNSUPPORTED, "learned warm start is not built yet");
+        ctx->opts = *opts;
+    }
+    ctx->tsp = *params;
+    fill_dev_params(ctx);
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream),
+       "params upload");
+    if (ctx->opts.collision != XPBD_COLLISION_NONE) {
+        int r = ensure_collision_buffers(ctx);
+        if (r != XPBD_OK) return r;
+    }
+    choose_schedule(ctx);
+    ctx->params_set = true;
+    return XPBD_OK;
+}
+
+static int run_frames(xpbd_ctx* ctx, uint32_t frames) {
+    cudaStream_t st = ctx->stream;
+    if (ctx->opts.use_graphs) {
+        std::string key = schedule_key(ctx);
+        if (!ctx->exec || key != ctx->graph_key) {
+            if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
+            ctx->exec = nullptr;
+            cudaGraph_t g = nullptr;
+            uint64_t launches = 0;
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+            cudaError_t e = enqueue_frame(ctx, st, &launches);
+            cudaError_t e2 = cudaStreamEndCapture(st, &g);
+            if (e != cudaSuccess || e2 != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                if (ctx->coop) {  // retry without the cooperative attribute (bounded barriers still hold)
+                    ctx->coop = false;
+                    return run_frames(ctx, frames);
+                }
+                return cuda_fail(ctx, e != cudaSuccess ? e : e2, "frame graph capture");
+            }
+            e = cudaGraphInstantiate(&ctx->exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "graph instantiate");
+            ctx->graph_key = key;
+            ctx->graph_nodes = launches;
+        }
+        for (uint32_t f = 0; f < frames; ++f) CK(cudaGraphLaunch(ctx->exec, st), "graph launch");
+        ctx->stats.kernel_launches += ctx->graph_nodes * frames;
+        ctx->stats.graph_captured = 1;
+    } else {
+        for (uint32_t f = 0; f < frames; ++f) {
+            uint64_t launches = 0;
+            cudaError_t e = enqueue_frame(ctx, st, &launches);
+            if (e != cudaSuccess && ctx->coop) {
+                cudaGetLastError();
+                ctx->coop = false;
+                e = enqueue_frame(ctx, st, &launches);
+            }
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "frame launch");
+            ctx->stats.kernel_launches += launches;
+        }
+        ctx->stats.graph_captured = 0;
+    }
+    ctx->stats.cooperative_launch = ctx->coop ? 1 : 0;
+    ctx->stats.frames += frames;
+    ctx->stats.substeps += (uint64_t)frames * std::max<uint32_t>(1, ctx->opts.substeps);
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_step(xpbd_ctx* ctx, uint32_t frames) {
+    int r = check_ready(ctx);
+    if (r != XPBD_OK) return r;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    return run_frames(ctx, frames);
+}
+
+extern "C" int xpbd_step_params(xpbd_ctx* ctx, const xpbd_time_step_params* params, uint32_t frames) {
+    int r = xpbd_set_params(ctx, params, nullptr);
+    if (r != XPBD_OK) return r;
+    return xpbd_step(ctx, frames);
+}
+
+extern "C" int xpbd_substep(xpbd_ctx* ctx, uint32_t substeps) {
+    int r = check_ready(ctx);
+    if (r != XPBD_OK) return r;
+    xpbd_solver_opts saved = ctx->opts;
+    ctx->opts.substeps = 1;
+    ctx->opts.use_graphs = 0;
+    choose_schedule(ctx);
+    for (uint32_t s = 0; s < substeps && r == XPBD_OK; ++s) r = run_frames(ctx, 1);
+    ctx->stats.frames -= substeps;
+    ctx->opts = saved;
+    choose_schedule(ctx);
+    return r;
+}
+
+static int read_status(xpbd_ctx* ctx) {
+    int h[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(h, ctx->W.status, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "status read");
+    CK(cudaStreamSynchronize(ctx->stream), "stream sync");
+    if (h[0] == 0) return XPBD_OK;
+    // clear the status and the barrier state so the context stays usable
+    CK(cudaMemsetAsync(ctx->W.status, 0, 4 * sizeof(int), ctx->stream), "memset");
+    CK(cudaMemsetAsync(ctx->W.sync, 0, sizeof(XpbdGridSync), ctx->stream), "memset");
+    CK(cudaStreamSynchronize(ctx->stream), "stream sync");
+    if (h[0] & XPBD_DEV_BARRIER_TIMEOUT) return fail(ctx, XPBD_ERR_BARRIER_TIMEOUT, "grid barrier wait timed out");
+    if (h[0] & XPBD_DEV_NONFINITE) return fail(ctx, XPBD_ERR_DEVICE_NONFINITE, "non-finite position or velocity");
+    if (h[0] & XPBD_DEV_CAPACITY) return fail(ctx, XPBD_ERR_CAPACITY, "device capacity exceeded");
+    return fail(ctx, XPBD_ERR_INDEX_RANGE, "device index out of range");
+}
+
+extern "C" int xpbd_sync(xpbd_ctx* ctx) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return XPBD_OK;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    return read_status(ctx);
+}
+
+// ------------------------------------------------------------------------------------------------- state
+__global__ static void pack_xyz_kernel(const float4* __restrict__ src, uint32_t n, float* __restrict__ dst) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 p = src[i];
+        dst[3 * i] = p.x;
+        dst[3 * i + 1] = p.y;
+        dst[3 * i + 2] = p.z;
+    }
+}
+
+static int read_vec(xpbd_ctx* ctx, const float4* src, uint32_t cloth_id, float* out) {
+    if (!ctx || !out) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    uint32_t off = 0, n = ctx->W.n;
+    if (cloth_id != 0xFFFFFFFFu) {
+        if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+        off = ctx->cloths[cloth_id].vtx_off;
+        n = ctx->cloths[cloth_id].n;
+    }
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    uint32_t grid = std::min<uint32_t>((n + 255) / 256, (uint32_t)ctx->sms * 8);
+    pack_xyz_kernel<<<std::max<uint32_t>(grid, 1), 256, 0, ctx->stream>>>(src + off, n, ctx->d_xyz);
+    CK(cudaGetLastError(), "pack");
+    const size_t bytes = 3 * (size_t)n * sizeof(float);
+    if (ctx->pinned && ctx->pinned_bytes >= bytes) {
+        CK(cudaMemcpyAsync(ctx->pinned, ctx->d_xyz, bytes, cudaMemcpyDeviceToHost, ctx->stream), "readback");
+        int r = read_status(ctx);
+        memcpy(out, ctx->pinned, bytes);
+        return r;
+    }
+    CK(cudaMemcpyAsync(out, ctx->d_xyz, bytes, cudaMemcpyDeviceToHost, ctx->stream), "readback");
+    return read_status(ctx);
+}
+
+extern "C" int xpbd_read_positions(xpbd_ctx* ctx, uint32_t cloth_id, float* out_xyz) {
+    return read_vec(ctx, ctx ? ctx->W.x : nullptr, cloth_id, out_xyz);
+}
+extern "C" int xpbd_read_velocities(xpbd_ctx* ctx, uint32_t cloth_id, float* out_xyz) {
+    return read_vec(ctx, ctx ? ctx->W.v : nullptr, cloth_id, out_xyz);
+}
+
+static int upload_state(xpbd_ctx* ctx, uint32_t cloth_id, const float* xyz, const float* vel, bool from_initial) {
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    for (uint32_t c = 0; c < ctx->cloths.size(); ++c) {
+        if (cloth_id != 0xFFFFFFFFu && c != cloth_id) continue;
+        ClothHost& h = ctx->cloths[c];
+        std::vector<float4> x(h.n), v(h.n);
+        for (uint32_t i = 0; i < h.n; ++i) {
+            const float* p = from_initial ? &h.pos[3 * i] : (xyz ? &xyz[3 * i] : nullptr);
+            const float* q = from_initial ? nullptr : (vel ? &vel[3 * i] : nullptr);
+            x[i] = p ? make_float4(p[0], p[1], p[2], h.w[i]) : make_float4(0, 0, 0, h.w[i]);
+            v[i] = q ? make_float4(q[0], q[1], q[2], 0.f) : make_float4(0, 0, 0, 0);
+        }
+        if (from_initial || xyz) {
+            if (!from_initial && !xyz) continue;
+            CK(cudaMemcpy(ctx->W.x + h.vtx_off, x.data(), h.n * sizeof(float4), cudaMemcpyHostToDevice), "upload");
+            CK(cudaMemcpy(ctx->W.jac[0] + h.vtx_off, x.data(), h.n * sizeof(float4), cudaMemcpyHostToDevice), "upload");
+            CK(cudaMemcpy(ctx->W.jac[1] + h.vtx_off, x.data(), h.n * sizeof(float4), cudaMemcpyHostToDevice), "upload");
+        }
+        if (from_initial || vel)
+            CK(cudaMemcpy(ctx->W.v + h.vtx_off, v.data(), h.n * sizeof(float4), cudaMemcpyHostToDevice), "upload");
+    }
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_write_state(xpbd_ctx* ctx, uint32_t cloth_id, const float* xyz, const float* vel_xyz) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    if (cloth_id != 0xFFFFFFFFu && cloth_id >= ctx->cloths.size())
+        return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+    if (cloth_id == 0xFFFFFFFFu && ctx->cloths.size() > 1 && (xyz || vel_xyz)) {
+        // packed arrays for all cloths
+        uint32_t off = 0;
+        for (uint32_t c = 0; c < ctx->cloths.size(); ++c) {
+            int r = upload_state(ctx, c, xyz ? xyz + 3 * (size_t)off : nullptr,
+                                 vel_xyz ? vel_xyz + 3 * (size_t)off : nullptr, false);
+            if (r != XPBD_OK) return r;
+            off += ctx->cloths[c].n;
+        }
+        return XPBD_OK;
+    }
+    return upload_state(ctx, cloth_id, xyz, vel_xyz, false);
+}
+
+extern "C" int xpbd_reset(xpbd_ctx* ctx) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    int r = upload_state(ctx, 0xFFFFFFFFu, nullptr, nullptr, true);
+    if (r != XPBD_OK) return r;
+    CK(cudaMemset(ctx->W.inc_lambda, 0, std::max<size_t>(ctx->W.n_inc, 1) * 4), "memset");
+    CK(cudaMemset(ctx->W.con_lambda, 0, std::max<size_t>(ctx->W.e, 1) * 4), "memset");
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_read_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out) {
+    if (!ctx || !out) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const ClothHost& h = ctx->cloths[cloth_id];
+    const bool jac = ctx->opts.solver == XPBD_SOLVER_JACOBI;
+    std::vector<float> all(jac ? std::max<uint32_t>(ctx->W.n_inc, 1) : std::max<uint32_t>(ctx->W.e, 1));
+    CK(cudaMemcpyAsync(all.data(), jac ? ctx->W.inc_lambda : ctx->W.con_lambda, all.size() * 4,
+                       cudaMemcpyDeviceToHost, ctx->stream), "readback");
+    int r = read_status(ctx);
+    for (uint32_t e = 0; e < h.e; ++e) {
+        if (jac) out[e] = h.lambda_inc[e] == 0xFFFFFFFFu ? 0.f : all[h.lambda_inc[e]];
+        else out[e] = all[h.lambda_gs[e]];
+    }
+    return r;
+}
+
+extern "C" int xpbd_strain_residual(xpbd_ctx* ctx, uint32_t cloth_id, float* out) {
+    if (!ctx || !out) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    uint32_t e0 = 0, e1 = ctx->W.e;
+    if (cloth_id != 0xFFFFFFFFu) {
+        if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+        e0 = ctx->cloths[cloth_id].con_off;
+        e1 = e0 + ctx->cloths[cloth_id].e;
+    }
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaMemsetAsync(ctx->d_resid, 0, 4, ctx->stream), "memset");
+    if (e1 > e0) CK(launch_strain_residual(ctx->W, e0, e1, ctx->d_resid, ctx->sms, ctx->stream), "residual");
+    unsigned bits = 0;
+    CK(cudaMemcpyAsync(&bits, ctx->d_resid, 4, cudaMemcpyDeviceToHost, ctx->stream), "readback");
+    int r = read_status(ctx);
+    memcpy(out, &bits, 4);
+    return r;
+}
+
+extern "C" int xpbd_get_stats(xpbd_ctx* ctx, xpbd_stats* out) {
+    if (!ctx || !out) return XPBD_ERR_INVALID_ARGUMENT;
+    *out = ctx->stats;
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_get_coloring(xpbd_ctx* ctx, uint32_t cloth_id, uint32_t* perm, uint32_t* offsets,
+                                 uint32_t* batch_count) {
+    if (!ctx || !batch_count) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+    const ClothHost& h = ctx->cloths[cloth_id];
+    *batch_count = (uint32_t)h.batch_off.size() - 1;
+    if (perm) std::copy(h.perm.begin(), h.perm.end(), perm);
+    if (offsets) std::copy(h.batch_off.begin(), h.batch_off.end(), offsets);
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_color_constraints(uint32_t n, uint32_t e_count, const uint32_t* ci, const uint32_t* cj,
+                                      uint32_t order, uint32_t* perm, uint32_t* offsets, uint32_t* batch_count) {
+    if (!batch_count || (e_count && (!ci || !cj || !perm || !offsets))) return XPBD_ERR_INVALID_ARGUMENT;
+    if (order != XPBD_ORDER_COLOR_REFERENCE && order != XPBD_ORDER_COLOR_INDEX) return XPBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t e = 0; e < e_count; ++e)
+        if (ci[e] >= n || cj[e] >= n || ci[e] == cj[e]) return XPBD_ERR_INDEX_RANGE;
+    std::vector<uint32_t> p, colors, offs;
+    color_constraints(n, e_count, ci, cj, order == XPBD_ORDER_COLOR_INDEX, p, colors, offs);
+    *batch_count = (uint32_t)offs.size() - 1;
+    if (perm) std::copy(p.begin(), p.end(), perm);
+    if (offsets) std::copy(offs.begin(), offs.end(), offsets);
+    return XPBD_OK;
+}
+
+// ------------------------------------------------------------------------------------------------- autotune
+extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* opts_out) {
+    int r = check_ready(ctx);
+    if (r != XPBD_OK) return r;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const uint32_t N = ctx->W.n;
+    float4 *sx = nullptr, *sv = nullptr;
+    CK(cudaMalloc(&sx, (size_t)N * sizeof(float4)), "snapshot");
+    CK(cudaMalloc(&sv, (size_t)N * sizeof(float4)), "snapshot");
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(sx, ctx->W.x, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "snapshot");
+    CK(cudaMemcpyAsync(sv, ctx->W.v, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "snapshot");
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    xpbd_solver_opts base = ctx->opts;
+    float best = 1e30f;
+    uint32_t best_block = 256, best_bps = 0;
+    const uint32_t blocks[] = {128, 256, 512};
+    for (uint32_t blk : blocks) {
+        int maxb = max_blocks_per_sm(base.solver, blk);
+        for (int bps = 1; bps <= maxb; bps *= 2) {
+            ctx->opts = base;
+            ctx->opts.block_threads = blk;
+            ctx->opts.blocks_per_sm = (uint32_t)bps;
+            choose_schedule(ctx);
+            r = run_frames(ctx, 1);  // warm-up / capture
+            if (r != XPBD_OK) break;
+            cudaEventRecord(a, st);
+            r = run_frames(ctx, std::max<uint32_t>(1, frames));
+            cudaEventRecord(b, st);
+            if (r != XPBD_OK) break;
+            r = read_status(ctx);
+            if (r != XPBD_OK) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (ms < best) {
+                best = ms;
+                best_block = blk;
+                best_bps = (uint32_t)bps;
+            }
+            CK(cudaMemcpyAsync(ctx->W.x, sx, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
+            CK(cudaMemcpyAsync(ctx->W.v, sv, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
+        }
+        if (r != XPBD_OK) break;
+    }
+    CK(cudaMemcpyAsync(ctx->W.x, sx, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
+    CK(cudaMemcpyAsync(ctx->W.v, sv, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
+    cudaStreamSynchronize(st);
+    cudaFree(sx);
+    cudaFree(sv);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    ctx->opts = base;
+    if (r == XPBD_OK) {
+        ctx->opts.block_threads = best_block;
+        ctx->opts.blocks_per_sm = best_bps;
+    }
+    choose_schedule(ctx);
+    if (opts_out) *opts_out = ctx->opts;
+    return r;
+}
+
+// ------------------------------------------------------------------------------------------------- collision
+extern "C" int xpbd_collision_keys(xpbd_ctx* ctx, uint32_t* keys, uint32_t* sorted_keys, uint32_t* sorted_vals) {
+    int r = check_ready(ctx);
+    if (r != XPBD_OK) return r;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    r = ensure_collision_buffers(ctx);
+    if (r != XPBD_OK) return r;
+    uint64_t launches = 0;
+    CK(collision_build(ctx->W, ctx->W.x, ctx->cb, ctx->hp.inv_cell, ctx->sms, ctx->stream, &launches), "build");
+    const size_t bytes = (size_t)ctx->W.n * 4;
+    if (keys) CK(cudaMemcpyAsync(keys, ctx->cb.keys, bytes, cudaMemcpyDeviceToHost, ctx->stream), "readback");
+    if (sorted_keys)
+        CK(cudaMemcpyAsync(sorted_keys, ctx->cb.keys_sorted, bytes, cudaMemcpyDeviceToHost, ctx->stream), "readback");
+    if (sorted_vals)
+        CK(cudaMemcpyAsync(sorted_vals, ctx->cb.vals_sorted, bytes, cudaMemcpyDeviceToHost, ctx->stream), "readback");
+    return read_status(ctx);
+}
+
+extern "C" int xpbd_collision_pairs(xpbd_ctx* ctx, uint32_t* pairs, uint64_t cap, uint64_t* count) {
+    int r = check_ready(ctx);
+    if (r != XPBD_OK) return r;
+    if (!count) return XPBD_ERR_INVALID_ARGUMENT;
+    if (ctx->opts.collision == XPBD_COLLISION_NONE) return fail(ctx, XPBD_ERR_STATE, "collision is off");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    r = ensure_collision_buffers(ctx);
+    if (r != XPBD_OK) return r;
+    uint64_t launches = 0;
+    CK(collision_build(ctx->W, ctx->W.x, ctx->cb, ctx->hp.inv_cell, ctx->sms, ctx->stream, &launches), "build");
+    uint32_t* dpairs = nullptr;
+    uint64_t cap_d = 0;
+    uint64_t total = 0;
+    // first pass counts; then allocate and write
+    CK(collision_pairs(ctx->W, ctx->W.x, ctx->cb, ctx->hp.inv_cell, ctx->opts.collision, nullptr, 0, &total,
+                       ctx->sms, ctx->stream), "pair count");
+    *count = total;
+    ctx->stats.collision_pairs = total;
+    if (pairs && cap > 0 && total > 0) {
+        cap_d = std::min<uint64_t>(cap, total);
+        CK(cudaMalloc(&dpairs, cap_d * 8), "pairs");
+        uint64_t t2 = 0;
+        cudaError_t e = collision_pairs(ctx->W, ctx->W.x, ctx->cb, ctx->hp.inv_cell, ctx->opts.collision, dpairs,
+                                        cap_d, &t2, ctx->sms, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(pairs, dpairs, cap_d * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        cudaFree(dpairs);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "pair write");
+    }
+    return read_status(ctx);
+}
+
+// ------------------------------------------------------------------------------------------------- primitives
+extern "C" size_t xpbd_radix_sort_scratch_bytes(uint32_t n) { return radix_sort_scratch_bytes(n); }
+
+extern "C" int xpbd_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                     uint32_t* vals_out, uint32_t n, uint32_t passes, void* scratch,
+                                     size_t scratch_bytes, void* stream) {
+    if (n && (!keys_in || !vals_in || !keys_out || !vals_out || !scratch)) return XPBD_ERR_INVALID_ARGUMENT;
+    if (passes < 1 || passes > 4) return XPBD_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < radix_sort_scratch_bytes(n)) return XPBD_ERR_INVALID_ARGUMENT;
+    if (keys_in == keys_out || vals_in == vals_out) return XPBD_ERR_INVALID_ARGUMENT;
+    cudaError_t e = radix_sort_pairs(keys_in, vals_in, keys_out, vals_out, n, passes, scratch, scratch_bytes,
+                                     (cudaStream_t)stream, nullptr);
+    return e == cudaSuccess ? XPBD_OK : XPBD_ERR_CUDA;
+}
+
+extern "C" int xpbd_hash_keys(const float* xyzw, uint32_t n, float inv_cell, uint32_t table_bits, uint32_t* keys,
+                              void* stream) {
+    if (n && (!xyzw || !keys)) return XPBD_ERR_INVALID_ARGUMENT;
+    if (table_bits < 1 || table_bits > 32) return XPBD_ERR_INVALID_ARGUMENT;
+    cudaError_t e = launch_hash_keys((const float4*)xyzw, n, inv_cell, table_bits, keys, nullptr,
+                                     (cudaStream_t)stream);
+    return e == cudaSuccess ? XPBD_OK : XPBD_ERR_CUDA;
+}
+
+// ------------------------------------------------------------------------------------------------- diagnostics
+extern "C" const char* xpbd_last_error(xpbd_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+extern "C" const char* xpbd_status_string(int s) {
+    switch (s) {
+        case XPBD_OK: return "ok";
+        case XPBD_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case XPBD_ERR_CUDA: return "CUDA error";
+        case XPBD_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case XPBD_ERR_UNSUPPORTED: return "unsupported";
+        case XPBD_ERR_STATE: return "invalid state";
+        case XPBD_ERR_DEVICE_NONFINITE: return "non-finite state on device";
+        case XPBD_ERR_BARRIER_TIMEOUT: return "grid barrier timeout";
+        case XPBD_ERR_INDEX_RANGE: return "index out of range";
+        case XPBD_ERR_CAPACITY: return "capacity exceeded";
+        case XPBD_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+extern "C" int xpbd_debug_force_barrier_timeout(xpbd_ctx* ctx, float timeout_ms) {
+    int r = check_ready(ctx);
+    if (r != XPBD_OK) return r;
+    if (!(timeout_ms > 0.f) || timeout_ms > 10000.f)
+        return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "timeout must be in (0, 10000] ms");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    // one extra expected block: the barrier can never complete and must time out
+    XpbdGridSync gs = {0u, 0u, 1u, 0u};
+    ctx->forced_timeout_ms = timeout_ms;
+    fill_dev_params(ctx);
+    CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream), "p");
+    CK(cudaMemcpyAsync(ctx->W.sync, &gs, sizeof(gs), cudaMemcpyHostToDevice, ctx->stream), "sync");
+    xpbd_solver_opts saved = ctx->opts;
+    ctx->opts.use_graphs = 0;
+    cudaError_t e = launch_solver(ctx->opts.solver, ctx->block, ctx->grid, ctx->coop, ctx->W, kEndFinalize, 1, 0, 0,
+                                  ctx->stream);
+    ctx->opts = saved;
+    ctx->forced_timeout_ms = 0.f;
+    fill_dev_params(ctx);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "forced launch");
+    r = read_status(ctx);  // expected XPBD_ERR_BARRIER_TIMEOUT; also resets the barrier state
+    CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream), "p");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    return r;
+}

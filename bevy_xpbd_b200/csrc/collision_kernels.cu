@@ -1,0 +1,448 @@
+// Self-collision for sm_100a: spatial-hash keys, stable LSD radix sort of (32-bit key, particle) pairs, bucket
+// table, 27-cell neighbour query with the reference narrow phase.
+//
+// Reference: the GPU path of cloth_sim_jacobi.wgsl (keys :243-253, radix sort :299-355, cell ranges :362-384,
+// collide_grid_cells + narrow_self_collision_pair :386-470, collide_apply :472-490) and the CPU solver it is judged
+// against, self_collision_resolve (xpbd_cpu.rs:67-137). Differences by design:
+//   * keys: integer cell coordinates floor(x / cell) hashed with the primes 73856093 / 19349663 / 83492791 (XOR of
+//     wrapping u32 products) into a 2^bits table, instead of a dense clamped grid;
+//   * the sort is stable (per-tile ranks from warp match_any in input order) — the reference's atomic scatter is not;
+//   * accumulation is deterministic: each particle gathers its own partners and sums their corrections in increasing
+//     partner index, which is exactly the order of the reference's all-pairs loop, so the FP32 result matches
+//     self_collision_resolve bit for bit (the reference GPU path truncates to i32 fixed point instead).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "xpbd_internal.h"
+#include "xpbd_kernels.h"
+
+namespace xpbd {
+
+constexpr unsigned kFullMask = 0xFFFFFFFFu;
+constexpr float kCollisionApplyClamp = 0.35f;  // COLLISION_APPLY_CLAMP, cloth_compute.rs:90
+
+// ---------------------------------------------------------------------------------------------- hash keys
+__device__ __forceinline__ int3 cell_of(float4 p, float inv_cell) {
+    return make_int3((int)floorf(__fmul_rn(p.x, inv_cell)), (int)floorf(__fmul_rn(p.y, inv_cell)),
+                     (int)floorf(__fmul_rn(p.z, inv_cell)));
+}
+__device__ __forceinline__ uint32_t hash_cell(int3 c, uint32_t mask) {
+    return (((uint32_t)c.x * 73856093u) ^ ((uint32_t)c.y * 19349663u) ^ ((uint32_t)c.z * 83492791u)) & mask;
+}
+
+__global__ void hash_keys_kernel(const float4* __restrict__ x, uint32_t n, float inv_cell, uint32_t mask,
+                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        keys[i] = hash_cell(cell_of(x[i], inv_cell), mask);
+        if (vals) vals[i] = i;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------- radix sort
+// Per pass (8-bit digit): per-tile digit histogram → one exclusive scan over the digit-major (digit, tile)
+// counts → stable scatter. Tile = 8 warps × 8 rounds × 32 keys; within a tile the order is warp, round, lane.
+constexpr int kSortBlock = 256;
+constexpr int kSortItems = 8;
+constexpr uint32_t kSortTile = kSortBlock * kSortItems;
+
+__global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(const uint32_t* __restrict__ keys, uint32_t n,
+                                                                 uint32_t shift, uint32_t tiles,
+                                                                 uint32_t* __restrict__ counts) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * kSortTile;
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        uint32_t idx = base + r * kSortBlock + threadIdx.x;
+        if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 0xFFu], 1u);
+    }
+    __syncthreads();
+    counts[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Single-block exclusive scan of `m` u32 values in place (each thread scans a contiguous chunk).
+__global__ void __launch_bounds__(1024) exclusive_scan_kernel(uint32_t* __restrict__ a, uint32_t m,
+                                                               uint32_t* __restrict__ total) {
+    __shared__ uint32_t ws[32];
+    const uint32_t per = (m + blockDim.x - 1) / blockDim.x;
+    const uint32_t b0 = threadIdx.x * per;
+    const uint32_t b1 = min(b0 + per, m);
+    uint32_t sum = 0;
+    for (uint32_t k = b0; k < b1; ++k) sum += a[k];
+    // block exclusive scan of per-thread sums
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(kFullMask, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    if (lane == 31) ws[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t v = (lane < (blockDim.x >> 5)) ? ws[lane] : 0u;
+        uint32_t inc2 = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(kFullMask, inc2, o);
+            if (lane >= (uint32_t)o) inc2 += t;
+        }
+        ws[lane] = inc2 - v;
+    }
+    __syncthreads();
+    uint32_t run = ws[warp] + incl - sum;
+    for (uint32_t k = b0; k < b1; ++k) {
+        uint32_t t = a[k];
+        a[k] = run;
+        run += t;
+    }
+    if (total && threadIdx.x == blockDim.x - 1) *total = run;
+}
+
+__global__ void __launch_bounds__(kSortBlock) radix_scatter_kernel(const uint32_t* __restrict__ keys_in,
+                                                                    const uint32_t* __restrict__ vals_in,
+                                                                    uint32_t* __restrict__ keys_out,
+                                                                    uint32_t* __restrict__ vals_out, uint32_t n,
+                                                                    uint32_t shift, uint32_t tiles,
+                                                                    const uint32_t* __restrict__ offsets) {
+    __shared__ uint32_t s_wcnt[kSortBlock / 32][256];
+    __shared__ uint32_t s_base[256];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (uint32_t k = threadIdx.x; k < (kSortBlock / 32) * 256; k += kSortBlock) (&s_wcnt[0][0])[k] = 0;
+    __syncthreads();
+    const uint32_t lanemask_lt = (1u << lane) - 1u;
+    const uint32_t wbase = blockIdx.x * kSortTile + warp * (32 * kSortItems);
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const uint32_t idx = wbase + r * 32 + lane;
+        const bool valid = idx < n;
+        key[r] = valid ? keys_in[idx] : 0u;
+        val[r] = valid ? vals_in[idx] : 0u;
+        const uint32_t d = valid ? ((key[r] >> shift) & 0xFFu) : 0x100u;
+        const uint32_t peers = __match_any_sync(kFullMask, d);
+        uint32_t before = 0;
+        if (valid) before = s_wcnt[warp][d];
+        __syncwarp();
+        if (valid && lane == (uint32_t)(__ffs(peers) - 1)) s_wcnt[warp][d] = before + __popc(peers);
+        __syncwarp();
+        rank[r] = valid ? before + __popc(peers & lanemask_lt) : 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    {  // exclusive prefix over warps, per digit; tile base from the global scan
+        const uint32_t d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kSortBlock / 32; ++w) {
+            uint32_t t = s_wcnt[w][d];
+            s_wcnt[w][d] = run;
+            run += t;
+        }
+        s_base[d] = offsets[d * tiles + blockIdx.x];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        if (rank[r] == 0xFFFFFFFFu) continue;
+        const uint32_t d = (key[r] >> shift) & 0xFFu;
+        const uint32_t pos = s_base[d] + s_wcnt[warp][d] + rank[r];
+        if (pos < n) {
+            keys_out[pos] = key[r];
+            vals_out[pos] = val[r];
+        }
+    }
+}
+
+size_t radix_sort_scratch_bytes(uint32_t n) {
+    size_t tiles = (n + kSortTile - 1) / kSortTile;
+    if (tiles == 0) tiles = 1;
+    size_t counts = 256 * tiles * sizeof(uint32_t);
+    size_t tmp = 2 * (size_t)n * sizeof(uint32_t);  // ping-pong keys/vals for even pass counts
+    return ((counts + 255) & ~(size_t)255) + ((tmp + 255) & ~(size_t)255) + 256;
+}
+
+cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                             uint32_t* vals_out, uint32_t n, uint32_t passes, void* scratch, size_t scratch_bytes,
+                             cudaStream_t st, uint64_t* launches) {
+    if (passes < 1 || passes > 4) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    if (scratch_bytes < radix_sort_scratch_bytes(n)) return cudaErrorInvalidValue;
+    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    size_t counts_bytes = ((256 * (size_t)tiles * sizeof(uint32_t)) + 255) & ~(size_t)255;
+    uint32_t* counts = (uint32_t*)scratch;
+    uint32_t* tmp_k = (uint32_t*)((char*)scratch + counts_bytes);
+    uint32_t* tmp_v = tmp_k + n;
+    // choose ping-pong so that the last pass writes keys_out/vals_out
+    const uint32_t* src_k = keys_in;
+    const uint32_t* src_v = vals_in;
+    for (uint32_t p = 0; p < passes; ++p) {
+        const bool to_out = ((passes - 1 - p) % 2) == 0;
+        uint32_t* dk = to_out ? keys_out : tmp_k;
+        uint32_t* dv = to_out ? vals_out : tmp_v;
+        const uint32_t shift = 8u * p;
+        radix_hist_kernel<<<tiles, kSortBlock, 0, st>>>(src_k, n, shift, tiles, counts);
+        exclusive_scan_kernel<<<1, 1024, 0, st>>>(counts, 256 * tiles, nullptr);
+        radix_scatter_kernel<<<tiles, kSortBlock, 0, st>>>(src_k, src_v, dk, dv, n, shift, tiles, counts);
+        if (launches) *launches += 3;
+        src_k = dk;
+        src_v = dv;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hash_keys(const float4* x, uint32_t n, float inv_cell, uint32_t bits, uint32_t* keys,
+                             uint32_t* vals, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    uint32_t grid = (n + 255) / 256;
+    if (grid > 148u * 16u) grid = 148u * 16u;
+    hash_keys_kernel<<<grid, 256, 0, st>>>(x, n, inv_cell, (bits >= 32) ? 0xFFFFFFFFu : ((1u << bits) - 1u), keys,
+                                           vals);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------- bucket table
+__global__ void bucket_table_kernel(const uint32_t* __restrict__ skeys, uint32_t n, uint32_t* __restrict__ start) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t k = skeys[p];
+        if (p == 0 || skeys[p - 1] != k) start[k] = p;
+    }
+}
+
+cudaError_t collision_build(const XpbdWorld& W, const float4* pos, const CollisionBuffers& B, float inv_cell,
+                            int sms, cudaStream_t st, uint64_t* launches) {
+    cudaError_t e = launch_hash_keys(pos, W.n, inv_cell, B.table_bits, B.keys, B.vals, st);
+    if (e != cudaSuccess) return e;
+    e = radix_sort_pairs(B.keys, B.vals, B.keys_sorted, B.vals_sorted, W.n, 4, B.sort_scratch,
+                         B.sort_scratch_bytes, st, launches);
+    if (e != cudaSuccess) return e;
+    uint32_t grid = (W.n + 255) / 256;
+    if (grid > (uint32_t)sms * 8) grid = (uint32_t)sms * 8;
+    if (grid == 0) grid = 1;
+    bucket_table_kernel<<<grid, 256, 0, st>>>(B.keys_sorted, W.n, B.table_start);
+    if (launches) *launches += 2;
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------- narrow phase
+struct F3c {
+    float x, y, z;
+};
+__device__ __forceinline__ float dot3c(F3c a, F3c b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+
+__device__ __forceinline__ bool ring_contains(const uint32_t* __restrict__ off, const uint32_t* __restrict__ idx,
+                                              uint32_t a, uint32_t b) {
+    uint32_t lo = off[a], hi = off[a + 1];
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint32_t v = idx[mid];
+        if (v == b) return true;
+        if (v < b) lo = mid + 1; else hi = mid;
+    }
+    return false;
+}
+
+// Pair (a<b) narrow phase of xpbd_cpu.rs:84-121 (filter 1: rest-distance test :94-100; filter 2: ring filter).
+// On acceptance returns the correction of particle `self` (a or b).
+__device__ __forceinline__ bool narrow_pair(const float4* __restrict__ src, const float4* __restrict__ rest,
+                                            const CollisionBuffers& B, uint32_t filter, float thickness,
+                                            float coll_scale, uint32_t a, uint32_t b, uint32_t self, F3c& out) {
+    const float4 pa = src[a], pb = src[b];
+    const float w_a = pa.w, w_b = pb.w;
+    if (w_a <= 0.0f && w_b <= 0.0f) return false;
+    const float t2 = __fmul_rn(thickness, thickness);
+    F3c d = {__fsub_rn(pb.x, pa.x), __fsub_rn(pb.y, pa.y), __fsub_rn(pb.z, pa.z)};
+    const float dist2 = dot3c(d, d);
+    if (dist2 > t2 || dist2 < 1e-18f) return false;
+    const float4 ra = rest[a], rb = rest[b];
+    const F3c rd = {__fsub_rn(rb.x, ra.x), __fsub_rn(rb.y, ra.y), __fsub_rn(rb.z, ra.z)};
+    const float rest2 = dot3c(rd, rd);
+    if (filter == 1u) {
+        if (dist2 > rest2) return false;
+    } else if (ring_contains(B.ring_off, B.ring_idx, a, b)) {
+        return false;
+    }
+    float min_d = thickness;
+    if (rest2 < t2) min_d = __fsqrt_rn(rest2);
+    const float dist = __fsqrt_rn(dist2);
+    const float corr = __fmul_rn(__fmul_rn(__fsub_rn(min_d, dist), 0.5f), coll_scale);
+    if (corr <= 0.0f) return false;
+    d = {__fmul_rn(__fdiv_rn(d.x, dist), corr), __fmul_rn(__fdiv_rn(d.y, dist), corr),
+         __fmul_rn(__fdiv_rn(d.z, dist), corr)};
+    const float inv_w = __fdiv_rn(1.0f, fmaxf(__fadd_rn(w_a, w_b), 1e-8f));
+    if (self == a)
+        out = {__fmul_rn(__fmul_rn(-d.x, w_a), inv_w), __fmul_rn(__fmul_rn(-d.y, w_a), inv_w),
+               __fmul_rn(__fmul_rn(-d.z, w_a), inv_w)};
+    else
+        out = {__fmul_rn(__fmul_rn(d.x, w_b), inv_w), __fmul_rn(__fmul_rn(d.y, w_b), inv_w),
+               __fmul_rn(__fmul_rn(d.z, w_b), inv_w)};
+    return true;
+}
+
+// Visits every particle j != i in the (deduplicated) buckets of the 27 cells around i's cell.
+template <typename F>
+__device__ __forceinline__ void for_each_candidate(const float4* __restrict__ src, const CollisionBuffers& B,
+                                                   uint32_t n, uint32_t i, float inv_cell, F&& f) {
+    const uint32_t mask = (B.table_bits >= 32) ? 0xFFFFFFFFu : ((1u << B.table_bits) - 1u);
+    const int3 c = cell_of(src[i], inv_cell);
+    uint32_t seen[27];
+    int nseen = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const uint32_t h = hash_cell(make_int3(c.x + dx, c.y + dy, c.z + dz), mask);
+                bool dup = false;
+                for (int q = 0; q < nseen; ++q) dup |= (seen[q] == h);
+                if (dup) continue;
+                seen[nseen++] = h;
+                const uint32_t s = B.table_start[h];
+                if (s >= n || B.keys_sorted[s] != h || (s > 0 && B.keys_sorted[s - 1] == h)) continue;
+                for (uint32_t q = s; q < n && B.keys_sorted[q] == h; ++q) {
+                    const uint32_t j = B.vals_sorted[q];
+                    if (j != i) f(j);
+                }
+            }
+}
+
+constexpr int kPartnerCap = 24;
+
+// Accepted partners of i with index in (lo, ∞), the kPartnerCap smallest, sorted. Returns true if more remain.
+template <bool ONLY_GREATER>
+__device__ __forceinline__ bool collect_partners(const float4* __restrict__ src, const float4* __restrict__ rest,
+                                                 const CollisionBuffers& B, uint32_t n, uint32_t i, float inv_cell,
+                                                 uint32_t filter, float thickness, float coll_scale, long long lo,
+                                                 uint32_t* pj, F3c* pc, int& cnt) {
+    cnt = 0;
+    bool overflow = false;
+    for_each_candidate(src, B, n, i, inv_cell, [&](uint32_t j) {
+        if ((long long)j <= lo) return;
+        if (ONLY_GREATER && j < i) return;
+        if (cnt == kPartnerCap && j > pj[kPartnerCap - 1]) {
+            // cheap reject before the narrow test; it may be accepted, so remember that more partners remain
+            F3c tmp;
+            const uint32_t a = min(i, j), b = max(i, j);
+            if (narrow_pair(src, rest, B, filter, thickness, coll_scale, a, b, i, tmp)) overflow = true;
+            return;
+        }
+        F3c corr;
+        const uint32_t a = min(i, j), b = max(i, j);
+        if (!narrow_pair(src, rest, B, filter, thickness, coll_scale, a, b, i, corr)) return;
+        if (cnt == kPartnerCap) overflow = true;  // evicts the largest
+        int p = (cnt < kPartnerCap) ? cnt++ : kPartnerCap - 1;
+        while (p > 0 && pj[p - 1] > j) {
+            pj[p] = pj[p - 1];
+            pc[p] = pc[p - 1];
+            --p;
+        }
+        pj[p] = j;
+        pc[p] = corr;
+    });
+    return overflow;
+}
+
+// collide: dst[i] = src[i] + clamp(Σ_j corr_ij) with partners in increasing index (xpbd_cpu.rs:82-136).
+__global__ void __launch_bounds__(128) collision_resolve_kernel(XpbdWorld W, const float4* __restrict__ src,
+                                                                float4* __restrict__ dst, CollisionBuffers B,
+                                                                float inv_cell, uint32_t filter) {
+    const XpbdDevParams& P = *W.params;
+    const float thickness = P.thickness, coll_scale = P.coll_scale;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < W.n; p += gridDim.x * blockDim.x) {
+        const uint32_t i = B.vals_sorted[p];  // sorted order: neighbouring threads query neighbouring cells
+        const float4 pi = src[i];
+        if (pi.w <= 0.0f) {
+            dst[i] = pi;
+            continue;
+        }
+        uint32_t pj[kPartnerCap];
+        F3c pc[kPartnerCap];
+        F3c acc = {0.0f, 0.0f, 0.0f};
+        long long lo = -1;
+        for (int round = 0; round < 1 << 16; ++round) {
+            int cnt = 0;
+            const bool more = collect_partners<false>(src, W.rest, B, W.n, i, inv_cell, filter, thickness,
+                                                      coll_scale, lo, pj, pc, cnt);
+            for (int q = 0; q < cnt; ++q) {
+                acc.x = __fadd_rn(acc.x, pc[q].x);
+                acc.y = __fadd_rn(acc.y, pc[q].y);
+                acc.z = __fadd_rn(acc.z, pc[q].z);
+            }
+            if (!more || cnt == 0) break;
+            lo = pj[cnt - 1];
+        }
+        const float m = kCollisionApplyClamp;
+        const float cx = fminf(fmaxf(acc.x, -m), m), cy = fminf(fmaxf(acc.y, -m), m), cz = fminf(fmaxf(acc.z, -m), m);
+        dst[i] = make_float4(__fadd_rn(pi.x, cx), __fadd_rn(pi.y, cy), __fadd_rn(pi.z, cz), pi.w);
+    }
+}
+
+cudaError_t collision_resolve(const XpbdWorld& W, const float4* src, float4* dst, const CollisionBuffers& B,
+                              float inv_cell, uint32_t filter, int sms, cudaStream_t st, uint64_t* launches) {
+    uint32_t grid = (W.n + 127) / 128;
+    if (grid > (uint32_t)sms * 16) grid = (uint32_t)sms * 16;
+    if (grid == 0) grid = 1;
+    collision_resolve_kernel<<<grid, 128, 0, st>>>(W, src, dst, B, inv_cell, filter);
+    if (launches) *launches += 1;
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------- pair list
+__global__ void pair_count_kernel(XpbdWorld W, const float4* __restrict__ src, CollisionBuffers B, float inv_cell,
+                                  uint32_t filter, uint32_t* __restrict__ counts) {
+    const XpbdDevParams& P = *W.params;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n; i += gridDim.x * blockDim.x) {
+        uint32_t c = 0;
+        for_each_candidate(src, B, W.n, i, inv_cell, [&](uint32_t j) {
+            if (j < i) return;
+            F3c tmp;
+            if (narrow_pair(src, W.rest, B, filter, P.thickness, P.coll_scale, i, j, i, tmp)) ++c;
+        });
+        counts[i] = c;
+    }
+}
+
+__global__ void pair_write_kernel(XpbdWorld W, const float4* __restrict__ src, CollisionBuffers B, float inv_cell,
+                                  uint32_t filter, const uint32_t* __restrict__ offsets, uint32_t* __restrict__ out,
+                                  unsigned long long cap) {
+    const XpbdDevParams& P = *W.params;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n; i += gridDim.x * blockDim.x) {
+        uint32_t pj[kPartnerCap];
+        F3c pc[kPartnerCap];
+        unsigned long long o = offsets[i];
+        long long lo = -1;
+        for (int round = 0; round < 1 << 16; ++round) {
+            int cnt = 0;
+            const bool more = collect_partners<true>(src, W.rest, B, W.n, i, inv_cell, filter, P.thickness,
+                                                     P.coll_scale, lo, pj, pc, cnt);
+            for (int q = 0; q < cnt; ++q, ++o)
+                if (o < cap) {
+                    out[2 * o] = i;
+                    out[2 * o + 1] = pj[q];
+                }
+            if (!more || cnt == 0) break;
+            lo = pj[cnt - 1];
+        }
+    }
+}
+
+cudaError_t collision_pairs(const XpbdWorld& W, const float4* pos, const CollisionBuffers& B, float inv_cell,
+                            uint32_t filter, uint32_t* pairs_out, uint64_t cap, uint64_t* total, int sms,
+                            cudaStream_t st) {
+    uint32_t grid = (W.n + 127) / 128;
+    if (grid > (uint32_t)sms * 16) grid = (uint32_t)sms * 16;
+    if (grid == 0) grid = 1;
+    pair_count_kernel<<<grid, 128, 0, st>>>(W, pos, B, inv_cell, filter, B.pair_count);
+    cudaError_t e = cudaMemsetAsync(B.pair_count + W.n, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    exclusive_scan_kernel<<<1, 1024, 0, st>>>(B.pair_count, W.n + 1, nullptr);
+    uint32_t h_total = 0;
+    e = cudaMemcpyAsync(&h_total, B.pair_count + W.n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    *total = h_total;
+    if (pairs_out && cap > 0) pair_write_kernel<<<grid, 128, 0, st>>>(W, pos, B, inv_cell, filter, B.pair_count,
+                                                                      pairs_out, cap);
+    return cudaGetLastError();
+}
+
+}  // namespace xpbd

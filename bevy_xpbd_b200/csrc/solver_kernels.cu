@@ -1,0 +1,513 @@
+// XPBD substep kernels for sm_100a: predict/integrate, Jacobi and colored Gauss–Seidel distance-constraint solves,
+// post-velocity, strain residual.
+//
+// Arithmetic follows the reference CPU solver src/xpbd_cpu.rs operation by operation with correctly rounded IEEE
+// single-precision intrinsics (__fadd_rn/__fmul_rn/__fdiv_rn/__fsqrt_rn never contract into FMA), so the CUDA path
+// reproduces the FP32 reference bit for bit:
+//   predict_particle          xpbd_cpu.rs:38-65     (WGSL predict_copy_sim_to_jac, cloth_sim_jacobi.wgsl:85-121)
+//   jacobi_edges_pass         xpbd_cpu.rs:139-184   (WGSL jacobi_edges :143-180)
+//   jacobi_gather_particle    xpbd_cpu.rs:186-226   (WGSL jacobi_gather :182-218)
+//   Gauss–Seidel sweep        xpbd_cpu.rs:344-386   (WGSL gs_edges, cloth_sim.wgsl:154-210)
+//   post_velocity             xpbd_cpu.rs:393-409   (WGSL post_velocity :220-233)
+//
+// B200 design. One persistent kernel runs whole substeps: a grid-stride predict phase, then the inner iterations
+// separated by a bounded grid barrier (no launch per iteration, no per-iteration λ clear launch). The Jacobi edge
+// and gather passes are fused: each warp owns a tile of up to 32 consecutive particles; its lanes stride over the
+// tile's incidences (coalesced 8-byte records), each lane computing one incidence's Δλ and correction, and the
+// corrections are then summed per particle in the reference's neighbour order from shared memory — a deterministic
+// warp-level segmented reduction without atomics. Finalize (velocity update) and the next substep's predict are
+// fused into the last iteration, so a frame of S substeps × I iterations needs S·I grid barriers.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "xpbd_internal.h"
+#include "xpbd_kernels.h"
+
+namespace xpbd {
+
+constexpr float kCorrectionCap = 0.28f;  // JACOBI_CORRECTION_CAP, cloth_compute.rs:82
+constexpr float kMaxSpeed = 12.0f;       // PREDICT_MAX_SPEED, cloth_compute.rs:84
+constexpr float kGrabMaxPull = 0.065f;   // GRAB_MAX_PULL_PER_SUBSTEP, cloth_compute.rs:86
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+struct F3 {
+    float x, y, z;
+};
+__device__ __forceinline__ F3 f3(float4 a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ F3 add3(F3 a, F3 b) { return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)}; }
+__device__ __forceinline__ F3 sub3(F3 a, F3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ F3 mul3(F3 a, float s) { return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)}; }
+__device__ __forceinline__ F3 div3(F3 a, float s) { return {__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s)}; }
+__device__ __forceinline__ F3 neg3(F3 a) { return {-a.x, -a.y, -a.z}; }
+// glam dot: (x*x' + y*y') + z*z'; length = sqrt(dot)
+__device__ __forceinline__ float dot3(F3 a, F3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ float len3(F3 a) { return __fsqrt_rn(dot3(a, a)); }
+__device__ __forceinline__ bool finite3(F3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+
+__device__ __forceinline__ void set_status(int* status, int flag) {
+    if ((*(volatile int*)status & flag) == 0) atomicOr(status, flag);
+}
+
+// clamp_correction, xpbd_cpu.rs:28-36
+__device__ __forceinline__ F3 clamp_correction(F3 dx) {
+    float ml = len3(dx);
+    if (ml > kCorrectionCap && ml > 0.0f) return mul3(dx, __fdiv_rn(kCorrectionCap, ml));
+    return dx;
+}
+
+// predict_particle, xpbd_cpu.rs:38-65 (callers handle inv_mass <= 0)
+__device__ __forceinline__ F3 predict_particle(uint32_t i, F3 sim, F3& vel, const XpbdDevParams& P) {
+    F3 g = {P.gravity[0], P.gravity[1], P.gravity[2]};
+    F3 v = add3(vel, mul3(g, P.dt));
+    float speed = len3(v);
+    if (speed > kMaxSpeed && speed > 0.0f) v = mul3(v, __fdiv_rn(kMaxSpeed, speed));
+    F3 pos = add3(sim, mul3(v, P.dt));
+    if (P.grab_active != 0u && (int32_t)i == P.grab_idx) {
+        F3 tgt = {P.grab_target[0], P.grab_target[1], P.grab_target[2]};
+        F3 pull = mul3(sub3(tgt, pos), P.grab_stiffness);
+        float pl = len3(pull);
+        if (pl > kGrabMaxPull && pl > 0.0f) pull = mul3(pull, __fdiv_rn(kGrabMaxPull, pl));
+        pos = add3(pos, pull);
+    }
+    vel = v;
+    return pos;
+}
+
+// xpbd_substep_post_velocity, xpbd_cpu.rs:393-409, for an unpinned particle: ground plane (extension), then
+// v = ((x - prev) * inv_dt) * exp(-k dt). Returns the (possibly clamped) new position.
+__device__ __forceinline__ F3 finalize_particle(F3 xn, F3 xo, F3& vel, const XpbdDevParams& P, int* status) {
+    if (P.ground_enabled != 0u && xn.y < P.ground_y) xn.y = P.ground_y;
+    vel = mul3(mul3(sub3(xn, xo), P.inv_dt), P.damp);
+    if (!finite3(xn) || !finite3(vel)) set_status(status, XPBD_DEV_NONFINITE);
+    return xn;
+}
+
+// ---------------------------------------------------------------------------------------------- grid barrier
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// All blocks of the grid meet here. Waits are bounded: after `barrier_timeout_ns` (or if another block already
+// reported an error) the waiting block records XPBD_DEV_BARRIER_TIMEOUT and every caller returns false, so a
+// launch that can never complete (blocks not co-resident, forced test timeout) ends instead of hanging.
+__device__ bool grid_barrier(const XpbdWorld& W, const XpbdDevParams& P) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        XpbdGridSync* gs = W.sync;
+        unsigned expected = gridDim.x + gs->expected_extra;
+        unsigned g = ld_acquire(&gs->gen);
+        __threadfence();
+        unsigned arrived = atomicAdd(&gs->count, 1u);
+        if (arrived == expected - 1) {
+            atomicExch(&gs->count, 0u);
+            __threadfence();
+            st_release(&gs->gen, g + 1);
+        } else {
+            unsigned long long t0 = global_ns();
+            unsigned spins = 0;
+            while (ld_acquire(&gs->gen) == g) {
+                ++spins;
+                if (spins > 32) __nanosleep(spins > 4096 ? 256 : 32);
+                if ((spins & 63) == 0) {
+                    if (*(volatile int*)W.status != 0) { ok = 0; break; }
+                    if (global_ns() - t0 > P.barrier_timeout_ns || spins > (1u << 30)) {
+                        set_status(W.status, XPBD_DEV_BARRIER_TIMEOUT);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__device__ __forceinline__ bool status_clear(const XpbdWorld& W) { return *(volatile int*)W.status == 0; }
+
+// ---------------------------------------------------------------------------------------------- predict phase
+// Grid-stride over particles. Optionally finalizes a pending substep (positions in jac[pend]) first, then predicts
+// into jac[start]. Pinned particles are written to both ping-pong buffers (they never move).
+__device__ void predict_phase(const XpbdWorld& W, const XpbdDevParams& P, bool finalize_pending, uint32_t pend,
+                              uint32_t start, bool predict) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n; i += stride) {
+        float4 xo4 = W.x[i];
+        F3 xo = f3(xo4);
+        const float w = xo4.w;
+        if (w <= 0.0f) {
+            if (predict) {
+                W.jac[0][i] = xo4;
+                W.jac[1][i] = xo4;
+            }
+            continue;
+        }
+        float4 vo4 = W.v[i];
+        F3 vel = f3(vo4);
+        if (finalize_pending) {
+            F3 xn = finalize_particle(f3(W.jac[pend][i]), xo, vel, P, W.status);
+            W.x[i] = make_float4(xn.x, xn.y, xn.z, w);
+            W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+            xo = xn;
+        }
+        if (predict) {
+            F3 pos = predict_particle(i, xo, vel, P);
+            W.jac[start][i] = make_float4(pos.x, pos.y, pos.z, w);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------- Jacobi tile
+enum TailMode : uint32_t { kTailNone = 0, kTailFinalize = 1, kTailFinalizePredict = 2 };
+
+// One Jacobi iteration for one warp tile (jacobi_edges + jacobi_gather fused). `sc` is the warp's 96-float
+// shared staging area. Contributions of incidence k: the reference's Δλ for its constraint (recomputed
+// identically from either endpoint) times n̂·w_self, summed per particle in neighbour-table order.
+__device__ __forceinline__ void jacobi_tile(const XpbdWorld& W, const XpbdDevParams& P, uint32_t tile,
+                                            const float4* __restrict__ jin, float4* __restrict__ jout, float* sc,
+                                            uint32_t lane, TailMode tail) {
+    const XpbdTile t = W.tiles[tile];
+    const uint32_t cnt = t.count;
+    const bool has_row = lane < cnt;
+    const uint32_t r = t.first + lane;
+    uint32_t rs = 0, re = 0;
+    float4 ps = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (has_row) {
+        rs = W.row_off[r];
+        re = W.row_off[r + 1];
+        ps = jin[r];
+    }
+    const uint32_t I0 = __shfl_sync(kFull, rs, 0);
+    const uint32_t I1 = __shfl_sync(kFull, re, cnt - 1);
+    const float* pal = W.palette_comp + (uint32_t)t.cloth * XPBD_PALETTE;
+    const bool persist = P.lambda_mode != 0u;
+    F3 acc = {0.0f, 0.0f, 0.0f};
+    for (uint32_t cb = I0; cb < I1; cb += 32) {
+        const uint32_t k = cb + lane;
+        // owner row of incidence k: smallest rr with row_end[rr] > k (binary search over the lanes' row ends)
+        uint32_t lo = 0, hi = cnt;
+#pragma unroll
+        for (int it = 0; it < 6; ++it) {
+            uint32_t mid = (lo + hi) >> 1;
+            uint32_t em = __shfl_sync(kFull, re, mid & 31u);
+            if (lo < hi) {
+                if (em > k) hi = mid; else lo = mid + 1;
+            }
+        }
+        const uint32_t rr = lo & 31u;
+        const float sx = __shfl_sync(kFull, ps.x, rr);
+        const float sy = __shfl_sync(kFull, ps.y, rr);
+        const float sz = __shfl_sync(kFull, ps.z, rr);
+        const float sw = __shfl_sync(kFull, ps.w, rr);
+        F3 c = {0.0f, 0.0f, 0.0f};
+        if (k < I1) {
+            const uint2 rec = W.inc[k];
+            const uint32_t other = rec.x & XPBD_OTHER_MASK;
+            const float rest = __uint_as_float(rec.y);
+            const float4 po = jin[other];
+            const F3 gv = sub3(F3{sx, sy, sz}, f3(po));
+            const float len = len3(gv);
+            if (!(len < 1e-8f)) {
+                const F3 nrm = div3(gv, len);
+                const float C = __fsub_rn(len, rest);
+                const float alpha_t = __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq);
+                const float wsum = __fadd_rn(__fadd_rn(sw, po.w), alpha_t);
+                float dlam = 0.0f;
+                if (!(wsum < 1e-8f)) {
+                    const float lam = persist ? W.inc_lambda[k] : 0.0f;
+                    dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
+                    if (persist) W.inc_lambda[k] = (tail == kTailFinalizePredict) ? 0.0f : __fadd_rn(lam, dlam);
+                } else if (persist && tail == kTailFinalizePredict) {
+                    W.inc_lambda[k] = 0.0f;
+                }
+                c = mul3(mul3(nrm, sw), dlam);
+            } else if (persist && tail == kTailFinalizePredict) {
+                W.inc_lambda[k] = 0.0f;
+            }
+        }
+        sc[lane] = c.x;
+        sc[32 + lane] = c.y;
+        sc[64 + lane] = c.z;
+        __syncwarp();
+        if (has_row) {
+            const uint32_t a = rs > cb ? rs : cb;
+            const uint32_t b = re < cb + 32 ? re : cb + 32;
+            for (uint32_t q = a; q < b; ++q) {
+                const uint32_t s = q - cb;
+                acc.x = __fadd_rn(acc.x, sc[s]);
+                acc.y = __fadd_rn(acc.y, sc[32 + s]);
+                acc.z = __fadd_rn(acc.z, sc[64 + s]);
+            }
+        }
+        __syncwarp();
+    }
+    if (!has_row || ps.w <= 0.0f) return;  // pinned: both buffers already hold the fixed position
+    F3 delta = {__fmul_rn(P.omega, acc.x), __fmul_rn(P.omega, acc.y), __fmul_rn(P.omega, acc.z)};
+    if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
+    delta = clamp_correction(delta);
+    F3 xn = add3(f3(ps), delta);
+    if (tail == kTailNone) {
+        jout[r] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        return;
+    }
+    // fused post_velocity (+ next substep's predict)
+    const F3 xo = f3(W.x[r]);
+    F3 vel = f3(W.v[r]);
+    xn = finalize_particle(xn, xo, vel, P, W.status);
+    W.x[r] = make_float4(xn.x, xn.y, xn.z, ps.w);
+    W.v[r] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+    if (tail == kTailFinalizePredict) {
+        F3 pos = predict_particle(r, xn, vel, P);
+        jout[r] = make_float4(pos.x, pos.y, pos.z, ps.w);
+    } else {
+        jout[r] = make_float4(xn.x, xn.y, xn.z, ps.w);
+    }
+}
+
+// Persistent Jacobi kernel: `substeps` substeps of the whole batch.
+//   flags & kBeginFinalize : a previous substep's result waits in jac[pend] (e.g. after collision) — finalize it
+//   flags & kEndFinalize   : finalize the last substep in place; otherwise its result stays in jac[final]
+// The predict of the first substep writes jac[start]; iteration k of a substep reads buffer (b+k)&1.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) jacobi_persistent_kernel(XpbdWorld W, uint32_t flags, uint32_t substeps,
+                                                                  uint32_t pend, uint32_t start) {
+    __shared__ float s_contrib[BLOCK / 32][96];
+    if (!status_clear(W)) return;
+    const XpbdDevParams P = *W.params;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t gwarp = blockIdx.x * (BLOCK / 32) + warp;
+    const uint32_t nwarps = gridDim.x * (BLOCK / 32);
+    float* sc = s_contrib[warp];
+    const bool persist = P.lambda_mode != 0u;
+
+    predict_phase(W, P, (flags & kBeginFinalize) != 0u, pend, start, true);
+    if (persist) {
+        const uint32_t stride = gridDim.x * blockDim.x;
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < W.n_inc; k += stride) W.inc_lambda[k] = 0.0f;
+    }
+    if (!grid_barrier(W, P)) return;
+    uint32_t b = start;
+    const uint32_t I = P.iterations;
+    for (uint32_t s = 0; s < substeps; ++s) {
+        const bool last_sub = (s + 1 == substeps);
+        if (I == 0) {  // no constraint iterations: the predicted positions are the result (xpbd_cpu.rs:302-309)
+            // finalize / re-predict per particle without reading neighbours
+            const uint32_t stride = gridDim.x * blockDim.x;
+            const bool fin = !last_sub || (flags & kEndFinalize);
+            for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n && fin; i += stride) {
+                float4 p4 = W.jac[b][i];
+                if (p4.w <= 0.0f) continue;
+                const F3 xo = f3(W.x[i]);
+                F3 vel = f3(W.v[i]);
+                F3 xn = finalize_particle(f3(p4), xo, vel, P, W.status);
+                W.x[i] = make_float4(xn.x, xn.y, xn.z, p4.w);
+                W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+                if (!last_sub) {
+                    F3 pos = predict_particle(i, xn, vel, P);
+                    W.jac[b][i] = make_float4(pos.x, pos.y, pos.z, p4.w);
+                }
+            }
+            if (!last_sub && !grid_barrier(W, P)) return;
+            continue;
+        }
+        for (uint32_t k = 0; k < I; ++k) {
+            const float4* jin = W.jac[(b + k) & 1u];
+            float4* jout = W.jac[(b + k + 1) & 1u];
+            TailMode tail = kTailNone;
+            if (k + 1 == I) {
+                if (!last_sub) tail = kTailFinalizePredict;
+                else if (flags & kEndFinalize) tail = kTailFinalize;
+            }
+            for (uint32_t tile = gwarp; tile < W.n_tiles; tile += nwarps) jacobi_tile(W, P, tile, jin, jout, sc, lane, tail);
+            const bool very_last = last_sub && (k + 1 == I);
+            if (!very_last && !grid_barrier(W, P)) return;
+        }
+        b = (b + I) & 1u;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------- Gauss–Seidel
+// One constraint of the colored sweep, xpbd_cpu.rs:349-385, in place on the working state.
+__device__ __forceinline__ void gs_constraint(const XpbdWorld& W, const XpbdDevParams& P, uint32_t e, float4* jw,
+                                              bool persist) {
+    const uint4 c = W.con[e];
+    const uint32_t i = c.x, j = c.y;
+    const float4 pi4 = jw[i];
+    const float4 pj4 = jw[j];
+    const float w_i = pi4.w, w_j = pj4.w;
+    if (w_j <= 0.0f && w_i <= 0.0f) return;
+    const F3 p_i = f3(pi4), p_j = f3(pj4);
+    F3 gv = sub3(p_i, p_j);
+    const float len = len3(gv);
+    if (len < 1e-8f) return;
+    gv = div3(gv, len);
+    const float C = __fsub_rn(len, __uint_as_float(c.z));
+    const float alpha_t = __fmul_rn(__uint_as_float(c.w), P.inv_dt_sq);
+    const float wsum = __fadd_rn(__fadd_rn(w_i, w_j), alpha_t);
+    if (wsum < 1e-8f) return;
+    const float lam = persist ? W.con_lambda[e] : 0.0f;
+    const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
+    if (persist) W.con_lambda[e] = __fadd_rn(lam, dlam);
+    const F3 og = {__fmul_rn(P.omega, gv.x), __fmul_rn(P.omega, gv.y), __fmul_rn(P.omega, gv.z)};
+    const F3 dx_i = clamp_correction(mul3(mul3(og, w_i), dlam));
+    const F3 dx_j = clamp_correction(neg3(mul3(mul3(og, w_j), dlam)));
+    if (w_i > 0.0f) {
+        const F3 n = add3(p_i, dx_i);
+        jw[i] = make_float4(n.x, n.y, n.z, w_i);
+    }
+    if (w_j > 0.0f) {
+        const F3 n = add3(p_j, dx_j);
+        jw[j] = make_float4(n.x, n.y, n.z, w_j);
+    }
+}
+
+// Persistent colored Gauss–Seidel: per inner iteration one sweep over the color batches, a grid barrier after each
+// color (colors are particle-disjoint, so a color's constraints run in parallel with the reference's result).
+// The working state is jac[0]; with kBeginFinalize the first substep finalizes positions waiting in jac[pend].
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) gs_persistent_kernel(XpbdWorld W, uint32_t flags, uint32_t substeps,
+                                                              uint32_t pend) {
+    if (!status_clear(W)) return;
+    const XpbdDevParams P = *W.params;
+    const bool persist = P.lambda_mode != 0u;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gstride = gridDim.x * blockDim.x;
+    float4* jw = W.jac[0];
+    bool pending = (flags & kBeginFinalize) != 0u;
+    for (uint32_t s = 0; s < substeps; ++s) {
+        predict_phase(W, P, pending, s == 0 ? pend : 0u, 0, true);
+        if (persist)
+            for (uint32_t e = gtid; e < W.e; e += gstride) W.con_lambda[e] = 0.0f;
+        if (!grid_barrier(W, P)) return;
+        for (uint32_t k = 0; k < P.iterations; ++k)
+            for (uint32_t c = 0; c < W.n_colors; ++c) {
+                const uint32_t e0 = W.color_off[c], e1 = W.color_off[c + 1];
+                for (uint32_t e = e0 + gtid; e < e1; e += gstride) gs_constraint(W, P, e, jw, persist);
+                if (!grid_barrier(W, P)) return;
+            }
+        pending = true;
+    }
+    if (flags & kEndFinalize) predict_phase(W, P, true, 0, 0, false);
+}
+
+// Standalone finalize of positions waiting in jac[pend] (after a collision pass on the last substep).
+__global__ void finalize_kernel(XpbdWorld W, uint32_t pend) {
+    const XpbdDevParams P = *W.params;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n; i += stride) {
+        float4 p4 = W.jac[pend][i];
+        if (p4.w <= 0.0f) continue;
+        const F3 xo = f3(W.x[i]);
+        F3 vel = f3(W.v[i]);
+        F3 xn = finalize_particle(f3(p4), xo, vel, P, W.status);
+        W.x[i] = make_float4(xn.x, xn.y, xn.z, p4.w);
+        W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+    }
+}
+
+// Max strain residual over constraints [e0, e1) of the input-order table (non-negative floats compare as ints).
+__global__ void strain_residual_kernel(XpbdWorld W, uint32_t e0, uint32_t e1, unsigned* out_bits) {
+    float m = 0.0f;
+    for (uint32_t e = e0 + blockIdx.x * blockDim.x + threadIdx.x; e < e1; e += gridDim.x * blockDim.x) {
+        const uint4 c = W.con_in[e];
+        const float len = len3(sub3(f3(W.x[c.x]), f3(W.x[c.y])));
+        const float rest = __uint_as_float(c.z);
+        const float s = fabsf(__fsub_rn(len, rest)) / rest;
+        m = fmaxf(m, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(kFull, m, o));
+    if ((threadIdx.x & 31u) == 0) atomicMax(out_bits, __float_as_uint(m));
+}
+
+// ---------------------------------------------------------------------------------------------- host launchers
+template <int BLOCK>
+static const void* jacobi_fn() { return (const void*)jacobi_persistent_kernel<BLOCK>; }
+template <int BLOCK>
+static const void* gs_fn() { return (const void*)gs_persistent_kernel<BLOCK>; }
+
+const void* solver_kernel_fn(uint32_t solver, uint32_t block) {
+    if (solver == 0) {
+        switch (block) {
+            case 128: return jacobi_fn<128>();
+            case 256: return jacobi_fn<256>();
+            case 512: return jacobi_fn<512>();
+            case 1024: return jacobi_fn<1024>();
+        }
+    } else {
+        switch (block) {
+            case 128: return gs_fn<128>();
+            case 256: return gs_fn<256>();
+            case 512: return gs_fn<512>();
+            case 1024: return gs_fn<1024>();
+        }
+    }
+    return nullptr;
+}
+
+cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool cooperative, const XpbdWorld& W,
+                          uint32_t flags, uint32_t substeps, uint32_t pend, uint32_t start, cudaStream_t st) {
+    const void* fn = solver_kernel_fn(solver, block);
+    if (!fn) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    if (cooperative) {
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    XpbdWorld w = W;
+    if (solver == 0) {
+        void* args[] = {&w, &flags, &substeps, &pend, &start};
+        return cudaLaunchKernelExC(&cfg, fn, args);
+    }
+    void* args[] = {&w, &flags, &substeps, &pend};
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+int max_blocks_per_sm(uint32_t solver, uint32_t block) {
+    const void* fn = solver_kernel_fn(solver, block);
+    int nb = 0;
+    if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, (int)block, 0) != cudaSuccess) return 0;
+    return nb;
+}
+
+cudaError_t launch_finalize(const XpbdWorld& W, uint32_t pend, int sms, cudaStream_t st) {
+    uint32_t grid = (W.n + 255) / 256;
+    if (grid > (uint32_t)sms * 8) grid = (uint32_t)sms * 8;
+    if (grid == 0) grid = 1;
+    finalize_kernel<<<grid, 256, 0, st>>>(W, pend);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_strain_residual(const XpbdWorld& W, uint32_t e0, uint32_t e1, unsigned* out_bits, int sms,
+                                   cudaStream_t st) {
+    uint32_t n = e1 - e0;
+    uint32_t grid = (n + 255) / 256;
+    if (grid > (uint32_t)sms * 4) grid = (uint32_t)sms * 4;
+    if (grid == 0) grid = 1;
+    strain_residual_kernel<<<grid, 256, 0, st>>>(W, e0, e1, out_bits);
+    return cudaGetLastError();
+}
+
+}  // namespace xpbd

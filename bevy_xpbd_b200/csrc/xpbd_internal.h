@@ -1,0 +1,74 @@
+// Internal layout of the packed cloth batch in HBM, shared by the host runtime and the sm_100a kernels.
+//
+// All cloths of a context are packed back to back (vertex offsets, constraint offsets). Vertex state is float4
+// per particle with w = inverse mass, so a neighbour gather brings position and mass in one 16-byte load:
+//   x      sim positions            (reference sim_pos, vec4 w=0 in cloth_sim_jacobi.wgsl:27)
+//   v      velocities               (w unused)
+//   jac[2] Jacobi ping-pong buffers (reference jac_a / jac_b); jac[0] is the Gauss–Seidel working state
+//   rest   rest positions           (collision rest filter)
+// Jacobi neighbour table (CSR over particles, rows of pinned particles left empty):
+//   row_off[n+1], inc[n_inc] = {other | palette<<28, rest bits}: 8 bytes per incidence. The compliance of an
+//   incidence is palette_comp[cloth*16 + palette] (at most 16 distinct compliance values per cloth).
+//   tiles[]: warp tiles of up to 32 consecutive particles of one cloth {first particle, count, cloth}.
+// Gauss–Seidel constraints, color-major over the whole batch: con[e] = {i, j, rest bits, compliance bits},
+//   color_off[ncolors+1]; λ per constraint in con_lambda.
+#pragma once
+#include <stdint.h>
+#include <vector_types.h>
+
+#define XPBD_PALETTE 16
+#define XPBD_OTHER_MASK 0x0FFFFFFFu
+#define XPBD_MAX_PARTICLES (1u << 28)
+
+// Device status word values (mirror the negative XPBD_ERR_* codes as positive flags).
+#define XPBD_DEV_NONFINITE 1
+#define XPBD_DEV_BARRIER_TIMEOUT 2
+#define XPBD_DEV_CAPACITY 4
+#define XPBD_DEV_INDEX 8
+
+struct XpbdDevParams {  // the per-call uniform block (ClothSimParamsGpu, cloth_compute.rs:245-273, + extensions)
+    float dt, inv_dt, inv_dt_sq, omega;
+    uint32_t iterations, relaxation, lambda_mode, solver;
+    float gravity[3];
+    float damp;  // exp(-linear_drag_per_sec * dt), evaluated on the host
+    int32_t grab_idx;
+    uint32_t grab_active;
+    float grab_stiffness;
+    float grab_target[3];
+    float thickness, coll_scale, inv_cell, ground_y;
+    uint32_t ground_enabled, collision, table_bits, warm_start;
+    unsigned long long barrier_timeout_ns;
+};
+
+struct XpbdGridSync {
+    unsigned int count;
+    unsigned int gen;
+    unsigned int expected_extra;  // test hook: blocks the barrier expects beyond the grid (0 in normal runs)
+    unsigned int pad;
+};
+
+struct XpbdTile {
+    uint32_t first;  // first particle
+    uint16_t count;  // particles in this tile (1..32)
+    uint16_t cloth;  // cloth index (palette row)
+};
+
+struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
+    uint32_t n, e, n_inc, n_tiles, n_colors, n_cloths;
+    float4* x;
+    float4* v;
+    float4* jac[2];
+    float4* rest;
+    const uint32_t* row_off;
+    const uint2* inc;
+    float* inc_lambda;
+    const XpbdTile* tiles;
+    const float* palette_comp;
+    const uint4* con;
+    float* con_lambda;
+    const uint32_t* color_off;
+    const uint4* con_in;            // constraints in input order, cloths contiguous (residual)
+    const XpbdDevParams* params;
+    int* status;
+    XpbdGridSync* sync;
+};

@@ -1,0 +1,53 @@
+// Host-side launchers of the sm_100a kernels (solver_kernels.cu, collision_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "xpbd_internal.h"
+
+namespace xpbd {
+
+constexpr uint32_t kBeginFinalize = 1u;  // finalize positions waiting in jac[pend] before predicting
+constexpr uint32_t kEndFinalize = 2u;    // finalize the launch's last substep in place
+
+// ---- solver (solver_kernels.cu)
+const void* solver_kernel_fn(uint32_t solver, uint32_t block);
+int max_blocks_per_sm(uint32_t solver, uint32_t block);
+cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool cooperative, const XpbdWorld& W,
+                          uint32_t flags, uint32_t substeps, uint32_t pend, uint32_t start, cudaStream_t st);
+cudaError_t launch_finalize(const XpbdWorld& W, uint32_t pend, int sms, cudaStream_t st);
+cudaError_t launch_strain_residual(const XpbdWorld& W, uint32_t e0, uint32_t e1, unsigned* out_bits, int sms,
+                                   cudaStream_t st);
+
+// ---- collision (collision_kernels.cu)
+struct CollisionBuffers {
+    uint32_t* keys;         // n
+    uint32_t* vals;         // n
+    uint32_t* keys_sorted;  // n
+    uint32_t* vals_sorted;  // n
+    uint32_t* table_start;  // 2^bits bucket -> first sorted position (validated on use, never cleared)
+    uint32_t* pair_count;   // n + 1 (pair extraction only)
+    void* sort_scratch;
+    size_t sort_scratch_bytes;
+    uint32_t table_bits;
+    const uint32_t* ring_off;  // n + 1 (ring filter)
+    const uint32_t* ring_idx;
+};
+size_t radix_sort_scratch_bytes(uint32_t n);
+cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                             uint32_t* vals_out, uint32_t n, uint32_t passes, void* scratch, size_t scratch_bytes,
+                             cudaStream_t st, uint64_t* launches);
+cudaError_t launch_hash_keys(const float4* x, uint32_t n, float inv_cell, uint32_t bits, uint32_t* keys,
+                             uint32_t* vals, cudaStream_t st);
+// Keys, sort and bucket table of the positions in `pos`.
+cudaError_t collision_build(const XpbdWorld& W, const float4* pos, const CollisionBuffers& B, float inv_cell,
+                            int sms, cudaStream_t st, uint64_t* launches);
+// Self collision of `src` into `dst` (reference narrow phase, contributions summed in partner-index order).
+cudaError_t collision_resolve(const XpbdWorld& W, const float4* src, float4* dst, const CollisionBuffers& B,
+                              float inv_cell, uint32_t filter, int sms, cudaStream_t st, uint64_t* launches);
+// Pair list (a<b, lexicographic). Two passes: count per particle, exclusive scan, write.
+cudaError_t collision_pairs(const XpbdWorld& W, const float4* pos, const CollisionBuffers& B, float inv_cell,
+                            uint32_t filter, uint32_t* pairs_out, uint64_t cap, uint64_t* total, int sms,
+                            cudaStream_t st);
+
+}  // namespace xpbd

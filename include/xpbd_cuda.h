@@ -1,0 +1,224 @@
+/*
+ * xpbd_cuda.h — C ABI of the B200 (sm_100a) XPBD cloth substep.
+ *
+ * Drop-in boundary for the GPU driver of the Rust crate `bevy_softbody` (mate-h/bevy_xpbd). The crate keeps its
+ * mesh preparation (src/mesh_prep.rs) and its plugin/resource types; what this library replaces is the wgpu host
+ * driver (src/cloth_jacobi.rs, src/cloth_compute.rs) and its WGSL kernels (src/shaders/cloth_sim_jacobi.wgsl,
+ * src/shaders/cloth_sim.wgsl). Each entry point below names the reference interface it stands in for.
+ *
+ * Conventions: plain pointers and sizes, no CUDA or torch types (streams are passed as `void*` holding a
+ * cudaStream_t). Every function returns XPBD_OK (0) or a negative XPBD_ERR_* code; xpbd_last_error() gives the
+ * message. Positions and velocities cross the boundary as packed xyz float triples (the reference's Vec3).
+ * One context per host thread; a context owns its device buffers and its stream. Device-side failures (non-finite
+ * positions, grid-barrier timeout, collision-list overflow, index out of range) are recorded in a device status
+ * word and returned by the next call that synchronises (xpbd_sync, xpbd_read_*).
+ */
+#ifndef XPBD_CUDA_H
+#define XPBD_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------------------------- */
+#define XPBD_OK 0
+#define XPBD_ERR_INVALID_ARGUMENT (-1)
+#define XPBD_ERR_CUDA (-2)
+#define XPBD_ERR_OUT_OF_MEMORY (-3)
+#define XPBD_ERR_UNSUPPORTED (-4)
+#define XPBD_ERR_STATE (-5)
+#define XPBD_ERR_DEVICE_NONFINITE (-6)
+#define XPBD_ERR_BARRIER_TIMEOUT (-7)
+#define XPBD_ERR_INDEX_RANGE (-8)
+#define XPBD_ERR_CAPACITY (-9)
+#define XPBD_ERR_NO_DEVICE (-10)
+
+/* ---- enumerations ---------------------------------------------------------------------------------------- */
+#define XPBD_SOLVER_JACOBI 0        /* Cargo feature solver-jacobi (default), cloth_jacobi.rs */
+#define XPBD_SOLVER_GAUSS_SEIDEL 1  /* Cargo feature solver-gauss-seidel, cloth_compute.rs:1271-1522 */
+
+#define XPBD_RELAX_OMEGA 0          /* Δx = ω·Σ (xpbd_cpu.rs:223, ω = jacobi_default_omega() = 0.32) */
+#define XPBD_RELAX_AVERAGE 1        /* Δx = ω·Σ / (constraints at the particle) — no reference counterpart */
+
+#define XPBD_LAMBDA_RESET_PER_ITERATION 0 /* λ cleared before every inner iteration (xpbd_cpu.rs:267) */
+#define XPBD_LAMBDA_PER_SUBSTEP 1         /* λ cleared (or warm-started) once per substep — standard XPBD */
+
+#define XPBD_COLLISION_NONE 0
+#define XPBD_COLLISION_REST_FILTER 1 /* self_collision_resolve filter: skip if dist² > rest² (xpbd_cpu.rs:98) */
+#define XPBD_COLLISION_RING_FILTER 2 /* skip partners within `ring_depth` topology rings (stretch+shear edges) */
+
+#define XPBD_ORDER_COLOR_REFERENCE 0 /* recolor: partition_constraints_for_gs_batches order (mesh_prep.rs:172-177) */
+#define XPBD_ORDER_COLOR_INDEX 1     /* recolor greedily in plain constraint-index order */
+#define XPBD_ORDER_PRESORTED 2       /* constraints already batch-sorted by the caller; use its batch offsets */
+
+#define XPBD_CONSTRAINT_STRETCH 0
+#define XPBD_CONSTRAINT_SHEAR 1
+#define XPBD_CONSTRAINT_BEND 2
+
+/* ---- parameter blocks ------------------------------------------------------------------------------------ */
+
+/* XpbdCpuTimeStepParams (xpbd_cpu.rs:11-26); on the GPU side the same fields travel in ClothSimParamsGpu
+ * (cloth_compute.rs:245-273), which this library derives (inv_dt², exp(-k·dt)) and uploads per call. */
+typedef struct xpbd_time_step_params {
+    float dt;                   /* substep length [s] */
+    float inv_dt;
+    float jacobi_omega;
+    uint32_t inner_iterations;
+    float gravity[3];
+    int32_t grab_idx;           /* particle index within the context (cloth offsets added), -1 = none */
+    uint32_t grab_active;
+    float grab_target[3];
+    float grab_stiffness;
+    float linear_drag_per_sec;  /* v *= exp(-k·dt) per substep */
+} xpbd_time_step_params;
+
+/* Solver configuration: ClothSimConfig (cloth_compute.rs:140-179) + ClothSimUniforms collision fields
+ * (:181-202), and the extension modes. Zero-initialise, then set what differs; xpbd_default_opts() fills the
+ * reference defaults. */
+typedef struct xpbd_solver_opts {
+    uint32_t solver;                  /* XPBD_SOLVER_* */
+    uint32_t relaxation;              /* XPBD_RELAX_* */
+    uint32_t lambda_mode;             /* XPBD_LAMBDA_* */
+    uint32_t substeps;                /* solve_substeps per frame */
+    uint32_t collision;               /* XPBD_COLLISION_* */
+    uint32_t collision_every_n_substeps; /* collision on substeps with si % N == N-1 (cloth_jacobi.rs:703-704) */
+    float thickness;                  /* THICKNESS (cloth_compute.rs:72) */
+    float coll_scale;                 /* DEFAULT_COLL_SCALE (cloth_compute.rs:74) */
+    float hash_cell;                  /* spatial hash cell edge [m], must be >= thickness */
+    uint32_t hash_table_bits;         /* hash table of 2^bits buckets */
+    uint32_t ring_depth;              /* for XPBD_COLLISION_RING_FILTER */
+    uint32_t ground_enabled;
+    float ground_y;
+    uint32_t use_graphs;              /* capture each frame as a CUDA graph */
+    float barrier_timeout_ms;         /* bound on every grid-barrier wait (default 2000) */
+    uint32_t block_threads;           /* 0 = autotuned / default */
+    uint32_t blocks_per_sm;           /* 0 = autotuned / default */
+    uint32_t warm_start;              /* 1: learned λ warm start (requires XPBD_LAMBDA_PER_SUBSTEP) */
+    uint32_t reserved[6];
+} xpbd_solver_opts;
+
+/* One cloth: the arrays of ClothMeshData / ClothSimConfig (mesh_prep.rs:103-131, cloth_compute.rs:140-179). All
+ * host pointers; copied by xpbd_add_cloth. Optional arrays may be NULL. */
+typedef struct xpbd_cloth_desc {
+    uint32_t num_particles;
+    const float* positions;           /* 3N, initial_pos */
+    const float* velocities;          /* 3N or NULL (zero) */
+    const float* inv_mass;            /* N, 0 = pinned */
+    const float* rest_positions;      /* 3N or NULL (= positions); used by the collision rest filter */
+    uint32_t num_constraints;
+    const uint32_t* constraint_i;
+    const uint32_t* constraint_j;
+    const float* rest_len;
+    const float* compliance;
+    const uint32_t* constraint_type;  /* E or NULL (all stretch); XPBD_CONSTRAINT_* */
+    uint32_t order;                   /* XPBD_ORDER_* */
+    const uint32_t* batch_offsets;    /* XPBD_ORDER_PRESORTED only: batch_count+1 entries */
+    uint32_t batch_count;
+} xpbd_cloth_desc;
+
+typedef struct xpbd_stats {
+    uint64_t frames;
+    uint64_t substeps;
+    uint32_t num_particles;
+    uint32_t num_constraints;
+    uint32_t num_cloths;
+    uint32_t num_colors;              /* max color batches over cloths (Gauss–Seidel sweep length) */
+    uint32_t grid_blocks;
+    uint32_t block_threads;
+    uint32_t graph_captured;
+    uint32_t cooperative_launch;
+    uint64_t kernel_launches;         /* launches issued by the library so far (graph nodes count once each) */
+    uint64_t warm_start_fallbacks;    /* substeps where the learned warm start was rejected */
+    uint64_t collision_pairs;         /* pairs found by the last collision pass (when counted) */
+} xpbd_stats;
+
+typedef struct xpbd_ctx xpbd_ctx;
+
+/* ---- lifetime ---------------------------------------------------------------------------------------------- */
+/* init_cloth_sim (cloth_compute.rs:571-623 → cloth_jacobi.rs:213-569): creates the context on `device`. */
+int xpbd_create(xpbd_ctx** out, int device);
+void xpbd_destroy(xpbd_ctx* ctx);
+void xpbd_default_opts(xpbd_solver_opts* opts);
+/* Use a caller stream (cudaStream_t as void*, NULL = the context's own stream). */
+int xpbd_set_stream(xpbd_ctx* ctx, void* stream);
+
+/* ---- building the batch ------------------------------------------------------------------------------------ */
+/* ClothMeshData::to_sim_config + the buffer creation of init_cloth_sim_jacobi (cloth_compute.rs:1597-1705,
+ * cloth_jacobi.rs:213-569, pack_neighbor_gpu :95-111). Cloths are packed by offset tables; ids count from 0. */
+int xpbd_add_cloth(xpbd_ctx* ctx, const xpbd_cloth_desc* desc, uint32_t* cloth_id);
+/* Builds coloring, neighbour tables and device buffers for every added cloth. */
+int xpbd_commit(xpbd_ctx* ctx);
+
+/* ---- per-frame --------------------------------------------------------------------------------------------- */
+/* prepare_cloth_bind_groups_jacobi's per-frame ClothSimParamsGpu::pack upload (cloth_jacobi.rs:583-584). */
+int xpbd_set_params(xpbd_ctx* ctx, const xpbd_time_step_params* params, const xpbd_solver_opts* opts);
+/* run_cloth_sim_jacobi / run_cloth_sim_gauss_seidel (cloth_jacobi.rs:675-916, cloth_compute.rs:1271-1522):
+ * enqueue `frames` frames of opts.substeps substeps each on the context stream (asynchronous). */
+int xpbd_step(xpbd_ctx* ctx, uint32_t frames);
+/* Headless `step(params)`: set_params(params, current opts) + step(frames). */
+int xpbd_step_params(xpbd_ctx* ctx, const xpbd_time_step_params* params, uint32_t frames);
+/* Enqueue single substeps (xpbd_substep_no_collision / _with_self_collision, xpbd_cpu.rs:411-578). */
+int xpbd_substep(xpbd_ctx* ctx, uint32_t substeps);
+/* Wait for the stream and report device-side errors. */
+int xpbd_sync(xpbd_ctx* ctx);
+
+/* ---- state ------------------------------------------------------------------------------------------------- */
+/* Readback of sim_pos / velocities (gpu_cpu_parity_jacobi.rs:766-797). cloth_id = UINT32_MAX reads all. */
+int xpbd_read_positions(xpbd_ctx* ctx, uint32_t cloth_id, float* out_xyz);
+int xpbd_read_velocities(xpbd_ctx* ctx, uint32_t cloth_id, float* out_xyz);
+int xpbd_write_state(xpbd_ctx* ctx, uint32_t cloth_id, const float* xyz, const float* vel_xyz);
+/* reset_cloth_sim_state_jacobi (cloth_jacobi.rs:918-944): back to the initial positions, zero velocity and λ. */
+int xpbd_reset(xpbd_ctx* ctx);
+/* Per-constraint λ after the last substep, in the cloth's input constraint order (extension). */
+int xpbd_read_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out);
+/* Max strain residual |‖xi−xj‖−rest|/rest over the constraints of a cloth (UINT32_MAX = all) — extension. */
+int xpbd_strain_residual(xpbd_ctx* ctx, uint32_t cloth_id, float* out);
+int xpbd_get_stats(xpbd_ctx* ctx, xpbd_stats* out);
+/* Color batches of a cloth: perm[k] = input index of the k-th batch-sorted constraint; offsets has batch_count+1
+ * entries (mesh_prep.rs:153-221). Pass NULL to query only *batch_count. */
+int xpbd_get_coloring(xpbd_ctx* ctx, uint32_t cloth_id, uint32_t* perm, uint32_t* offsets, uint32_t* batch_count);
+
+/* Host-only (no device needed): greedy edge coloring of one cloth's constraints exactly as
+ * partition_constraints_for_gs_batches (mesh_prep.rs:153-221) — order XPBD_ORDER_COLOR_REFERENCE — or in plain index
+ * order (XPBD_ORDER_COLOR_INDEX). perm: num_constraints entries; offsets: num_constraints+1 entries capacity. */
+int xpbd_color_constraints(uint32_t num_particles, uint32_t num_constraints, const uint32_t* constraint_i,
+                           const uint32_t* constraint_j, uint32_t order, uint32_t* perm, uint32_t* offsets,
+                           uint32_t* batch_count);
+
+/* ---- autotuning -------------------------------------------------------------------------------------------- */
+/* Times `frames` frames per candidate schedule (block size × resident blocks per SM) on a snapshot of the state,
+ * restores the state and keeps the fastest. Writes the chosen block_threads / blocks_per_sm to opts_out. */
+int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* opts_out);
+
+/* ---- collision pipeline introspection (bit-exact parity tests) ---------------------------------------------- */
+/* Runs the spatial hash on the current positions: keys[i] = hash(cell(x_i)) & (2^bits-1); then the stable LSD
+ * radix sort (4 × 8-bit passes) of (key, particle index). Any output may be NULL. */
+int xpbd_collision_keys(xpbd_ctx* ctx, uint32_t* keys, uint32_t* sorted_keys, uint32_t* sorted_vals);
+/* Collision pairs (a<b, lexicographic) of the current positions under opts.collision; *count = total pairs,
+ * at most `cap` written as (a,b) uint32 pairs. */
+int xpbd_collision_pairs(xpbd_ctx* ctx, uint32_t* pairs, uint64_t cap, uint64_t* count);
+
+/* ---- standalone device primitives (device pointers, caller stream) ----------------------------------------- */
+/* Stable LSD radix sort of 32-bit keys with 32-bit payload, 8-bit digits, `passes` (1..4) passes from the least
+ * significant digit. keys_in/vals_in are not modified. `scratch` must hold xpbd_radix_sort_scratch_bytes(n). */
+size_t xpbd_radix_sort_scratch_bytes(uint32_t n);
+int xpbd_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                          uint32_t n, uint32_t passes, void* scratch, size_t scratch_bytes, void* stream);
+/* keys[i] = prime-hash(floor(xyz_i * inv_cell)) & (2^bits - 1), positions as float4 (w ignored). */
+int xpbd_hash_keys(const float* xyzw, uint32_t n, float inv_cell, uint32_t table_bits, uint32_t* keys,
+                   void* stream);
+
+/* ---- diagnostics ------------------------------------------------------------------------------------------- */
+const char* xpbd_last_error(xpbd_ctx* ctx);
+const char* xpbd_status_string(int status);
+/* Test hook for failure detection: the next step's first grid barrier expects one block more than the grid has,
+ * so it can never complete and times out after `timeout_ms`, setting XPBD_ERR_BARRIER_TIMEOUT. */
+int xpbd_debug_force_barrier_timeout(xpbd_ctx* ctx, float timeout_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XPBD_CUDA_H */
