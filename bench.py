@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Throughput of the XPBD cloth substep on B200: cloth-steps/s (one cloth advanced one 1/60 s frame of 10 substeps x
+10 iterations).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c3|c0|c2] [--impl ours|reference]
+
+Default workload (the headline): c1 — one 256x256 sheet (65,536 particles, 390,658 constraints), colored
+Gauss–Seidel, damping 0.01. The same JSON line also carries the batched workload c3 (256 seeded cloths of 16..192
+vertices a side, plain Jacobi with degree-averaged corrections) under "batched", measured the same way.
+
+Timing: W untimed warm-up steps, then exactly K steps bracketed by a barrier + device synchronize; each step is timed
+with CUDA events on the stream the library launches on, max over ranks. Working sets below the 126 MB L2 are
+flushed (256 MiB write) between timed steps outside the events; larger ones are not. `e2e` is the same metric through
+the public API with host buffers: per step the parameter block goes host->device, one frame is stepped and the
+positions come back device->host, timed on the host clock. Multi-GPU: one process per GPU (torchrun); c1 runs one
+independent replica per rank, c3 shards the cloths across ranks — no collective in the step (weak scaling).
+
+--impl reference times the CPU restatement of the reference solver (src/xpbd_cpu.rs, OpenMP over the independent
+loops) on the same workload and prints the same line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "cloth-steps/s at 256² & batched; iters to 1e-4 strain residual, learned vs plain"
+UNIT = "cloth-steps/s"
+L2_BYTES = 126 * 1024 * 1024
+DEV_PARAMS_BYTES = 112  # sizeof(XpbdDevParams): the per-call parameter block uploaded by xpbd_set_params
+
+
+# ------------------------------------------------------------------------------------------------ workloads
+def make_workload(name: str, rank: int = 0, world: int = 1) -> dict:
+    from bevy_xpbd_b200 import plugin as P
+    from bevy_xpbd_b200 import workloads as wl
+    dt, inv_dt = wl.substep_dt(10)
+    if name == "c1":
+        specs = [wl.config1_sheet()]
+        prm = P.XpbdCpuTimeStepParams(float(dt), float(inv_dt), 1.0, 10, linear_drag_per_sec=0.01)
+        cfg = P.ClothSimConfig(solver=P.SOLVER_GAUSS_SEIDEL, solve_substeps=10)
+        desc = "c1: 256x256 sheet, 2 m, top edge pinned, colored Gauss-Seidel, 10 substeps x 10 iterations, damping 0.01"
+        total_cloths = world  # one replica per rank
+    elif name == "c0":
+        specs = [wl.config0_sheet()]
+        prm = P.XpbdCpuTimeStepParams(float(dt), float(inv_dt), 1.0, 10)
+        cfg = P.ClothSimConfig(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
+        desc = "c0: 32x32 sheet, 1 m, two corners pinned, plain Jacobi (degree-averaged), 10 substeps x 10 iterations"
+        total_cloths = world
+    elif name == "c2":
+        specs = [wl.config2_sheet()]
+        prm = P.XpbdCpuTimeStepParams(float(dt), float(inv_dt), 1.0, 10)
+        cfg = P.ClothSimConfig(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10,
+                               collision=P.COLLISION_RING_FILTER, thickness=0.002, hash_cell=0.004,
+                               hash_table_bits=20, ring_depth=2, ground_enabled=True, ground_y=0.0)
+        desc = ("c2: 512x512 sheet, 2 m, unpinned, falling and folding; self collision every substep (hash cell 4 mm, "
+                "2^20 table, stable 4x8-bit radix sort, 27-cell query, 2-ring filter, thickness 2 mm); Jacobi 10x10")
+        total_cloths = world
+    elif name == "c3":
+        allspecs = wl.config3_batch()
+        specs = [s for k, s in enumerate(allspecs) if k % world == rank]
+        prm = P.XpbdCpuTimeStepParams(float(dt), float(inv_dt), 1.0, 10)
+        cfg = P.ClothSimConfig(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
+        desc = ("c3: 256 cloths, sides seeded uniform 16..192 vertices, random pins and stretch compliance, packed into "
+                "one persistent launch per frame, plain Jacobi (degree-averaged), 10 substeps x 10 iterations")
+        total_cloths = len(allspecs)
+    else:
+        raise ValueError(name)
+    n = sum(s.num_particles for s in specs)
+    e = sum(s.num_constraints for s in specs)
+    S, I = cfg.solve_substeps, prm.inner_iterations
+    # algorithmic bytes per frame (fp32): S*(100N + I*(28N + 16E)); see DESIGN.md
+    bytes_alg = S * (100 * n + I * (28 * n + 16 * e))
+    return dict(name=name, specs=specs, params=prm, cfg=cfg, desc=desc, n=n, e=e, cloths=len(specs),
+                total_cloths=total_cloths, bytes_per_frame=bytes_alg)
+
+
+def working_set_bytes(w: dict) -> int:
+    # x, v, two Jacobi buffers, rest (16 B each per particle); 8 B per incidence + 16 B per constraint (two tables)
+    return 80 * w["n"] + 16 * w["e"] + 32 * w["e"]
+
+
+# ------------------------------------------------------------------------------------------------ helpers
+def load_peaks() -> dict:
+    for p in (os.path.join(ROOT, "MEASURED_PEAKS.json"),):
+        if os.path.exists(p):
+            with open(p) as f:
+                d = json.load(f)
+            return dict(hbm_gbs=float(d["hbm_gbs"]), source="measured")
+    return dict(hbm_gbs=6650.0, source="fallback")
+
+
+def load_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu summary (profiles/traffic.txt lines
+    'workload kernel bytes_per_launch'), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 3 and not line.startswith("#") and parts[0] == workload and parts[1] == kernel:
+            return float(parts[2])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples (every 200 ms) while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        import tempfile
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if self.proc is None or not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------------------------ GPU arm
+def build_plugin(w: dict, device: int):
+    from bevy_xpbd_b200 import plugin as P
+    plug = P.ClothComputePlugin(device)
+    for s in w["specs"]:
+        plug.add_spec(s)
+    plug.commit()
+    plug.set_params(w["params"], w["cfg"])
+    return plug
+
+
+def time_device(w: dict, plug, steps: int, warmup: int, world: int, device: int, flush: bool):
+    """K frames, each bracketed by CUDA events on the library's stream (torch's current stream)."""
+    import torch
+    stream = torch.cuda.current_stream()
+    plug.set_stream(stream.cuda_stream)
+    flush_buf = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda") if flush else None
+    for _ in range(warmup):
+        plug.step(frames=1)
+    plug.sync()
+    torch.cuda.synchronize()
+    st0 = plug.stats()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clk:
+        for a, b in evs:
+            if flush_buf is not None:
+                flush_buf.zero_()
+            a.record(stream)
+            plug.step(frames=1)
+            b.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    plug.sync()
+    st1 = plug.stats()
+    per = [a.elapsed_time(b) for a, b in evs]
+    total_ms = max_over_ranks(sum(per), world)
+    launches = int(st1["kernel_launches"] - st0["kernel_launches"])
+    plug.set_stream(None)
+    return total_ms, per, launches, clk.summary(), st1
+
+
+def time_e2e(w: dict, plug, steps: int, warmup: int, world: int):
+    """Through the public API with host buffers: params H2D, one frame, positions D2H, per step (host clock)."""
+    import torch
+    host = np.empty((plug.num_particles, 3), np.float32)
+    for _ in range(warmup):
+        plug.set_params(w["params"])
+        plug.step(frames=1)
+        plug.positions_into(host)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        plug.set_params(w["params"])
+        plug.step(frames=1)
+        plug.positions_into(host)
+    t1 = time.perf_counter()
+    barrier(world)
+    ms = max_over_ranks((t1 - t0) * 1e3, world)
+    return ms, host
+
+
+def roofline(w: dict, mean_ms: float, kernel: str, peaks: dict) -> dict:
+    achieved = w["bytes_per_frame"] / (mean_ms * 1e-3) / 1e9
+    traffic = load_traffic(kernel, w["name"])
+    return {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
+            "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peaks["source"],
+            "alg_bytes_per_launch": int(w["bytes_per_frame"]), "traffic": traffic}
+
+
+def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks: dict, with_e2e: bool) -> dict:
+    w = make_workload(name, rank, world)
+    t0 = time.time()
+    plug = build_plugin(w, device)
+    setup_s = time.time() - t0
+    tuned = plug.autotune(frames=2)
+    flush = working_set_bytes(w) < L2_BYTES
+    steps = args.steps if name == args.workload else args.batched_steps
+    total_ms, per, launches, clocks, st = time_device(w, plug, steps, args.warmup, world, device, flush)
+    mean_ms = total_ms / steps
+    cloth_steps = w["total_cloths"] * steps
+    kernel = "gs_persistent_kernel" if w["cfg"].solver == 1 else "jacobi_persistent_kernel"
+    res = {
+        "value": round(cloth_steps / (total_ms * 1e-3), 2),
+        "ms_per_step": round(mean_ms, 4),
+        "steps": steps,
+        "gpu_launches": launches,
+        "config": {"workload": w["desc"], "particles": w["n"], "constraints": w["e"], "cloths": w["cloths"],
+                   "substeps": w["cfg"].solve_substeps, "iterations": w["params"].inner_iterations,
+                   "colors": st["num_colors"], "block_threads": st["block_threads"], "grid_blocks": st["grid_blocks"],
+                   "blocks_per_sm_tuned": tuned.blocks_per_sm, "cuda_graph": bool(st["graph_captured"]),
+                   "cooperative_launch": bool(st["cooperative_launch"]),
+                   "l2": ("flushed between timed steps (256 MiB write outside the events)" if flush
+                          else f"inputs larger than L2 (working set {working_set_bytes(w) / 1e6:.0f} MB)"),
+                   "setup_s": round(setup_s, 2)},
+        "roofline": roofline(w, mean_ms, kernel, peaks) if w["cfg"].collision == 0 else None,
+        "clocks": clocks,
+        "step_ms_min_max": [round(min(per), 4), round(max(per), 4)],
+    }
+    if with_e2e:
+        e2e_ms, _ = time_e2e(w, plug, steps, args.warmup, world)
+        res["e2e"] = {"value": round(cloth_steps / (e2e_ms * 1e-3), 2), "unit": UNIT,
+                      "h2d_bytes_per_step": DEV_PARAMS_BYTES, "d2h_bytes_per_step": 12 * w["n"],
+                      "ms_per_step": round(e2e_ms / steps, 4)}
+    plug.close()
+    res["_w"] = w
+    return res
+
+
+# ------------------------------------------------------------------------------------------------ CPU arm
+def cpu_oracle_run(w: dict, budget_s: float, max_cloths: int | None = None, min_frames: int = 1):
+    """Times the OpenMP build of the CPU restatement of xpbd_cpu.rs on a bounded sample of workload `w`: every
+    `len/max_cloths`-th cloth, as many whole frames as fit in `budget_s` (at least `min_frames`)."""
+    from oracle import oracle as orc
+    from tests.helpers import oracle_params
+    orc.select("omp")
+    specs = w["specs"]
+    if max_cloths is not None and len(specs) > max_cloths:
+        specs = specs[:: len(specs) // max_cloths][:max_cloths]
+    sims = []
+    for sp in specs:
+        perm, _, offs = orc.partition(sp.num_particles, sp.constraint_i, sp.constraint_j)
+        s = orc.OracleSim(sp.positions, sp.inv_mass, sp.constraint_i[perm], sp.constraint_j[perm],
+                          sp.rest_len[perm], sp.compliance[perm], v=sp.velocities, rest_pos=sp.rest_positions,
+                          ctype=sp.constraint_type[perm])
+        s.set_params(oracle_params(w["params"], w["cfg"]))
+        s.set_batches(offs)
+        sims.append(s)
+    S = w["cfg"].solve_substeps
+    t0 = time.perf_counter()
+    for s in sims:  # one untimed frame: warm-up and per-frame estimate
+        s.substeps(S)
+    per_frame = time.perf_counter() - t0
+    frames = max(min_frames, int(budget_s / max(per_frame, 1e-6)))
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        for s in sims:
+            s.substeps(S)
+    t1 = time.perf_counter()
+    return dict(value=len(sims) * frames / (t1 - t0), frames=frames, cloths=len(sims), seconds=t1 - t0,
+                cores=orc.threads(), per_frame_s=(t1 - t0) / frames)
+
+
+def run_reference(args, rank: int, world: int):
+    """CPU restatement of the reference solver on all host cores; rank 0 only (other ranks exit without work)."""
+    if rank != 0:
+        return
+    w = make_workload(args.workload, 0, 1)
+    max_cloths = 16 if args.workload == "c3" else None
+    res = cpu_oracle_run(w, budget_s=0.0, max_cloths=max_cloths, min_frames=args.steps)
+    sample = (f"{res['frames']} frames of {res['cloths']} of the workload's {len(w['specs'])} cloths"
+              if max_cloths else f"{res['frames']} frames of the workload")
+    line = {"metric": METRIC, "value": round(res["value"], 4), "unit": UNIT, "n_gpus": world,
+            "steps": res["frames"], "warmup": 1, "ms_per_step": round(res["per_frame_s"] * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
+            "data": "synthetic: seeded procedural sheets (no dataset)",
+            "config": {"workload": w["desc"], "particles": w["n"], "constraints": w["e"]},
+            "cpu_baseline": {"value": round(res["value"], 4), "unit": UNIT, "cores": res["cores"], "kind": "port",
+                             "sample": sample + ", OpenMP build of the oracle"},
+            "e2e": {"value": round(res["value"], 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3"])
+    ap.add_argument("--batched-steps", type=int, default=10)
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    peaks = load_peaks()
+    main_res = run_gpu_workload(args.workload, args, rank, world, local, peaks, with_e2e=True)
+    w = main_res.pop("_w")
+    line = {"metric": METRIC, "value": main_res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": main_res["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded procedural sheets (no dataset)", "config": main_res["config"],
+            "roofline": main_res["roofline"], "e2e": main_res["e2e"], "gpu_launches": main_res["gpu_launches"],
+            "clocks": main_res["clocks"], "step_ms_min_max": main_res["step_ms_min_max"]}
+    line["config"]["parallelism"] = ("replicas" if args.workload != "c3" else "cloth shards") + f" x{world}"
+    if not args.no_batched and args.workload != "c3":
+        b = run_gpu_workload("c3", args, rank, world, local, peaks, with_e2e=False)
+        b.pop("_w")
+        line["batched"] = {"value": b["value"], "unit": UNIT, "ms_per_step": b["ms_per_step"], "steps": b["steps"],
+                           "config": b["config"], "roofline": b["roofline"], "gpu_launches": b["gpu_launches"],
+                           "clocks": b["clocks"]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_oracle_run(w, args.cpu_seconds, max_cloths=16 if args.workload == "c3" else None)
+        line["cpu_baseline"] = {"value": round(r["value"], 4), "unit": UNIT, "cores": r["cores"], "kind": "port",
+                                "sample": f"{r['frames']} frames of {r['cloths']} cloth(s) of the workload, "
+                                          f"{r['seconds']:.1f} s, OpenMP build of the oracle"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

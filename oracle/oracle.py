@@ -13,6 +13,18 @@ import numpy as np
 from . import build_oracle
 
 _lib = None
+_variant = "serial"
+
+
+def select(variant: str):
+    """'serial' (checker, the reference's loop order) or 'omp' (OpenMP build, used only as the timed CPU baseline;
+    it parallelises loops whose iterations are independent, so results are identical)."""
+    global _lib, _variant
+    if variant not in ("serial", "omp"):
+        raise ValueError(variant)
+    if variant != _variant:
+        _variant = variant
+        _lib = None
 
 
 class OracleParams(C.Structure):
@@ -30,7 +42,8 @@ class OracleParams(C.Structure):
 def lib():
     global _lib
     if _lib is None:
-        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "liboracle.so")
+        name = "liboracle.so" if _variant == "serial" else "liboracle_omp.so"
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), name)
         if not os.path.exists(path):
             build_oracle.build()
         L = C.CDLL(path)
@@ -67,6 +80,8 @@ def lib():
         L.oracle_stable_radix_sort.argtypes = [C.c_uint32, u32p, u32p, C.c_int]
         L.oracle_sim_collision_pairs.restype = C.c_uint64
         L.oracle_sim_collision_pairs.argtypes = [P, u32p, C.c_uint64]
+        L.oracle_sim_set_batches.argtypes = [P, C.c_void_p, C.c_uint32]
+        L.oracle_threads.restype = C.c_int
         _lib = L
     return _lib
 
@@ -198,6 +213,11 @@ class OracleSim:
         self._warm = None if lam is None else np.ascontiguousarray(lam, np.float32)
         lib().oracle_sim_set_warm_lambda(self.h, _ptr(self._warm))
 
+    def set_batches(self, offsets):
+        """Color-batch offsets of the (batch-sorted) constraints: lets the OpenMP build sweep a batch in parallel."""
+        self._batches = np.ascontiguousarray(offsets, np.uint32)
+        lib().oracle_sim_set_batches(self.h, _ptr(self._batches), len(self._batches) - 1)
+
     def strain_residual(self) -> float:
         return float(lib().oracle_sim_strain_residual(self.h))
 
@@ -207,6 +227,10 @@ class OracleSim:
         if cnt > cap:
             return self.collision_pairs(cnt)
         return buf[: 2 * cnt].reshape(-1, 2).copy()
+
+
+def threads() -> int:
+    return int(lib().oracle_threads())
 
 
 def self_collision_resolve(x, inv_mass, rest_pos, thickness, coll_scale):

@@ -2,6 +2,9 @@
 // oracle/build_oracle.py with -O2 -ffp-contract=off; loaded by oracle/oracle.py through ctypes.
 #include <cstdio>
 #include <memory>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include "xpbd_oracle.hpp"
 
@@ -238,6 +241,20 @@ void oracle_sim_set_warm_lambda(void* h, const float* lam) {
     s->f.warm_lambda.assign(lam, lam + e);
     s->d.warm_lambda.resize(e);
     for (size_t k = 0; k < e; ++k) s->d.warm_lambda[k] = lam[k];
+}
+void oracle_sim_set_batches(void* h, const uint32_t* offsets, uint32_t count) {
+    auto* s = (OracleSim*)h;
+    std::vector<uint32_t> b;
+    if (offsets) b.assign(offsets, offsets + count + 1);
+    s->f.batch_off = b;
+    s->d.batch_off = b;
+}
+int oracle_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
 }
 double oracle_sim_strain_residual(void* h) {
     auto* s = (OracleSim*)h;

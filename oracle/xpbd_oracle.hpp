@@ -523,7 +523,7 @@ struct Sim {
     std::vector<uint32_t> ci, cj, ctype;
     std::vector<T> rest, comp;
     std::vector<uint32_t> nb_off, nb_other, nb_eid;
-    std::vector<uint32_t> batch_off;
+    std::vector<uint32_t> batch_off;  // optional color batches: lets the OpenMP build sweep a batch in parallel
     std::vector<T> lambda, delta_lambda;
     std::vector<T> warm_lambda;  // extension: initial λ for the per-substep mode (empty → zeros)
     // 2-ring topology lists (extension collision filter): sorted, per vertex
@@ -565,6 +565,7 @@ struct Sim {
 
     // jacobi_edges_pass, xpbd_cpu.rs:139-184
     void jacobi_edges_pass(const std::vector<V>& jin, T inv_dt_sq) {
+#pragma omp parallel for schedule(static)
         for (size_t e = 0; e < ci.size(); ++e) {
             uint32_t i = ci[e], j = cj[e];
             T w_i = inv_mass[i], w_j = inv_mass[j];
@@ -608,6 +609,7 @@ struct Sim {
     }
 
     void predict_all() {  // xpbd_cpu.rs:251-260
+#pragma omp parallel for schedule(static)
         for (uint32_t i = 0; i < n; ++i) {
             if (inv_mass[i] <= (T)0) { prev_pos[i] = sim_pos[i]; continue; }
             V v = vel[i];
@@ -639,6 +641,7 @@ struct Sim {
             const std::vector<V>& rd = (k % 2 == 0) ? jac_b : jac_a;
             std::vector<V>& wr = (k % 2 == 0) ? jac_a : jac_b;
             jacobi_edges_pass(rd, inv_dt_sq);
+#pragma omp parallel for schedule(static)
             for (uint32_t i = 0; i < n; ++i) wr[i] = jacobi_gather_particle(i, rd);
         }
         const std::vector<V>& fin = (p.inner_iterations % 2 == 0) ? jac_b : jac_a;
@@ -653,21 +656,19 @@ struct Sim {
         begin_substep_lambda();
         T omega = (T)p.jacobi_omega;
         T inv_dt_sq = (T)p.inv_dt * (T)p.inv_dt;
-        for (uint32_t k = 0; k < p.inner_iterations; ++k) {
-            if (p.lambda_mode == 0) std::fill(lambda.begin(), lambda.end(), (T)0);
-            for (size_t e = 0; e < ci.size(); ++e) {
+        auto solve = [&](size_t e) {
                 uint32_t i = ci[e], j = cj[e];
                 T w_i = inv_mass[i], w_j = inv_mass[j];
-                if (w_j <= (T)0 && w_i <= (T)0) continue;
+                if (w_j <= (T)0 && w_i <= (T)0) return;
                 V p_i = jw[i], p_j = jw[j];
                 V gv = p_i - p_j;
                 T len = length(gv);
-                if (len < (T)1e-8f) continue;
+                if (len < (T)1e-8f) return;
                 gv = gv / len;
                 T c = len - rest[e];
                 T alpha_t = comp[e] * inv_dt_sq;
                 T wsum = w_i + w_j + alpha_t;
-                if (wsum < (T)1e-8f) continue;
+                if (wsum < (T)1e-8f) return;
                 T lam = lambda[e];
                 T dlam = (-c - alpha_t * lam) / wsum;
                 lambda[e] = lam + dlam;
@@ -675,6 +676,18 @@ struct Sim {
                 V dx_j = clamp_correction(-(((omega * gv) * w_j) * dlam));
                 if (w_i > (T)0) jw[i] = p_i + dx_i;
                 if (w_j > (T)0) jw[j] = p_j + dx_j;
+        };
+        for (uint32_t k = 0; k < p.inner_iterations; ++k) {
+            if (p.lambda_mode == 0) std::fill(lambda.begin(), lambda.end(), (T)0);
+            if (batch_off.size() >= 2) {
+                // a batch's constraints share no particle: any order (or parallel) gives the sequential result
+                for (size_t b = 0; b + 1 < batch_off.size(); ++b) {
+                    const long e0 = batch_off[b], e1 = batch_off[b + 1];
+#pragma omp parallel for schedule(static)
+                    for (long e = e0; e < e1; ++e) solve((size_t)e);
+                }
+            } else {
+                for (size_t e = 0; e < ci.size(); ++e) solve(e);
             }
         }
         for (uint32_t i = 0; i < n; ++i) sim_pos[i] = jw[i];
@@ -748,9 +761,9 @@ struct Sim {
         }
         std::vector<V> accum(n, V{0, 0, 0});
         uint64_t pairs = 0;
-        std::vector<uint32_t> cand;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : pairs)
         for (uint32_t i = 0; i < n; ++i) {
-            cand.clear();
+            std::vector<uint32_t> cand;
             for (int dz = -1; dz <= 1; ++dz)
                 for (int dy = -1; dy <= 1; ++dy)
                     for (int dx = -1; dx <= 1; ++dx) {
@@ -788,6 +801,7 @@ struct Sim {
         T damp = (T)p.damp;
         T inv_dt = (T)p.inv_dt;
         T gy = (T)p.ground_y;
+#pragma omp parallel for schedule(static)
         for (uint32_t i = 0; i < n; ++i) {
             if (inv_mass[i] <= (T)0) continue;
             if (p.ground_enabled && sim_pos[i].y < gy) sim_pos[i].y = gy;

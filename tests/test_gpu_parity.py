@@ -202,12 +202,25 @@ def test_self_collision_ring_filter_trajectory_bit_exact():
     assert plug.positions()[:, 1].min() >= 0.0
 
 
+def _folded_state(sp, gap=0.03):
+    """The sheet folded in half along its middle row: the upper half lies `gap` above the lower half."""
+    s = sp.side
+    x = sp.positions.reshape(s, s, 3).astype(np.float64).copy()
+    zf = x[s // 2, 0, 2]
+    x[s // 2:, :, 2] = 2 * zf - x[s // 2:, :, 2]
+    x[s // 2:, :, 1] += gap
+    return x.reshape(-1, 3).astype(np.float32)
+
+
 def test_hash_keys_sorted_order_and_pairs_bit_exact():
-    """Spatial hash keys, stable 4x8-bit LSD radix sort and the collision pair list of a folded state."""
+    """Spatial hash keys, stable 4x8-bit LSD radix sort and the collision pair list of a folded sheet, then the
+    collision-heavy trajectory from that state."""
     sp, prm, cfg = _folding_sheet(64)
     plug = gpu_sim(sp, prm, cfg)
-    plug.step(frames=60)
+    xf = _folded_state(sp)
+    plug.write_state(xf, np.zeros_like(xf))
     x = plug.positions()
+    assert np.array_equal(x, xf)
     keys, skeys, svals = plug.collision_keys()
     inv_cell = float(np.float32(1.0) / np.float32(cfg.hash_cell))
     okeys = orc.hash_keys(x, inv_cell, cfg.hash_table_bits)
@@ -217,10 +230,14 @@ def test_hash_keys_sorted_order_and_pairs_bit_exact():
     assert np.array_equal(svals, np.argsort(okeys, kind="stable").astype(np.uint32))
     pairs = plug.collision_pairs()
     o = oracle_sim(sp, prm, cfg)
-    o.set_state(x)
+    o.set_state(x, np.zeros_like(x))
     opairs = o.collision_pairs()
-    assert len(pairs) > 0
+    assert len(pairs) > 1000
     assert np.array_equal(pairs, opairs)
+    # trajectory with many contacts
+    plug.step(frames=5)
+    o.substeps(50)
+    assert max_abs(plug.positions(), o.state()[0]) == 0.0
 
 
 def test_radix_sort_primitive_matches_stable_argsort():

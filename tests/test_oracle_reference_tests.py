@@ -200,3 +200,28 @@ def test_oracle_fp32_vs_fp64_small_drift(cloth):
     xa, _ = a.state()
     xb, _ = b.state()
     assert np.max(np.abs(xa - xb)) < 1e-4
+
+
+@pytest.mark.parametrize("solver", SOLVERS)
+def test_oracle_openmp_build_matches_serial(solver):
+    """The OpenMP build (timed CPU baseline only) gives the serial checker's result bit for bit."""
+    from bevy_xpbd_b200 import workloads as wl
+    sp = wl.make_sheet(48, 1.0, 1.0, "top_edge", seed=2)
+    perm, _, offs = orc.partition(sp.num_particles, sp.constraint_i, sp.constraint_j)
+    p = default_params(solver)
+    p.update(relaxation=1 if solver == 0 else 0, inner_iterations=10)
+    out = []
+    for variant in ("serial", "omp"):
+        orc.select(variant)
+        try:
+            s = orc.OracleSim(sp.positions, sp.inv_mass, sp.constraint_i[perm], sp.constraint_j[perm],
+                              sp.rest_len[perm], sp.compliance[perm])
+            s.set_params(p)
+            if variant == "omp":
+                s.set_batches(offs)
+            s.substeps(20)
+            out.append(s.state()[0])
+            del s
+        finally:
+            orc.select("serial")
+    assert np.array_equal(out[0], out[1])
