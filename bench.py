@@ -224,7 +224,7 @@ def build_plugin(w: dict, device: int):
 def time_device(w: dict, plug, steps: int, warmup: int, world: int, device: int, flush: bool):
     """K frames, each bracketed by CUDA events on the library's stream (torch's current stream)."""
     import torch
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a real stream handle: the library launches on it, the events are recorded on it
     plug.set_stream(stream.cuda_stream)
     flush_buf = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda") if flush else None
     for _ in range(warmup):
@@ -232,13 +232,16 @@ def time_device(w: dict, plug, steps: int, warmup: int, world: int, device: int,
     plug.sync()
     torch.cuda.synchronize()
     st0 = plug.stats()
+    if flush_buf is not None:
+        flush_buf.record_stream(stream)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(device) as clk:
         for a, b in evs:
             if flush_buf is not None:
-                flush_buf.zero_()
+                with torch.cuda.stream(stream):
+                    flush_buf.zero_()
             a.record(stream)
             plug.step(frames=1)
             b.record(stream)

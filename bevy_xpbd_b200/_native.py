@@ -49,7 +49,8 @@ class SolverOpts(C.Structure):
         ("coll_scale", C.c_float), ("hash_cell", C.c_float), ("hash_table_bits", C.c_uint32),
         ("ring_depth", C.c_uint32), ("ground_enabled", C.c_uint32), ("ground_y", C.c_float),
         ("use_graphs", C.c_uint32), ("barrier_timeout_ms", C.c_float), ("block_threads", C.c_uint32),
-        ("blocks_per_sm", C.c_uint32), ("warm_start", C.c_uint32), ("reserved", C.c_uint32 * 6),
+        ("blocks_per_sm", C.c_uint32), ("warm_start", C.c_uint32), ("cluster_ctas", C.c_uint32),
+        ("reserved", C.c_uint32 * 5),
     ]
 
 

@@ -67,6 +67,11 @@ struct xpbd_ctx {
     // schedule
     uint32_t block = 256, grid = 0;
     bool coop = false;
+    uint32_t cl = 0;                 // >0: Gauss–Seidel runs in one cluster of `cl` CTAs
+    std::vector<uint4> con_host;     // color-major constraint table (host copy, for the cluster table)
+    std::vector<uint32_t> color_off_host;
+    ClusterTable ct{};
+    uint32_t ct_cl = 0;
     // graph
     cudaGraphExec_t exec = nullptr;
     std::string graph_key;
@@ -448,6 +453,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     }
     CK(cudaMemsetAsync(lam_con, 0, std::max<size_t>(E, 1) * sizeof(float), st), "memset");
     H2D(color_d, color_off.data(), color_off.size() * sizeof(uint32_t));
+    ctx->con_host = con;
+    ctx->color_off_host = color_off;
     CK(cudaMemsetAsync(status, 0, 4 * sizeof(int), st), "memset");
     CK(cudaMemsetAsync(sync, 0, sizeof(XpbdGridSync), st), "memset");
     CK(cudaStreamSynchronize(st), "commit sync");
@@ -478,9 +485,76 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
 }
 
 // ------------------------------------------------------------------------------------------------- schedule
+static uint32_t ceil_log2(uint32_t v) {
+    uint32_t s = 0;
+    while ((1u << s) < v) ++s;
+    return s;
+}
+
+// Groups the color-major constraint table by (color, rank owning the first endpoint) for a cluster of `cl` CTAs.
+static bool build_cluster_table(xpbd_ctx* ctx, uint32_t cl) {
+    if (ctx->ct_cl == cl) return true;
+    const uint32_t N = ctx->W.n;
+    const uint32_t shift = ceil_log2((N + cl - 1) / cl);
+    const uint32_t ncol = ctx->W.n_colors;
+    std::vector<uint32_t> cnt((size_t)ncol * cl + 1, 0);
+    for (uint32_t c = 0; c < ncol; ++c)
+        for (uint32_t e = ctx->color_off_host[c]; e < ctx->color_off_host[c + 1]; ++e)
+            ++cnt[(size_t)c * cl + (ctx->con_host[e].x >> shift) + 1];
+    uint32_t max_chunk = 0;
+    for (size_t k = 1; k < cnt.size(); ++k) max_chunk = std::max(max_chunk, cnt[k]);
+    for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
+    if (cluster_gs_smem_bytes(shift, max_chunk) > 220 * 1024) return false;
+    std::vector<uint4> rec(ctx->W.e);
+    std::vector<uint32_t> cur(cnt.begin(), cnt.end() - 1);
+    for (uint32_t c = 0; c < ncol; ++c)
+        for (uint32_t e = ctx->color_off_host[c]; e < ctx->color_off_host[c + 1]; ++e)
+            rec[cur[(size_t)c * cl + (ctx->con_host[e].x >> shift)]++] = ctx->con_host[e];
+    cudaError_t err = cudaSuccess;
+    uint4* drec = dev_alloc<uint4>(ctx, rec.size(), &err);
+    uint32_t* doff = nullptr;
+    if (err == cudaSuccess) doff = dev_alloc<uint32_t>(ctx, cnt.size(), &err);
+    if (err != cudaSuccess) return false;
+    if (!rec.empty() && cudaMemcpy(drec, rec.data(), rec.size() * 16, cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    if (cudaMemcpy(doff, cnt.data(), cnt.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) return false;
+    ctx->ct.rec = drec;
+    ctx->ct.off = doff;
+    ctx->ct.shift = shift;
+    ctx->ct.max_chunk = std::max<uint32_t>(max_chunk, 1);
+    ctx->ct_cl = cl;
+    return true;
+}
+
+// Cluster path: Gauss–Seidel, λ cleared per iteration, every particle fits in the cluster's shared memory.
+static uint32_t pick_cluster(xpbd_ctx* ctx, uint32_t want, uint32_t block) {
+    if (ctx->opts.solver != XPBD_SOLVER_GAUSS_SEIDEL || ctx->opts.lambda_mode != XPBD_LAMBDA_RESET_PER_ITERATION)
+        return 0;
+    if (want == 1) return 0;
+    const uint32_t cands[2] = {16, 8};
+    for (uint32_t cl : cands) {
+        if (want && want != cl) continue;
+        if (ctx->W.n > cl * 16384u) continue;
+        if (!build_cluster_table(ctx, cl)) continue;
+        if (cluster_gs_supported(cl, ctx->ct.shift, ctx->ct.max_chunk, block)) return cl;
+        cudaGetLastError();
+    }
+    return 0;
+}
+
 static void choose_schedule(xpbd_ctx* ctx) {
     uint32_t block = ctx->opts.block_threads ? ctx->opts.block_threads : 256;
     if (block != 128 && block != 256 && block != 512 && block != 1024) block = 256;
+    const uint32_t cblock = ctx->opts.block_threads ? block : 1024;
+    ctx->cl = pick_cluster(ctx, ctx->opts.cluster_ctas, cblock);
+    if (ctx->cl) {
+        ctx->block = cblock;
+        ctx->grid = ctx->cl;
+        ctx->coop = false;
+        ctx->stats.grid_blocks = ctx->cl;
+        ctx->stats.block_threads = cblock;
+        return;
+    }
     int maxb = max_blocks_per_sm(ctx->opts.solver, block);
     if (maxb < 1) maxb = 1;
     int bps = ctx->opts.blocks_per_sm ? (int)ctx->opts.blocks_per_sm : maxb;
@@ -495,6 +569,13 @@ static void choose_schedule(xpbd_ctx* ctx) {
     ctx->coop = ctx->coop_supported;
     ctx->stats.grid_blocks = grid;
     ctx->stats.block_threads = block;
+}
+
+static cudaError_t launch_substeps(xpbd_ctx* ctx, uint32_t flags, uint32_t substeps, uint32_t pend, uint32_t start,
+                                   cudaStream_t st) {
+    if (ctx->cl)
+        return launch_cluster_gs(ctx->cl, ctx->block, ctx->W, ctx->ct, flags, substeps, pend, st);
+    return launch_solver(ctx->opts.solver, ctx->block, ctx->grid, ctx->coop, ctx->W, flags, substeps, pend, start, st);
 }
 
 static int ensure_collision_buffers(xpbd_ctx* ctx) {
@@ -549,7 +630,7 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
     const float inv_cell = ctx->hp.inv_cell;
     cudaError_t e;
     if (!coll) {
-        e = launch_solver(solver, ctx->block, ctx->grid, ctx->coop, ctx->W, kEndFinalize, S, 0, 0, st);
+        e = launch_substeps(ctx, kEndFinalize, S, 0, 0, st);
         *launches += 1;
         return e;
     }
@@ -561,7 +642,7 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
         uint32_t flags = pending ? kBeginFinalize : 0u;
         if (last && !run_coll) flags |= kEndFinalize;
         const uint32_t start = (solver == XPBD_SOLVER_JACOBI) ? pend : 0u;
-        e = launch_solver(solver, ctx->block, ctx->grid, ctx->coop, ctx->W, flags, 1, pend, start, st);
+        e = launch_substeps(ctx, flags, 1, pend, start, st);
         *launches += 1;
         if (e != cudaSuccess) return e;
         if (last && !run_coll) return cudaSuccess;
@@ -586,9 +667,9 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
 static std::string schedule_key(xpbd_ctx* ctx) {
     const xpbd_solver_opts& o = ctx->opts;
     char buf[256];
-    snprintf(buf, sizeof(buf), "%u/%u/%u/%u/%u/%u/%u/%u/%d/%p/%u/%u", o.solver, o.substeps, o.collision,
+    snprintf(buf, sizeof(buf), "%u/%u/%u/%u/%u/%u/%u/%u/%d/%p/%u/%u/%u", o.solver, o.substeps, o.collision,
              o.collision_every_n_substeps, ctx->tsp.inner_iterations, ctx->block, ctx->grid, (int)ctx->coop,
-             (int)(o.coll_scale > 1e-12f), (void*)ctx->stream, o.hash_table_bits, o.ring_depth);
+             (int)(o.coll_scale > 1e-12f), (void*)ctx->stream, o.hash_table_bits, o.ring_depth, ctx->cl);
     return buf;
 }
 
@@ -907,34 +988,42 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
     cudaEventCreate(&b);
     xpbd_solver_opts base = ctx->opts;
     float best = 1e30f;
-    uint32_t best_block = 256, best_bps = 0;
+    xpbd_solver_opts best_opts = base;
+    struct Cand {
+        uint32_t block, bps, cl;
+    };
+    std::vector<Cand> cands;
     const uint32_t blocks[] = {128, 256, 512};
     for (uint32_t blk : blocks) {
         int maxb = max_blocks_per_sm(base.solver, blk);
-        for (int bps = 1; bps <= maxb; bps *= 2) {
-            ctx->opts = base;
-            ctx->opts.block_threads = blk;
-            ctx->opts.blocks_per_sm = (uint32_t)bps;
-            choose_schedule(ctx);
-            r = run_frames(ctx, 1);  // warm-up / capture
-            if (r != XPBD_OK) break;
-            cudaEventRecord(a, st);
-            r = run_frames(ctx, std::max<uint32_t>(1, frames));
-            cudaEventRecord(b, st);
-            if (r != XPBD_OK) break;
-            r = read_status(ctx);
-            if (r != XPBD_OK) break;
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, a, b);
-            if (ms < best) {
-                best = ms;
-                best_block = blk;
-                best_bps = (uint32_t)bps;
-            }
-            CK(cudaMemcpyAsync(ctx->W.x, sx, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
-            CK(cudaMemcpyAsync(ctx->W.v, sv, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
-        }
+        for (int bps = 1; bps <= maxb; bps *= 2) cands.push_back({blk, (uint32_t)bps, 1});
+    }
+    if (base.solver == XPBD_SOLVER_GAUSS_SEIDEL && base.cluster_ctas != 1)
+        for (uint32_t cl : {16u, 8u})
+            for (uint32_t blk : {512u, 1024u}) cands.push_back({blk, 0, cl});
+    for (const Cand& cd : cands) {
+        ctx->opts = base;
+        ctx->opts.block_threads = cd.block;
+        ctx->opts.blocks_per_sm = cd.bps;
+        ctx->opts.cluster_ctas = cd.cl;
+        choose_schedule(ctx);
+        if (cd.cl > 1 && ctx->cl != cd.cl) continue;  // cluster candidate not launchable here
+        r = run_frames(ctx, 1);  // warm-up / capture
         if (r != XPBD_OK) break;
+        cudaEventRecord(a, st);
+        r = run_frames(ctx, std::max<uint32_t>(1, frames));
+        cudaEventRecord(b, st);
+        if (r != XPBD_OK) break;
+        r = read_status(ctx);
+        if (r != XPBD_OK) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best) {
+            best = ms;
+            best_opts = ctx->opts;
+        }
+        CK(cudaMemcpyAsync(ctx->W.x, sx, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
+        CK(cudaMemcpyAsync(ctx->W.v, sv, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
     }
     CK(cudaMemcpyAsync(ctx->W.x, sx, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
     CK(cudaMemcpyAsync(ctx->W.v, sv, (size_t)N * 16, cudaMemcpyDeviceToDevice, st), "restore");
@@ -943,11 +1032,7 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
     cudaFree(sv);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    ctx->opts = base;
-    if (r == XPBD_OK) {
-        ctx->opts.block_threads = best_block;
-        ctx->opts.blocks_per_sm = best_bps;
-    }
+    ctx->opts = (r == XPBD_OK) ? best_opts : base;
     choose_schedule(ctx);
     if (opts_out) *opts_out = ctx->opts;
     return r;
@@ -1067,6 +1152,7 @@ extern "C" int xpbd_debug_force_barrier_timeout(xpbd_ctx* ctx, float timeout_ms)
     ctx->forced_timeout_ms = 0.f;
     fill_dev_params(ctx);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "forced launch");
+    (void)saved;
     r = read_status(ctx);  // expected XPBD_ERR_BARRIER_TIMEOUT; also resets the barrier state
     CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream), "p");
     CK(cudaStreamSynchronize(ctx->stream), "sync");

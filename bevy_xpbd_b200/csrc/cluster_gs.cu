@@ -1,0 +1,321 @@
+// Colored Gauss–Seidel for a sheet that fits in one thread-block cluster (sm_100a distributed shared memory).
+//
+// Same arithmetic as the grid-wide solver (gs_constraint, xpbd_cpu.rs:349-385; WGSL gs_edges,
+// cloth_sim.wgsl:154-210), different execution. A cluster of CL CTAs (8 portable or 16 non-portable) keeps the whole
+// working state — every particle as float4 {x, y, z, inverse mass} — in distributed shared memory: CTA r owns
+// particles [r*P, (r+1)*P) with P a power of two. A color batch is split by the CTA owning its first endpoint; each
+// CTA streams its chunk of constraint records from global memory into shared memory with a TMA bulk copy
+// (cp.async.bulk, completion on an mbarrier), double-buffered so the next color's chunk lands while the current one
+// is solved, and reads/writes both endpoints through shared::cluster loads and stores. Colors are separated by the
+// hardware cluster barrier (barrier.cluster arrive.release / wait.acquire) instead of a global-memory grid barrier.
+// Every CTA executes the same barrier sequence (no early exit); mbarrier waits are bounded and report
+// XPBD_DEV_BARRIER_TIMEOUT if exceeded.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "xpbd_internal.h"
+#include "xpbd_kernels.h"
+
+namespace xpbd {
+
+namespace {
+
+constexpr float kCap = 0.28f;     // JACOBI_CORRECTION_CAP
+constexpr float kVmax = 12.0f;    // PREDICT_MAX_SPEED
+constexpr float kGrab = 0.065f;   // GRAB_MAX_PULL_PER_SUBSTEP
+
+struct V3 {
+    float x, y, z;
+};
+__device__ __forceinline__ V3 v3(float4 a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ V3 vadd(V3 a, V3 b) { return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)}; }
+__device__ __forceinline__ V3 vsub(V3 a, V3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ V3 vmul(V3 a, float s) { return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)}; }
+__device__ __forceinline__ V3 vdiv(V3 a, float s) { return {__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s)}; }
+__device__ __forceinline__ float vlen(V3 a) {
+    return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)), __fmul_rn(a.z, a.z)));
+}
+__device__ __forceinline__ V3 vclamp(V3 dx) {
+    const float ml = vlen(dx);
+    if (ml > kCap && ml > 0.0f) return vmul(dx, __fdiv_rn(kCap, ml));
+    return dx;
+}
+__device__ __forceinline__ bool vfinite(V3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+
+__device__ __forceinline__ V3 predict(uint32_t i, V3 sim, V3& vel, const XpbdDevParams& P) {
+    V3 v = vadd(vel, vmul(V3{P.gravity[0], P.gravity[1], P.gravity[2]}, P.dt));
+    const float speed = vlen(v);
+    if (speed > kVmax && speed > 0.0f) v = vmul(v, __fdiv_rn(kVmax, speed));
+    V3 pos = vadd(sim, vmul(v, P.dt));
+    if (P.grab_active != 0u && (int32_t)i == P.grab_idx) {
+        V3 pull = vmul(vsub(V3{P.grab_target[0], P.grab_target[1], P.grab_target[2]}, pos), P.grab_stiffness);
+        const float pl = vlen(pull);
+        if (pl > kGrab && pl > 0.0f) pull = vmul(pull, __fdiv_rn(kGrab, pl));
+        pos = vadd(pos, pull);
+    }
+    vel = v;
+    return pos;
+}
+
+__device__ __forceinline__ V3 finalize(V3 xn, V3 xo, V3& vel, const XpbdDevParams& P, int* status) {
+    if (P.ground_enabled != 0u && xn.y < P.ground_y) xn.y = P.ground_y;
+    vel = vmul(vmul(vsub(xn, xo), P.inv_dt), P.damp);
+    if (!vfinite(xn) || !vfinite(vel)) atomicOr(status, XPBD_DEV_NONFINITE);
+    return xn;
+}
+
+// ---- PTX wrappers: cluster rank, distributed shared memory, cluster barrier, mbarrier + bulk copy
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint32_t map_rank(uint32_t addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ float4 ld_dsmem(uint32_t addr) {
+    float4 v;
+    asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"(addr)
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_dsmem(uint32_t addr, float4 v) {
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v.x), "f"(v.y), "f"(v.z),
+                 "f"(v.w)
+                 : "memory");
+}
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// Bounded wait for phase `parity` of `bar`; false if the limit was reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t it = 0; it < (1u << 26); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+// T.off[(c * CL + r)] .. T.off[c * CL + r + 1]: records of color c owned by rank r (uint4 {i, j, rest, comp}).
+template <int CL>
+__global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, ClusterTable T, uint32_t flags,
+                                                              uint32_t substeps, uint32_t pend) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const XpbdDevParams P = *W.params;
+    const uint32_t rank = cluster_rank();
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t shift = T.shift, mask = (1u << T.shift) - 1u;
+    const uint32_t base = rank << shift;
+    const uint32_t cnt = base < W.n ? min(1u << shift, W.n - base) : 0u;
+    float4* xs = reinterpret_cast<float4*>(smem);
+    uint4* buf0 = reinterpret_cast<uint4*>(smem + ((size_t)16 << shift));
+    uint4* buf1 = buf0 + T.max_chunk;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(buf1 + T.max_chunk);
+    __shared__ uint32_t s_rank_base[16];
+    if (tid < CL) s_rank_base[tid] = map_rank(smem_u32(xs), tid);
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    bool failed = false;
+    const uint32_t ncol = W.n_colors;
+    const uint32_t I = P.iterations;
+    // chunk schedule: q = 0, 1, 2, ... over (substep, iteration, color); chunk q uses buffer q&1
+    uint32_t phase[2] = {0u, 0u};
+    auto chunk_range = [&](uint32_t c, uint32_t& e0, uint32_t& e1) {
+        e0 = T.off[c * CL + rank];
+        e1 = T.off[c * CL + rank + 1];
+    };
+    auto issue = [&](uint32_t c, uint32_t b) {
+        uint32_t e0, e1;
+        chunk_range(c, e0, e1);
+        if (tid == 0 && e1 > e0) bulk_load(b ? buf1 : buf0, T.rec + e0, (e1 - e0) * 16u, &bars[b]);
+    };
+    const uint32_t total_chunks = substeps * I * ncol;
+    bool pending = (flags & kBeginFinalize) != 0u;
+    if (total_chunks > 0) issue(0, 0);
+    uint32_t q = 0;
+    for (uint32_t s = 0; s < substeps; ++s) {
+        // predict (own particles): optionally finalize the pending result first
+        for (uint32_t k = tid; k < cnt; k += nthr) {
+            const uint32_t i = base + k;
+            const float4 x4 = W.x[i];
+            if (x4.w <= 0.0f) {
+                xs[k] = x4;
+                continue;
+            }
+            V3 xo = v3(x4);
+            V3 vel = v3(W.v[i]);
+            if (pending) {
+                const V3 xn = finalize(v3(W.jac[s == 0 ? pend : 0u][i]), xo, vel, P, W.status);
+                W.x[i] = make_float4(xn.x, xn.y, xn.z, x4.w);
+                W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+                xo = xn;
+            }
+            const V3 p = predict(i, xo, vel, P);
+            xs[k] = make_float4(p.x, p.y, p.z, x4.w);
+        }
+        pending = true;
+        cluster_sync();
+        for (uint32_t it = 0; it < I; ++it) {
+            for (uint32_t c = 0; c < ncol; ++c, ++q) {
+                const uint32_t b = q & 1u;
+                if (q + 1 < total_chunks) issue((c + 1) % ncol, b ^ 1u);  // prefetch the next color's chunk
+                uint32_t e0, e1;
+                chunk_range(c, e0, e1);
+                if (e1 > e0) {
+                    if (!mbar_wait(&bars[b], phase[b])) {
+                        failed = true;
+                        if (tid == 0) atomicOr(W.status, XPBD_DEV_BARRIER_TIMEOUT);
+                    }
+                    phase[b] ^= 1u;
+                    const uint4* rec = b ? buf1 : buf0;
+                    for (uint32_t e = tid; e < e1 - e0 && !failed; e += nthr) {
+                        const uint4 cr = rec[e];
+                        const uint32_t ai = s_rank_base[cr.x >> shift] + ((cr.x & mask) << 4);
+                        const uint32_t aj = s_rank_base[cr.y >> shift] + ((cr.y & mask) << 4);
+                        const float4 pi4 = ld_dsmem(ai);
+                        const float4 pj4 = ld_dsmem(aj);
+                        const float w_i = pi4.w, w_j = pj4.w;
+                        if (w_j <= 0.0f && w_i <= 0.0f) continue;
+                        const V3 p_i = v3(pi4), p_j = v3(pj4);
+                        V3 gv = vsub(p_i, p_j);
+                        const float len = vlen(gv);
+                        if (len < 1e-8f) continue;
+                        gv = vdiv(gv, len);
+                        const float C = __fsub_rn(len, __uint_as_float(cr.z));
+                        const float alpha_t = __fmul_rn(__uint_as_float(cr.w), P.inv_dt_sq);
+                        const float wsum = __fadd_rn(__fadd_rn(w_i, w_j), alpha_t);
+                        if (wsum < 1e-8f) continue;
+                        const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
+                        const V3 og = {__fmul_rn(P.omega, gv.x), __fmul_rn(P.omega, gv.y), __fmul_rn(P.omega, gv.z)};
+                        const V3 dx_i = vclamp(vmul(vmul(og, w_i), dlam));
+                        V3 dxj = vmul(vmul(og, w_j), dlam);
+                        const V3 dx_j = vclamp(V3{-dxj.x, -dxj.y, -dxj.z});
+                        if (w_i > 0.0f) {
+                            const V3 n = vadd(p_i, dx_i);
+                            st_dsmem(ai, make_float4(n.x, n.y, n.z, w_i));
+                        }
+                        if (w_j > 0.0f) {
+                            const V3 n = vadd(p_j, dx_j);
+                            st_dsmem(aj, make_float4(n.x, n.y, n.z, w_j));
+                        }
+                    }
+                }
+                cluster_sync();
+            }
+        }
+        // finalize own particles (the predict of the next substep re-reads x, v)
+        const bool last = s + 1 == substeps;
+        if (!last || (flags & kEndFinalize)) {
+            for (uint32_t k = tid; k < cnt; k += nthr) {
+                const uint32_t i = base + k;
+                const float4 p4 = xs[k];
+                if (p4.w <= 0.0f) continue;
+                const V3 xo = v3(W.x[i]);
+                V3 vel = v3(W.v[i]);
+                const V3 xn = finalize(v3(p4), xo, vel, P, W.status);
+                W.x[i] = make_float4(xn.x, xn.y, xn.z, p4.w);
+                W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+            }
+            pending = false;
+        } else {
+            for (uint32_t k = tid; k < cnt; k += nthr) W.jac[0][base + k] = xs[k];
+        }
+        __syncthreads();
+    }
+    // no copy may still target this CTA's shared memory when it exits (every issued chunk was waited for)
+    cluster_sync();
+}
+
+size_t cluster_gs_smem_bytes(uint32_t shift, uint32_t max_chunk) {
+    return ((size_t)16 << shift) + 2 * (size_t)max_chunk * 16 + 2 * sizeof(uint64_t);
+}
+
+static const void* cluster_fn(uint32_t cl) {
+    if (cl == 8) return (const void*)gs_cluster_kernel<8>;
+    if (cl == 16) return (const void*)gs_cluster_kernel<16>;
+    return nullptr;
+}
+
+bool cluster_gs_supported(uint32_t cl, uint32_t shift, uint32_t max_chunk, uint32_t block) {
+    const void* fn = cluster_fn(cl);
+    if (!fn) return false;
+    const size_t smem = cluster_gs_smem_bytes(shift, max_chunk);
+    if (smem > 220 * 1024) return false;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+    if (cl > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+        return false;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return clusters >= 1;
+}
+
+cudaError_t launch_cluster_gs(uint32_t cl, uint32_t block, const XpbdWorld& W, const ClusterTable& T,
+                              uint32_t flags, uint32_t substeps, uint32_t pend, cudaStream_t st) {
+    const void* fn = cluster_fn(cl);
+    if (!fn) return cudaErrorInvalidValue;
+    const size_t smem = cluster_gs_smem_bytes(T.shift, T.max_chunk);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    XpbdWorld w = W;
+    ClusterTable t = T;
+    void* args[] = {&w, &t, &flags, &substeps, &pend};
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+}  // namespace xpbd

@@ -99,37 +99,34 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// All blocks of the grid meet here. Waits are bounded: after `barrier_timeout_ns` (or if another block already
-// reported an error) the waiting block records XPBD_DEV_BARRIER_TIMEOUT and every caller returns false, so a
-// launch that can never complete (blocks not co-resident, forced test timeout) ends instead of hanging.
+// All blocks of the grid meet here. One atomic per block: block 0 adds 2^31 - (expected - 1), every other block adds
+// 1, so the counter's top bit flips exactly when the last block arrives and the low bits return to their value;
+// each block then polls for the flip. Waits are bounded: after `barrier_timeout_ns` (or once another block reported
+// an error) the waiting block records XPBD_DEV_BARRIER_TIMEOUT and every caller returns false, so a launch that
+// cannot complete (blocks not co-resident, forced test timeout) ends instead of hanging.
 __device__ bool grid_barrier(const XpbdWorld& W, const XpbdDevParams& P) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
         XpbdGridSync* gs = W.sync;
-        unsigned expected = gridDim.x + gs->expected_extra;
-        unsigned g = ld_acquire(&gs->gen);
+        const unsigned expected = gridDim.x + gs->expected_extra;
+        const unsigned inc = (blockIdx.x == 0) ? (0x80000000u - (expected - 1u)) : 1u;
         __threadfence();
-        unsigned arrived = atomicAdd(&gs->count, 1u);
-        if (arrived == expected - 1) {
-            atomicExch(&gs->count, 0u);
-            __threadfence();
-            st_release(&gs->gen, g + 1);
-        } else {
-            unsigned long long t0 = global_ns();
-            unsigned spins = 0;
-            while (ld_acquire(&gs->gen) == g) {
-                ++spins;
-                if (spins > 32) __nanosleep(spins > 4096 ? 256 : 32);
-                if ((spins & 63) == 0) {
-                    if (*(volatile int*)W.status != 0) { ok = 0; break; }
-                    if (global_ns() - t0 > P.barrier_timeout_ns || spins > (1u << 30)) {
-                        set_status(W.status, XPBD_DEV_BARRIER_TIMEOUT);
-                        ok = 0;
-                        break;
-                    }
+        const unsigned old = atomicAdd(&gs->count, inc);
+        unsigned spins = 0;
+        unsigned long long t0 = 0;
+        while (((old ^ ld_acquire(&gs->count)) & 0x80000000u) == 0u) {
+            ++spins;
+            if ((spins & 255u) == 0u) {
+                if (t0 == 0) t0 = global_ns();
+                if (*(volatile int*)W.status != 0) { ok = 0; break; }
+                if (global_ns() - t0 > P.barrier_timeout_ns || spins > (1u << 30)) {
+                    set_status(W.status, XPBD_DEV_BARRIER_TIMEOUT);
+                    ok = 0;
+                    break;
                 }
+                if (spins > (1u << 16)) __nanosleep(128);
             }
         }
         __threadfence();
@@ -176,9 +173,13 @@ __device__ void predict_phase(const XpbdWorld& W, const XpbdDevParams& P, bool f
 // ---------------------------------------------------------------------------------------------- Jacobi tile
 enum TailMode : uint32_t { kTailNone = 0, kTailFinalize = 1, kTailFinalizePredict = 2 };
 
-// One Jacobi iteration for one warp tile (jacobi_edges + jacobi_gather fused). `sc` is the warp's 96-float
-// shared staging area. Contributions of incidence k: the reference's Δλ for its constraint (recomputed
-// identically from either endpoint) times n̂·w_self, summed per particle in neighbour-table order.
+constexpr uint32_t kTileChunk = 512;  // incidences staged per warp pass (a 32-particle cloth tile holds ~384)
+
+// One Jacobi iteration for one warp tile (jacobi_edges + jacobi_gather fused). Phase A: the lanes stride over the
+// tile's incidences (coalesced 8-byte records), each computing one incidence's correction — the reference's Δλ of
+// its constraint (recomputed identically from either endpoint) times n̂·w_self — into shared memory. Phase B: each
+// particle's lane sums its own incidences from shared memory in neighbour-table order (the reference's order), so
+// the result is bit-identical to jacobi_gather_particle. `sc` is the warp's 3 x kTileChunk staging area.
 __device__ __forceinline__ void jacobi_tile(const XpbdWorld& W, const XpbdDevParams& P, uint32_t tile,
                                             const float4* __restrict__ jin, float4* __restrict__ jout, float* sc,
                                             uint32_t lane, TailMode tail) {
@@ -197,32 +198,39 @@ __device__ __forceinline__ void jacobi_tile(const XpbdWorld& W, const XpbdDevPar
     const uint32_t I1 = __shfl_sync(kFull, re, cnt - 1);
     const float* pal = W.palette_comp + (uint32_t)t.cloth * XPBD_PALETTE;
     const bool persist = P.lambda_mode != 0u;
-    F3 acc = {0.0f, 0.0f, 0.0f};
-    for (uint32_t cb = I0; cb < I1; cb += 32) {
-        const uint32_t k = cb + lane;
-        // owner row of incidence k: smallest rr with row_end[rr] > k (binary search over the lanes' row ends)
-        uint32_t lo = 0, hi = cnt;
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    for (uint32_t cb = I0; cb < I1; cb += kTileChunk) {
+        const uint32_t ce = min(I1, cb + kTileChunk);
+        for (uint32_t k = cb + lane; k < ce + ((32u - ((ce - cb) & 31u)) & 31u); k += 32) {
+            // owner row of incidence k: smallest rr with row_end[rr] > k (binary search over the lanes' row ends)
+            uint32_t lo = 0, hi = cnt;
 #pragma unroll
-        for (int it = 0; it < 6; ++it) {
-            uint32_t mid = (lo + hi) >> 1;
-            uint32_t em = __shfl_sync(kFull, re, mid & 31u);
-            if (lo < hi) {
-                if (em > k) hi = mid; else lo = mid + 1;
+            for (int it = 0; it < 6; ++it) {
+                const uint32_t mid = (lo + hi) >> 1;
+                const uint32_t em = __shfl_sync(kFull, re, mid & 31u);
+                if (lo < hi) {
+                    if (em > k) hi = mid; else lo = mid + 1;
+                }
             }
-        }
-        const uint32_t rr = lo & 31u;
-        const float sx = __shfl_sync(kFull, ps.x, rr);
-        const float sy = __shfl_sync(kFull, ps.y, rr);
-        const float sz = __shfl_sync(kFull, ps.z, rr);
-        const float sw = __shfl_sync(kFull, ps.w, rr);
-        F3 c = {0.0f, 0.0f, 0.0f};
-        if (k < I1) {
+            const uint32_t rr = lo & 31u;
+            const float sx = __shfl_sync(kFull, ps.x, rr);
+            const float sy = __shfl_sync(kFull, ps.y, rr);
+            const float sz = __shfl_sync(kFull, ps.z, rr);
+            const float sw = __shfl_sync(kFull, ps.w, rr);
+            if (k >= ce) continue;
+            F3 c = {0.0f, 0.0f, 0.0f};
             const uint2 rec = W.inc[k];
             const uint32_t other = rec.x & XPBD_OTHER_MASK;
+            if (other >= W.n) {  // corrupt table: record and skip
+                set_status(W.status, XPBD_DEV_INDEX);
+                continue;
+            }
             const float rest = __uint_as_float(rec.y);
             const float4 po = jin[other];
             const F3 gv = sub3(F3{sx, sy, sz}, f3(po));
             const float len = len3(gv);
+            float lam_next = 0.0f;
+            bool write_lam = persist;
             if (!(len < 1e-8f)) {
                 const F3 nrm = div3(gv, len);
                 const float C = __fsub_rn(len, rest);
@@ -232,33 +240,35 @@ __device__ __forceinline__ void jacobi_tile(const XpbdWorld& W, const XpbdDevPar
                 if (!(wsum < 1e-8f)) {
                     const float lam = persist ? W.inc_lambda[k] : 0.0f;
                     dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
-                    if (persist) W.inc_lambda[k] = (tail == kTailFinalizePredict) ? 0.0f : __fadd_rn(lam, dlam);
-                } else if (persist && tail == kTailFinalizePredict) {
-                    W.inc_lambda[k] = 0.0f;
+                    lam_next = __fadd_rn(lam, dlam);
+                } else {
+                    write_lam = persist && tail == kTailFinalizePredict;
                 }
                 c = mul3(mul3(nrm, sw), dlam);
-            } else if (persist && tail == kTailFinalizePredict) {
-                W.inc_lambda[k] = 0.0f;
+            } else {
+                write_lam = persist && tail == kTailFinalizePredict;
             }
+            if (write_lam) W.inc_lambda[k] = (tail == kTailFinalizePredict) ? 0.0f : lam_next;
+            const uint32_t s = k - cb;
+            sc[s] = c.x;
+            sc[kTileChunk + s] = c.y;
+            sc[2 * kTileChunk + s] = c.z;
         }
-        sc[lane] = c.x;
-        sc[32 + lane] = c.y;
-        sc[64 + lane] = c.z;
         __syncwarp();
-        if (has_row) {
-            const uint32_t a = rs > cb ? rs : cb;
-            const uint32_t b = re < cb + 32 ? re : cb + 32;
+        if (has_row && re > cb && rs < ce) {
+            const uint32_t a = (rs > cb ? rs : cb) - cb;
+            const uint32_t b = (re < ce ? re : ce) - cb;
+#pragma unroll 4
             for (uint32_t q = a; q < b; ++q) {
-                const uint32_t s = q - cb;
-                acc.x = __fadd_rn(acc.x, sc[s]);
-                acc.y = __fadd_rn(acc.y, sc[32 + s]);
-                acc.z = __fadd_rn(acc.z, sc[64 + s]);
+                ax = __fadd_rn(ax, sc[q]);
+                ay = __fadd_rn(ay, sc[kTileChunk + q]);
+                az = __fadd_rn(az, sc[2 * kTileChunk + q]);
             }
         }
         __syncwarp();
     }
     if (!has_row || ps.w <= 0.0f) return;  // pinned: both buffers already hold the fixed position
-    F3 delta = {__fmul_rn(P.omega, acc.x), __fmul_rn(P.omega, acc.y), __fmul_rn(P.omega, acc.z)};
+    F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
     if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
     delta = clamp_correction(delta);
     F3 xn = add3(f3(ps), delta);
@@ -287,14 +297,14 @@ __device__ __forceinline__ void jacobi_tile(const XpbdWorld& W, const XpbdDevPar
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) jacobi_persistent_kernel(XpbdWorld W, uint32_t flags, uint32_t substeps,
                                                                   uint32_t pend, uint32_t start) {
-    __shared__ float s_contrib[BLOCK / 32][96];
+    extern __shared__ float s_contrib[];  // (BLOCK/32) x 3 x kTileChunk floats
     if (!status_clear(W)) return;
     const XpbdDevParams P = *W.params;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t gwarp = blockIdx.x * (BLOCK / 32) + warp;
     const uint32_t nwarps = gridDim.x * (BLOCK / 32);
-    float* sc = s_contrib[warp];
+    float* sc = s_contrib + warp * 3 * kTileChunk;
     const bool persist = P.lambda_mode != 0u;
 
     predict_phase(W, P, (flags & kBeginFinalize) != 0u, pend, start, true);
@@ -461,13 +471,26 @@ const void* solver_kernel_fn(uint32_t solver, uint32_t block) {
     return nullptr;
 }
 
+static size_t solver_dyn_smem(uint32_t solver, uint32_t block) {
+    return solver == 0 ? (size_t)(block / 32) * 3 * kTileChunk * sizeof(float) : 0;
+}
+
+// Opt in to the dynamic shared memory explicitly: the default 48 KB limit covers static + dynamic together.
+static bool set_smem_attr(const void* fn, size_t dyn) {
+    if (dyn == 0) return true;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) == cudaSuccess;
+}
+
 cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool cooperative, const XpbdWorld& W,
                           uint32_t flags, uint32_t substeps, uint32_t pend, uint32_t start, cudaStream_t st) {
     const void* fn = solver_kernel_fn(solver, block);
     if (!fn) return cudaErrorInvalidValue;
+    const size_t dyn = solver_dyn_smem(solver, block);
+    if (!set_smem_attr(fn, dyn)) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = dyn;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     if (cooperative) {
@@ -487,8 +510,10 @@ cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool c
 
 int max_blocks_per_sm(uint32_t solver, uint32_t block) {
     const void* fn = solver_kernel_fn(solver, block);
+    const size_t dyn = solver_dyn_smem(solver, block);
     int nb = 0;
-    if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, (int)block, 0) != cudaSuccess) return 0;
+    if (!fn || !set_smem_attr(fn, dyn)) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, (int)block, dyn) != cudaSuccess) return 0;
     return nb;
 }
 

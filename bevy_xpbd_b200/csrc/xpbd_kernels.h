@@ -19,6 +19,18 @@ cudaError_t launch_finalize(const XpbdWorld& W, uint32_t pend, int sms, cudaStre
 cudaError_t launch_strain_residual(const XpbdWorld& W, uint32_t e0, uint32_t e1, unsigned* out_bits, int sms,
                                    cudaStream_t st);
 
+// ---- cluster Gauss–Seidel (cluster_gs.cu)
+struct ClusterTable {
+    const uint4* rec;    // constraint records grouped by (color, owning rank)
+    const uint32_t* off; // ncolors * CL + 1 offsets into rec
+    uint32_t shift;      // particles per CTA = 1 << shift
+    uint32_t max_chunk;  // largest (color, rank) group, in records
+};
+size_t cluster_gs_smem_bytes(uint32_t shift, uint32_t max_chunk);
+bool cluster_gs_supported(uint32_t cl, uint32_t shift, uint32_t max_chunk, uint32_t block);
+cudaError_t launch_cluster_gs(uint32_t cl, uint32_t block, const XpbdWorld& W, const ClusterTable& T, uint32_t flags,
+                              uint32_t substeps, uint32_t pend, cudaStream_t st);
+
 // ---- collision (collision_kernels.cu)
 struct CollisionBuffers {
     uint32_t* keys;         // n

@@ -119,6 +119,7 @@ class ClothSimConfig:
     block_threads: int = 0
     blocks_per_sm: int = 0
     warm_start: bool = False
+    cluster_ctas: int = 0
 
     def to_c(self) -> N.SolverOpts:
         o = N.SolverOpts()
@@ -130,6 +131,7 @@ class ClothSimConfig:
         o.ground_enabled, o.ground_y = int(self.ground_enabled), self.ground_y
         o.use_graphs, o.barrier_timeout_ms = int(self.use_graphs), self.barrier_timeout_ms
         o.block_threads, o.blocks_per_sm, o.warm_start = self.block_threads, self.blocks_per_sm, int(self.warm_start)
+        o.cluster_ctas = self.cluster_ctas
         return o
 
 
@@ -295,6 +297,7 @@ class ClothComputePlugin:
         o = N.SolverOpts()
         self._check(self._L.xpbd_autotune(self._h, frames, C.byref(o)))
         self.config.block_threads, self.config.blocks_per_sm = o.block_threads, o.blocks_per_sm
+        self.config.cluster_ctas = o.cluster_ctas
         return self.config
 
     # ---- collision introspection

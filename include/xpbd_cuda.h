@@ -97,7 +97,8 @@ typedef struct xpbd_solver_opts {
     uint32_t block_threads;           /* 0 = autotuned / default */
     uint32_t blocks_per_sm;           /* 0 = autotuned / default */
     uint32_t warm_start;              /* 1: learned λ warm start (requires XPBD_LAMBDA_PER_SUBSTEP) */
-    uint32_t reserved[6];
+    uint32_t cluster_ctas;            /* Gauss–Seidel in one thread-block cluster: 0 auto, 1 off, 8 or 16 CTAs */
+    uint32_t reserved[5];
 } xpbd_solver_opts;
 
 /* One cloth: the arrays of ClothMeshData / ClothSimConfig (mesh_prep.rs:103-131, cloth_compute.rs:140-179). All

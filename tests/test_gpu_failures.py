@@ -23,7 +23,7 @@ def test_grid_barrier_wait_times_out_and_context_recovers(solver):
     XPBD_ERR_BARRIER_TIMEOUT, and the context keeps working afterwards."""
     sp, plug = _plug(solver)
     st = plug.debug_force_barrier_timeout(20.0)
-    assert st == N.ERR_BARRIER_TIMEOUT
+    assert st == N.ERR_BARRIER_TIMEOUT, plug._L.xpbd_last_error(plug._h).decode()
     plug.reset()
     plug.step(frames=2)
     x = plug.positions()

@@ -305,3 +305,27 @@ def test_full_size_config1_gauss_seidel_properties():
     perm, offs = plug.coloring(0)
     operm, _, ooffs = orc.partition(sp.num_particles, sp.constraint_i, sp.constraint_j)
     assert np.array_equal(perm, operm) and np.array_equal(offs, ooffs)
+
+
+@pytest.mark.parametrize("cluster", [1, 8, 16], ids=["grid_barrier", "cluster8", "cluster16"])
+def test_gauss_seidel_execution_paths_bit_exact(cluster):
+    """Both Gauss–Seidel executions — the grid-wide persistent kernel and the thread-block-cluster kernel with
+    the state in distributed shared memory — give the reference result, with and without a collision pass."""
+    sp = wl.make_sheet(72, 2.0, 1.0, "top_edge", seed=5)
+    prm = params_for(10, 10, 1.0, drag=0.01)
+    cfg = _cfg(solver=P.SOLVER_GAUSS_SEIDEL, solve_substeps=10, cluster_ctas=cluster)
+    plug = gpu_sim(sp, prm, cfg)
+    st = plug.stats()
+    if cluster > 1:
+        assert st["grid_blocks"] == cluster
+    plug.step(frames=6)
+    o = oracle_sim(sp, prm, cfg)
+    o.substeps(60)
+    assert max_abs(plug.positions(), o.state()[0]) == 0.0
+    cfg2 = _cfg(solver=P.SOLVER_GAUSS_SEIDEL, solve_substeps=10, cluster_ctas=cluster,
+                collision=P.COLLISION_RING_FILTER, thickness=0.03, hash_cell=0.06, ground_enabled=True)
+    plug2 = gpu_sim(sp, prm, cfg2)
+    plug2.step(frames=4)
+    o2 = oracle_sim(sp, prm, cfg2)
+    o2.substeps(40)
+    assert max_abs(plug2.positions(), o2.state()[0]) == 0.0
