@@ -296,7 +296,8 @@ def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks:
     total_ms, per, launches, clocks, st = time_device(w, plug, steps, args.warmup, world, device, flush)
     mean_ms = total_ms / steps
     cloth_steps = w["total_cloths"] * steps
-    kernel = "gs_persistent_kernel" if w["cfg"].solver == 1 else "jacobi_persistent_kernel"
+    kernel = {0: "jacobi_persistent_kernel", 1: "gs_persistent_kernel", 2: "jacobi_patch_kernel",
+              3: "gs_cluster_kernel"}[st["solver_kernel"]]
     res = {
         "value": round(cloth_steps / (total_ms * 1e-3), 2),
         "ms_per_step": round(mean_ms, 4),
@@ -305,7 +306,8 @@ def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks:
         "config": {"workload": w["desc"], "particles": w["n"], "constraints": w["e"], "cloths": w["cloths"],
                    "substeps": w["cfg"].solve_substeps, "iterations": w["params"].inner_iterations,
                    "colors": st["num_colors"], "block_threads": st["block_threads"], "grid_blocks": st["grid_blocks"],
-                   "blocks_per_sm_tuned": tuned.blocks_per_sm, "cuda_graph": bool(st["graph_captured"]),
+                   "blocks_per_sm_tuned": tuned.blocks_per_sm, "solver_kernel": kernel,
+                   "cluster_ctas": st["cluster_ctas"], "cuda_graph": bool(st["graph_captured"]),
                    "cooperative_launch": bool(st["cooperative_launch"]),
                    "l2": ("flushed between timed steps (256 MiB write outside the events)" if flush
                           else f"inputs larger than L2 (working set {working_set_bytes(w) / 1e6:.0f} MB)"),

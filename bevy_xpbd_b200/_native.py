@@ -50,7 +50,7 @@ class SolverOpts(C.Structure):
         ("ring_depth", C.c_uint32), ("ground_enabled", C.c_uint32), ("ground_y", C.c_float),
         ("use_graphs", C.c_uint32), ("barrier_timeout_ms", C.c_float), ("block_threads", C.c_uint32),
         ("blocks_per_sm", C.c_uint32), ("warm_start", C.c_uint32), ("cluster_ctas", C.c_uint32),
-        ("reserved", C.c_uint32 * 5),
+        ("jacobi_kernel", C.c_uint32), ("reserved", C.c_uint32 * 4),
     ]
 
 
@@ -70,7 +70,7 @@ class Stats(C.Structure):
         ("num_constraints", C.c_uint32), ("num_cloths", C.c_uint32), ("num_colors", C.c_uint32),
         ("grid_blocks", C.c_uint32), ("block_threads", C.c_uint32), ("graph_captured", C.c_uint32),
         ("cooperative_launch", C.c_uint32), ("kernel_launches", C.c_uint64), ("warm_start_fallbacks", C.c_uint64),
-        ("collision_pairs", C.c_uint64),
+        ("collision_pairs", C.c_uint64), ("solver_kernel", C.c_uint32), ("cluster_ctas", C.c_uint32),
     ]
 
 

@@ -37,6 +37,7 @@ struct ClothHost {
     uint32_t vtx_off = 0, con_off = 0;
     std::vector<uint32_t> lambda_inc;  // per input constraint: incidence holding its λ (Jacobi), or UINT32_MAX
     std::vector<uint32_t> lambda_gs;   // per input constraint: position in the color-major table
+    std::vector<uint32_t> lambda_patch;  // per input constraint: patch slot holding its λ, or UINT32_MAX
 };
 
 struct DeviceBuf {
@@ -68,6 +69,8 @@ struct xpbd_ctx {
     uint32_t block = 256, grid = 0;
     bool coop = false;
     uint32_t cl = 0;                 // >0: Gauss–Seidel runs in one cluster of `cl` CTAs
+    uint32_t kernel = 0;             // solver kernel id (0 Jacobi tiles, 1 Gauss–Seidel, 2 Jacobi patches)
+    bool patches_ok = false;
     std::vector<uint4> con_host;     // color-major constraint table (host copy, for the cluster table)
     std::vector<uint32_t> color_off_host;
     ClusterTable ct{};
@@ -310,6 +313,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     std::vector<float> palette((size_t)C * XPBD_PALETTE, 0.f);
     std::vector<uint4> con_in(E);
     inc.reserve(2 * (size_t)E);
+    PatchArrays patch_arrays;
+    bool patches_ok = true;
     for (uint32_t ci_ = 0; ci_ < C; ++ci_) {
         ClothHost& c = ctx->cloths[ci_];
         for (uint32_t i = 0; i < c.n; ++i) {
@@ -346,6 +351,20 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
         }
         std::vector<uint32_t> roff, other, eid;
         neighbor_csr(c.n, c.e, si.data(), sj.data(), roff, other, eid);
+        if (patches_ok) {  // spatial patches for the shared-memory Jacobi kernel
+            std::vector<float> srest(c.e);
+            std::vector<uint32_t> spal(c.e), slot;
+            for (uint32_t k = 0; k < c.e; ++k) {
+                srest[k] = c.rest[c.perm[k]];
+                spal[k] = pidx[c.perm[k]];
+            }
+            patches_ok = build_cloth_patches(c.n, c.rest_pos.data(), c.w.data(), c.e, si.data(), sj.data(),
+                                             srest.data(), spal.data(), roff, other, eid, c.vtx_off, ci_, 256,
+                                             4096, patch_arrays, slot);
+            c.lambda_patch.assign(c.e, 0xFFFFFFFFu);
+            if (patches_ok)
+                for (uint32_t k = 0; k < c.e; ++k) c.lambda_patch[c.perm[k]] = slot[k];
+        }
         c.lambda_inc.assign(c.e, 0xFFFFFFFFu);
         for (uint32_t i = 0; i < c.n; ++i) {
             const uint32_t g = c.vtx_off + i;
@@ -456,6 +475,51 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     ctx->con_host = con;
     ctx->color_off_host = color_off;
     CK(cudaMemsetAsync(status, 0, 4 * sizeof(int), st), "memset");
+    ctx->patches_ok = patches_ok && !patch_arrays.header.empty();
+    if (ctx->patches_ok) {
+        const size_t np_ = patch_arrays.header.size() / 6;
+        std::vector<XpbdPatch> ph(np_);
+        for (size_t k = 0; k < np_; ++k) {
+            const uint32_t* h = &patch_arrays.header[6 * k];
+            ph[k].parts_off = h[0];
+            ph[k].con_off = h[1];
+            ph[k].gofs_off = h[2];
+            ph[k].np = (uint16_t)(h[3] & 0xFFFF);
+            ph[k].nh = (uint16_t)(h[3] >> 16);
+            ph[k].nc_hi = (uint16_t)(h[4] >> 16);
+            ph[k].nc_lo = (uint16_t)(h[4] & 0xFFFF);
+            ph[k].cloth = (uint16_t)h[5];
+            ph[k].pad = 0;
+        }
+        XpbdPatch* d_ph;
+        uint32_t *d_parts, *d_gofs;
+        uint2* d_pcon;
+        uint16_t* d_slots;
+        float* d_plam;
+        const size_t ncon = patch_arrays.con.size() / 2;
+        ALLOC(d_ph, XpbdPatch, np_);
+        ALLOC(d_parts, uint32_t, patch_arrays.parts.size());
+        ALLOC(d_pcon, uint2, ncon);
+        ALLOC(d_gofs, uint32_t, patch_arrays.gofs.size());
+        ALLOC(d_slots, uint16_t, patch_arrays.slots.size());
+        ALLOC(d_plam, float, ncon);
+        H2D(d_ph, ph.data(), np_ * sizeof(XpbdPatch));
+        H2D(d_parts, patch_arrays.parts.data(), patch_arrays.parts.size() * 4);
+        if (ncon) H2D(d_pcon, patch_arrays.con.data(), ncon * 8);
+        H2D(d_gofs, patch_arrays.gofs.data(), patch_arrays.gofs.size() * 4);
+        if (!patch_arrays.slots.empty()) H2D(d_slots, patch_arrays.slots.data(), patch_arrays.slots.size() * 2);
+        CK(cudaMemsetAsync(d_plam, 0, std::max<size_t>(ncon, 1) * 4, st), "memset");
+        W.n_patches = (uint32_t)np_;
+        W.patch_max_local = patch_arrays.max_local;
+        W.patch_max_con = std::max<uint32_t>(patch_arrays.max_con, 1);
+        W.patch_con_total = (uint32_t)ncon;
+        W.patches = d_ph;
+        W.patch_parts = d_parts;
+        W.patch_con = d_pcon;
+        W.patch_gofs = d_gofs;
+        W.patch_slots = d_slots;
+        W.patch_lambda = d_plam;
+    }
     CK(cudaMemsetAsync(sync, 0, sizeof(XpbdGridSync), st), "memset");
     CK(cudaStreamSynchronize(st), "commit sync");
     W.x = x;
@@ -548,34 +612,45 @@ static void choose_schedule(xpbd_ctx* ctx) {
     const uint32_t cblock = ctx->opts.block_threads ? block : 1024;
     ctx->cl = pick_cluster(ctx, ctx->opts.cluster_ctas, cblock);
     if (ctx->cl) {
+        ctx->kernel = 1;
         ctx->block = cblock;
         ctx->grid = ctx->cl;
         ctx->coop = false;
         ctx->stats.grid_blocks = ctx->cl;
         ctx->stats.block_threads = cblock;
+        ctx->stats.solver_kernel = 3;
+        ctx->stats.cluster_ctas = ctx->cl;
         return;
     }
-    int maxb = max_blocks_per_sm(ctx->opts.solver, block);
+    if (ctx->opts.solver == XPBD_SOLVER_GAUSS_SEIDEL)
+        ctx->kernel = 1;
+    else
+        ctx->kernel = (ctx->patches_ok && ctx->opts.jacobi_kernel != 1) ? 2 : 0;
+    int maxb = max_blocks_per_sm(ctx->kernel, block, ctx->W);
     if (maxb < 1) maxb = 1;
     int bps = ctx->opts.blocks_per_sm ? (int)ctx->opts.blocks_per_sm : maxb;
     if (bps > maxb) bps = maxb;
     // never more blocks than useful work
-    uint64_t work = ctx->opts.solver == XPBD_SOLVER_JACOBI ? (uint64_t)ctx->W.n_tiles * 32 : ctx->W.n;
+    uint64_t need;
+    if (ctx->kernel == 0) need = ((uint64_t)ctx->W.n_tiles * 32 + block - 1) / block;
+    else if (ctx->kernel == 2) need = ctx->W.n_patches;
+    else need = (ctx->W.n + block - 1) / block;
     uint32_t grid = (uint32_t)ctx->sms * (uint32_t)bps;
-    uint32_t need = (uint32_t)std::max<uint64_t>(1, (work + block - 1) / block);
-    if (grid > need) grid = need;
+    if (grid > need) grid = (uint32_t)std::max<uint64_t>(1, need);
     ctx->block = block;
     ctx->grid = grid;
     ctx->coop = ctx->coop_supported;
     ctx->stats.grid_blocks = grid;
     ctx->stats.block_threads = block;
+    ctx->stats.solver_kernel = ctx->kernel;
+    ctx->stats.cluster_ctas = 0;
 }
 
 static cudaError_t launch_substeps(xpbd_ctx* ctx, uint32_t flags, uint32_t substeps, uint32_t pend, uint32_t start,
                                    cudaStream_t st) {
     if (ctx->cl)
         return launch_cluster_gs(ctx->cl, ctx->block, ctx->W, ctx->ct, flags, substeps, pend, st);
-    return launch_solver(ctx->opts.solver, ctx->block, ctx->grid, ctx->coop, ctx->W, flags, substeps, pend, start, st);
+    return launch_solver(ctx->kernel, ctx->block, ctx->grid, ctx->coop, ctx->W, flags, substeps, pend, start, st);
 }
 
 static int ensure_collision_buffers(xpbd_ctx* ctx) {
@@ -667,9 +742,9 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
 static std::string schedule_key(xpbd_ctx* ctx) {
     const xpbd_solver_opts& o = ctx->opts;
     char buf[256];
-    snprintf(buf, sizeof(buf), "%u/%u/%u/%u/%u/%u/%u/%u/%d/%p/%u/%u/%u", o.solver, o.substeps, o.collision,
+    snprintf(buf, sizeof(buf), "%u/%u/%u/%u/%u/%u/%u/%u/%d/%p/%u/%u/%u/%u", o.solver, o.substeps, o.collision,
              o.collision_every_n_substeps, ctx->tsp.inner_iterations, ctx->block, ctx->grid, (int)ctx->coop,
-             (int)(o.coll_scale > 1e-12f), (void*)ctx->stream, o.hash_table_bits, o.ring_depth, ctx->cl);
+             (int)(o.coll_scale > 1e-12f), (void*)ctx->stream, o.hash_table_bits, o.ring_depth, ctx->cl, ctx->kernel);
     return buf;
 }
 
@@ -899,6 +974,8 @@ extern "C" int xpbd_reset(xpbd_ctx* ctx) {
     if (r != XPBD_OK) return r;
     CK(cudaMemset(ctx->W.inc_lambda, 0, std::max<size_t>(ctx->W.n_inc, 1) * 4), "memset");
     CK(cudaMemset(ctx->W.con_lambda, 0, std::max<size_t>(ctx->W.e, 1) * 4), "memset");
+    if (ctx->W.patch_lambda)
+        CK(cudaMemset(ctx->W.patch_lambda, 0, std::max<size_t>(ctx->W.patch_con_total, 1) * 4), "memset");
     return XPBD_OK;
 }
 
@@ -908,15 +985,14 @@ extern "C" int xpbd_read_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out) {
     if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const ClothHost& h = ctx->cloths[cloth_id];
-    const bool jac = ctx->opts.solver == XPBD_SOLVER_JACOBI;
-    std::vector<float> all(jac ? std::max<uint32_t>(ctx->W.n_inc, 1) : std::max<uint32_t>(ctx->W.e, 1));
-    CK(cudaMemcpyAsync(all.data(), jac ? ctx->W.inc_lambda : ctx->W.con_lambda, all.size() * 4,
-                       cudaMemcpyDeviceToHost, ctx->stream), "readback");
+    const uint32_t kern = ctx->kernel;
+    const float* src = kern == 0 ? ctx->W.inc_lambda : (kern == 2 ? ctx->W.patch_lambda : ctx->W.con_lambda);
+    const size_t cnt = kern == 0 ? ctx->W.n_inc : (kern == 2 ? ctx->W.patch_con_total : ctx->W.e);
+    std::vector<float> all(std::max<size_t>(cnt, 1));
+    if (cnt) CK(cudaMemcpyAsync(all.data(), src, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream), "readback");
     int r = read_status(ctx);
-    for (uint32_t e = 0; e < h.e; ++e) {
-        if (jac) out[e] = h.lambda_inc[e] == 0xFFFFFFFFu ? 0.f : all[h.lambda_inc[e]];
-        else out[e] = all[h.lambda_gs[e]];
-    }
+    const std::vector<uint32_t>& map = kern == 0 ? h.lambda_inc : (kern == 2 ? h.lambda_patch : h.lambda_gs);
+    for (uint32_t e = 0; e < h.e; ++e) out[e] = map[e] == 0xFFFFFFFFu ? 0.f : all[map[e]];
     return r;
 }
 
@@ -990,22 +1066,29 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
     float best = 1e30f;
     xpbd_solver_opts best_opts = base;
     struct Cand {
-        uint32_t block, bps, cl;
+        uint32_t block, bps, cl, jk;
     };
     std::vector<Cand> cands;
     const uint32_t blocks[] = {128, 256, 512};
-    for (uint32_t blk : blocks) {
-        int maxb = max_blocks_per_sm(base.solver, blk);
-        for (int bps = 1; bps <= maxb; bps *= 2) cands.push_back({blk, (uint32_t)bps, 1});
+    const uint32_t jks[2] = {2, 1};
+    for (uint32_t jk : jks) {
+        if (base.solver != XPBD_SOLVER_JACOBI && jk == 2) continue;
+        if (jk == 2 && !ctx->patches_ok) continue;
+        const uint32_t kid = base.solver == XPBD_SOLVER_JACOBI ? (jk == 2 ? 2u : 0u) : 1u;
+        for (uint32_t blk : blocks) {
+            int maxb = max_blocks_per_sm(kid, blk, ctx->W);
+            for (int bps = 1; bps <= maxb; bps *= 2) cands.push_back({blk, (uint32_t)bps, 1, jk});
+        }
     }
     if (base.solver == XPBD_SOLVER_GAUSS_SEIDEL && base.cluster_ctas != 1)
         for (uint32_t cl : {16u, 8u})
-            for (uint32_t blk : {512u, 1024u}) cands.push_back({blk, 0, cl});
+            for (uint32_t blk : {512u, 1024u}) cands.push_back({blk, 0, cl, 0});
     for (const Cand& cd : cands) {
         ctx->opts = base;
         ctx->opts.block_threads = cd.block;
         ctx->opts.blocks_per_sm = cd.bps;
         ctx->opts.cluster_ctas = cd.cl;
+        ctx->opts.jacobi_kernel = cd.jk;
         choose_schedule(ctx);
         if (cd.cl > 1 && ctx->cl != cd.cl) continue;  // cluster candidate not launchable here
         r = run_frames(ctx, 1);  // warm-up / capture
@@ -1146,8 +1229,9 @@ extern "C" int xpbd_debug_force_barrier_timeout(xpbd_ctx* ctx, float timeout_ms)
     CK(cudaMemcpyAsync(ctx->W.sync, &gs, sizeof(gs), cudaMemcpyHostToDevice, ctx->stream), "sync");
     xpbd_solver_opts saved = ctx->opts;
     ctx->opts.use_graphs = 0;
-    cudaError_t e = launch_solver(ctx->opts.solver, ctx->block, ctx->grid, ctx->coop, ctx->W, kEndFinalize, 1, 0, 0,
-                                  ctx->stream);
+    cudaError_t e = launch_solver(ctx->cl ? 1u : ctx->kernel, ctx->cl ? 256u : ctx->block,
+                                  ctx->cl ? (uint32_t)ctx->sms : ctx->grid, ctx->coop_supported, ctx->W, kEndFinalize,
+                                  1, 0, 0, ctx->stream);
     ctx->opts = saved;
     ctx->forced_timeout_ms = 0.f;
     fill_dev_params(ctx);

@@ -35,8 +35,11 @@ __device__ __forceinline__ V3 vdiv(V3 a, float s) { return {__fdiv_rn(a.x, s), _
 __device__ __forceinline__ float vlen(V3 a) {
     return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)), __fmul_rn(a.z, a.z)));
 }
+// clamp_correction (xpbd_cpu.rs:28-36), skipping the root when |dx|² <= the largest float not above 0.28f².
 __device__ __forceinline__ V3 vclamp(V3 dx) {
-    const float ml = vlen(dx);
+    const float d = __fadd_rn(__fadd_rn(__fmul_rn(dx.x, dx.x), __fmul_rn(dx.y, dx.y)), __fmul_rn(dx.z, dx.z));
+    if (d <= __uint_as_float(0x3da0902du)) return dx;
+    const float ml = __fsqrt_rn(d);
     if (ml > kCap && ml > 0.0f) return vmul(dx, __fdiv_rn(kCap, ml));
     return dx;
 }
@@ -44,8 +47,11 @@ __device__ __forceinline__ bool vfinite(V3 a) { return isfinite(a.x) && isfinite
 
 __device__ __forceinline__ V3 predict(uint32_t i, V3 sim, V3& vel, const XpbdDevParams& P) {
     V3 v = vadd(vel, vmul(V3{P.gravity[0], P.gravity[1], P.gravity[2]}, P.dt));
-    const float speed = vlen(v);
-    if (speed > kVmax && speed > 0.0f) v = vmul(v, __fdiv_rn(kVmax, speed));
+    const float v2 = __fadd_rn(__fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)), __fmul_rn(v.z, v.z));
+    if (v2 >= 144.0f) {
+        const float speed = __fsqrt_rn(v2);
+        if (speed > kVmax && speed > 0.0f) v = vmul(v, __fdiv_rn(kVmax, speed));
+    }
     V3 pos = vadd(sim, vmul(v, P.dt));
     if (P.grab_active != 0u && (int32_t)i == P.grab_idx) {
         V3 pull = vmul(vsub(V3{P.grab_target[0], P.grab_target[1], P.grab_target[2]}, pos), P.grab_stiffness);

@@ -11,7 +11,10 @@
 #include "mesh_prep.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+
+#include "xpbd_internal.h"
 
 namespace xpbd {
 
@@ -184,6 +187,121 @@ void topology_rings(uint32_t n, uint32_t e_count, const uint32_t* ci, const uint
         off.push_back((uint32_t)idx.size());
     }
     (void)off0;
+}
+
+namespace {
+struct PatchBuilder {
+    uint32_t n;
+    const float* rest;
+    const float* w;
+    const uint32_t *si, *sj, *spal;
+    const float* srest;
+    const std::vector<uint32_t>&row_off, &other, &eid;
+    uint32_t vtx_off, cloth, target, max_entries;
+    PatchArrays& out;
+    std::vector<uint32_t>& slot_of_con;
+    std::vector<int32_t> local;      // particle -> local index in the current patch, -1 otherwise
+    std::vector<int32_t> con_slot;   // sorted constraint -> slot in the current patch, -1 otherwise
+    std::vector<uint32_t> ids;
+
+    bool emit(uint32_t lo, uint32_t hi) {
+        std::vector<uint32_t> owned(ids.begin() + lo, ids.begin() + hi);
+        std::sort(owned.begin(), owned.end());
+        for (uint32_t k = 0; k < owned.size(); ++k) local[owned[k]] = (int32_t)k;
+        std::vector<uint32_t> halo, cons;
+        for (uint32_t p : owned) {
+            if (w[p] <= 0.f) continue;  // only unpinned particles gather; their constraints are all a patch needs
+            for (uint32_t q = row_off[p]; q < row_off[p + 1]; ++q) {
+                const uint32_t e = eid[q];
+                if (con_slot[e] < 0) {
+                    con_slot[e] = 0;
+                    cons.push_back(e);
+                }
+                const uint32_t o = other[q];
+                if (local[o] == -1) {
+                    local[o] = -2;  // provisional halo mark
+                    halo.push_back(o);
+                }
+            }
+        }
+        std::sort(halo.begin(), halo.end());
+        std::sort(cons.begin(), cons.end());
+        const size_t nl = owned.size() + halo.size();
+        bool ok = nl <= XPBD_PATCH_MAX_LOCAL && cons.size() <= XPBD_PATCH_MAX_CON && nl + cons.size() <= max_entries &&
+                  owned.size() <= 0xFFFF && halo.size() <= 0xFFFF;
+        if (ok) {
+            for (uint32_t k = 0; k < halo.size(); ++k) local[halo[k]] = (int32_t)(owned.size() + k);
+            for (uint32_t k = 0; k < cons.size(); ++k) con_slot[cons[k]] = (int32_t)k;
+            const uint32_t parts_off = (uint32_t)out.parts.size();
+            const uint32_t con_off = (uint32_t)(out.con.size() / 2);
+            const uint32_t gofs_off = (uint32_t)out.gofs.size();
+            for (uint32_t p : owned) out.parts.push_back(p + vtx_off);
+            for (uint32_t p : halo) out.parts.push_back(p + vtx_off);
+            for (uint32_t e : cons) {
+                const uint32_t li = (uint32_t)local[si[e]], lj = (uint32_t)local[sj[e]];
+                uint32_t rb;
+                memcpy(&rb, &srest[e], 4);
+                out.con.push_back(li | (lj << 12) | (spal[e] << 24));
+                out.con.push_back(rb);
+                if (slot_of_con[e] == 0xFFFFFFFFu) slot_of_con[e] = con_off + (uint32_t)con_slot[e];
+            }
+            for (uint32_t p : owned) {
+                out.gofs.push_back((uint32_t)out.slots.size());
+                if (w[p] <= 0.f) continue;  // pinned: jacobi_gather returns jac_in unchanged
+                for (uint32_t q = row_off[p]; q < row_off[p + 1]; ++q) {
+                    const uint32_t e = eid[q];
+                    out.slots.push_back((uint16_t)((uint32_t)con_slot[e] | (sj[e] == p ? 0x8000u : 0u)));
+                }
+            }
+            out.gofs.push_back((uint32_t)out.slots.size());
+            out.header.insert(out.header.end(), {parts_off, con_off, gofs_off,
+                                                 (uint32_t)owned.size() | ((uint32_t)halo.size() << 16),
+                                                 (uint32_t)cons.size(), cloth});
+            out.max_local = std::max<uint32_t>(out.max_local, (uint32_t)nl);
+            out.max_con = std::max<uint32_t>(out.max_con, (uint32_t)cons.size());
+        }
+        for (uint32_t p : owned) local[p] = -1;
+        for (uint32_t p : halo) local[p] = -1;
+        for (uint32_t e : cons) con_slot[e] = -1;
+        return ok;
+    }
+
+    bool split(uint32_t lo, uint32_t hi, bool force) {
+        if (!force && hi - lo <= target) {
+            if (emit(lo, hi)) return true;
+            if (hi - lo == 1) return false;
+        }
+        if (hi - lo <= 1) return emit(lo, hi);
+        float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (uint32_t k = lo; k < hi; ++k)
+            for (int a = 0; a < 3; ++a) {
+                mn[a] = std::min(mn[a], rest[3 * ids[k] + a]);
+                mx[a] = std::max(mx[a], rest[3 * ids[k] + a]);
+            }
+        int axis = 0;
+        for (int a = 1; a < 3; ++a)
+            if (mx[a] - mn[a] > mx[axis] - mn[axis]) axis = a;
+        const uint32_t mid = lo + (hi - lo) / 2;
+        std::nth_element(ids.begin() + lo, ids.begin() + mid, ids.begin() + hi, [&](uint32_t x, uint32_t y) {
+            const float cx = rest[3 * x + axis], cy = rest[3 * y + axis];
+            return cx != cy ? cx < cy : x < y;
+        });
+        return split(lo, mid, false) && split(mid, hi, false);
+    }
+};
+}  // namespace
+
+bool build_cloth_patches(uint32_t n, const float* rest_xyz, const float* inv_mass, uint32_t e_count,
+                         const uint32_t* si, const uint32_t* sj, const float* srest, const uint32_t* spal,
+                         const std::vector<uint32_t>& row_off, const std::vector<uint32_t>& other,
+                         const std::vector<uint32_t>& eid, uint32_t vtx_off, uint32_t cloth, uint32_t target,
+                         uint32_t max_entries, PatchArrays& out, std::vector<uint32_t>& slot_of_con) {
+    slot_of_con.assign(e_count, 0xFFFFFFFFu);
+    PatchBuilder b{n, rest_xyz, inv_mass, si, sj, spal, srest, row_off, other, eid, vtx_off, cloth, target,
+                   max_entries, out, slot_of_con, std::vector<int32_t>(n, -1), std::vector<int32_t>(e_count, -1),
+                   std::vector<uint32_t>(n)};
+    for (uint32_t k = 0; k < n; ++k) b.ids[k] = k;
+    return b.split(0, n, false);
 }
 
 }  // namespace xpbd

@@ -50,9 +50,12 @@ __device__ __forceinline__ void set_status(int* status, int flag) {
     if ((*(volatile int*)status & flag) == 0) atomicOr(status, flag);
 }
 
-// clamp_correction, xpbd_cpu.rs:28-36
+// clamp_correction, xpbd_cpu.rs:28-36. When |dx|² <= 0x3da0902d (the largest float not above 0.28f²), sqrt(|dx|²)
+// <= 0.28f holds exactly, so the reference does not clamp and the square root can be skipped: same bits, cheaper.
 __device__ __forceinline__ F3 clamp_correction(F3 dx) {
-    float ml = len3(dx);
+    const float d = dot3(dx, dx);
+    if (d <= __uint_as_float(0x3da0902du)) return dx;
+    const float ml = __fsqrt_rn(d);
     if (ml > kCorrectionCap && ml > 0.0f) return mul3(dx, __fdiv_rn(kCorrectionCap, ml));
     return dx;
 }
@@ -61,8 +64,11 @@ __device__ __forceinline__ F3 clamp_correction(F3 dx) {
 __device__ __forceinline__ F3 predict_particle(uint32_t i, F3 sim, F3& vel, const XpbdDevParams& P) {
     F3 g = {P.gravity[0], P.gravity[1], P.gravity[2]};
     F3 v = add3(vel, mul3(g, P.dt));
-    float speed = len3(v);
-    if (speed > kMaxSpeed && speed > 0.0f) v = mul3(v, __fdiv_rn(kMaxSpeed, speed));
+    const float v2 = dot3(v, v);
+    if (v2 >= 144.0f) {  // below 12² the reference's speed = sqrt(v2) cannot exceed 12: skip the root
+        const float speed = __fsqrt_rn(v2);
+        if (speed > kMaxSpeed && speed > 0.0f) v = mul3(v, __fdiv_rn(kMaxSpeed, speed));
+    }
     F3 pos = add3(sim, mul3(v, P.dt));
     if (P.grab_active != 0u && (int32_t)i == P.grab_idx) {
         F3 tgt = {P.grab_target[0], P.grab_target[1], P.grab_target[2]};
@@ -353,6 +359,148 @@ __global__ void __launch_bounds__(BLOCK) jacobi_persistent_kernel(XpbdWorld W, u
     }
 }
 
+// ---------------------------------------------------------------------------------------------- Jacobi patches
+// One Jacobi iteration for one spatial patch (a CTA): stage the patch's particles and halo in shared memory, solve
+// each of its constraints once (reference jacobi_edges: Δλ and n̂ = (p_i - p_j)/len), then let every owned
+// particle sum its incidences in neighbour-table order (reference jacobi_gather: (±n̂·w)·Δλ) — bit-identical to the
+// reference with each constraint's square root and divisions evaluated once instead of once per endpoint.
+__device__ __forceinline__ void jacobi_patch(const XpbdWorld& W, const XpbdDevParams& P, uint32_t pid,
+                                             const float4* __restrict__ jin, float4* __restrict__ jout, float4* sm,
+                                             TailMode tail) {
+    const XpbdPatch pt = W.patches[pid];
+    const uint32_t np = pt.np, nl = (uint32_t)pt.np + pt.nh;
+    const uint32_t nc = ((uint32_t)pt.nc_hi << 16) | pt.nc_lo;
+    float4* spos = sm;
+    float4* sres = sm + W.patch_max_local;
+    const uint32_t* parts = W.patch_parts + pt.parts_off;
+    for (uint32_t t = threadIdx.x; t < nl; t += blockDim.x) spos[t] = jin[parts[t]];
+    __syncthreads();
+    const float* pal = W.palette_comp + (uint32_t)pt.cloth * XPBD_PALETTE;
+    const bool persist = P.lambda_mode != 0u;
+    const uint2* con = W.patch_con + pt.con_off;
+    for (uint32_t c = threadIdx.x; c < nc; c += blockDim.x) {
+        const uint2 rec = con[c];
+        const uint32_t li = rec.x & 0xFFFu, lj = (rec.x >> 12) & 0xFFFu;
+        const float4 pi = spos[li], pj = spos[lj];
+        const F3 gv = sub3(f3(pi), f3(pj));
+        const float len = len3(gv);
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool reset_lam = persist && tail == kTailFinalizePredict;
+        if (!(len < 1e-8f)) {
+            const F3 nrm = div3(gv, len);
+            const float C = __fsub_rn(len, __uint_as_float(rec.y));
+            const float alpha_t = __fmul_rn(pal[(rec.x >> 24) & 0xFu], P.inv_dt_sq);
+            const float wsum = __fadd_rn(__fadd_rn(pi.w, pj.w), alpha_t);
+            float dlam = 0.0f;
+            if (!(wsum < 1e-8f)) {
+                const float lam = persist ? W.patch_lambda[pt.con_off + c] : 0.0f;
+                dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
+                if (persist) {
+                    W.patch_lambda[pt.con_off + c] = reset_lam ? 0.0f : __fadd_rn(lam, dlam);
+                    reset_lam = false;
+                }
+            }
+            r = make_float4(nrm.x, nrm.y, nrm.z, dlam);
+        }
+        if (reset_lam) W.patch_lambda[pt.con_off + c] = 0.0f;
+        sres[c] = r;
+    }
+    __syncthreads();
+    const uint32_t* gofs = W.patch_gofs + pt.gofs_off;
+    for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
+        const float4 ps = spos[k];
+        if (ps.w <= 0.0f) continue;  // pinned: both buffers already hold the fixed position
+        const uint32_t q0 = gofs[k], q1 = gofs[k + 1];
+        float ax = 0.0f, ay = 0.0f, az = 0.0f;
+        for (uint32_t q = q0; q < q1; ++q) {
+            const uint32_t sl = W.patch_slots[q];
+            const float4 r = sres[sl & 0x7FFFu];
+            const float nx = (sl & 0x8000u) ? -r.x : r.x;
+            const float ny = (sl & 0x8000u) ? -r.y : r.y;
+            const float nz = (sl & 0x8000u) ? -r.z : r.z;
+            ax = __fadd_rn(ax, __fmul_rn(__fmul_rn(nx, ps.w), r.w));
+            ay = __fadd_rn(ay, __fmul_rn(__fmul_rn(ny, ps.w), r.w));
+            az = __fadd_rn(az, __fmul_rn(__fmul_rn(nz, ps.w), r.w));
+        }
+        F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
+        if (P.relaxation == 1u && q1 > q0) delta = div3(delta, (float)(q1 - q0));
+        delta = clamp_correction(delta);
+        F3 xn = add3(f3(ps), delta);
+        const uint32_t g = parts[k];
+        if (tail == kTailNone) {
+            jout[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+            continue;
+        }
+        const F3 xo = f3(W.x[g]);
+        F3 vel = f3(W.v[g]);
+        xn = finalize_particle(xn, xo, vel, P, W.status);
+        W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+        if (tail == kTailFinalizePredict) {
+            const F3 pos = predict_particle(g, xn, vel, P);
+            jout[g] = make_float4(pos.x, pos.y, pos.z, ps.w);
+        } else {
+            jout[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        }
+    }
+    __syncthreads();
+}
+
+// Persistent Jacobi over spatial patches; same flags / buffer protocol as jacobi_persistent_kernel.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) jacobi_patch_kernel(XpbdWorld W, uint32_t flags, uint32_t substeps,
+                                                             uint32_t pend, uint32_t start) {
+    extern __shared__ float4 s_patch[];
+    if (!status_clear(W)) return;
+    const XpbdDevParams P = *W.params;
+    const bool persist = P.lambda_mode != 0u;
+    predict_phase(W, P, (flags & kBeginFinalize) != 0u, pend, start, true);
+    if (persist) {  // λ of every patch constraint slot starts the substep at zero
+        const uint32_t stride = gridDim.x * blockDim.x;
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < W.patch_con_total; k += stride)
+            W.patch_lambda[k] = 0.0f;
+    }
+    if (!grid_barrier(W, P)) return;
+    uint32_t b = start;
+    const uint32_t I = P.iterations;
+    for (uint32_t s = 0; s < substeps; ++s) {
+        const bool last_sub = (s + 1 == substeps);
+        if (I == 0) {
+            const uint32_t stride = gridDim.x * blockDim.x;
+            const bool fin = !last_sub || (flags & kEndFinalize);
+            for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n && fin; i += stride) {
+                float4 p4 = W.jac[b][i];
+                if (p4.w <= 0.0f) continue;
+                const F3 xo = f3(W.x[i]);
+                F3 vel = f3(W.v[i]);
+                F3 xn = finalize_particle(f3(p4), xo, vel, P, W.status);
+                W.x[i] = make_float4(xn.x, xn.y, xn.z, p4.w);
+                W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+                if (!last_sub) {
+                    F3 pos = predict_particle(i, xn, vel, P);
+                    W.jac[b][i] = make_float4(pos.x, pos.y, pos.z, p4.w);
+                }
+            }
+            if (!last_sub && !grid_barrier(W, P)) return;
+            continue;
+        }
+        for (uint32_t k = 0; k < I; ++k) {
+            const float4* jin = W.jac[(b + k) & 1u];
+            float4* jout = W.jac[(b + k + 1) & 1u];
+            TailMode tail = kTailNone;
+            if (k + 1 == I) {
+                if (!last_sub) tail = kTailFinalizePredict;
+                else if (flags & kEndFinalize) tail = kTailFinalize;
+            }
+            for (uint32_t pid = blockIdx.x; pid < W.n_patches; pid += gridDim.x)
+                jacobi_patch(W, P, pid, jin, jout, s_patch, tail);
+            const bool very_last = last_sub && (k + 1 == I);
+            if (!very_last && !grid_barrier(W, P)) return;
+        }
+        b = (b + I) & 1u;
+    }
+}
+
 // ---------------------------------------------------------------------------------------------- Gauss–Seidel
 // One constraint of the colored sweep, xpbd_cpu.rs:349-385, in place on the working state.
 __device__ __forceinline__ void gs_constraint(const XpbdWorld& W, const XpbdDevParams& P, uint32_t e, float4* jw,
@@ -450,29 +598,33 @@ __global__ void strain_residual_kernel(XpbdWorld W, uint32_t e0, uint32_t e1, un
 template <int BLOCK>
 static const void* jacobi_fn() { return (const void*)jacobi_persistent_kernel<BLOCK>; }
 template <int BLOCK>
+static const void* patch_fn() { return (const void*)jacobi_patch_kernel<BLOCK>; }
+template <int BLOCK>
 static const void* gs_fn() { return (const void*)gs_persistent_kernel<BLOCK>; }
 
+// solver 0: Jacobi over warp tiles, 1: Gauss–Seidel, 2: Jacobi over spatial patches
 const void* solver_kernel_fn(uint32_t solver, uint32_t block) {
-    if (solver == 0) {
-        switch (block) {
-            case 128: return jacobi_fn<128>();
-            case 256: return jacobi_fn<256>();
-            case 512: return jacobi_fn<512>();
-            case 1024: return jacobi_fn<1024>();
-        }
-    } else {
-        switch (block) {
-            case 128: return gs_fn<128>();
-            case 256: return gs_fn<256>();
-            case 512: return gs_fn<512>();
-            case 1024: return gs_fn<1024>();
-        }
+    switch (solver * 10000 + block) {
+        case 128: return jacobi_fn<128>();
+        case 256: return jacobi_fn<256>();
+        case 512: return jacobi_fn<512>();
+        case 1024: return jacobi_fn<1024>();
+        case 10128: return gs_fn<128>();
+        case 10256: return gs_fn<256>();
+        case 10512: return gs_fn<512>();
+        case 11024: return gs_fn<1024>();
+        case 20128: return patch_fn<128>();
+        case 20256: return patch_fn<256>();
+        case 20512: return patch_fn<512>();
+        case 21024: return patch_fn<1024>();
     }
     return nullptr;
 }
 
-static size_t solver_dyn_smem(uint32_t solver, uint32_t block) {
-    return solver == 0 ? (size_t)(block / 32) * 3 * kTileChunk * sizeof(float) : 0;
+static size_t solver_dyn_smem(uint32_t solver, uint32_t block, const XpbdWorld& W) {
+    if (solver == 0) return (size_t)(block / 32) * 3 * kTileChunk * sizeof(float);
+    if (solver == 2) return ((size_t)W.patch_max_local + W.patch_max_con) * sizeof(float4);
+    return 0;
 }
 
 // Opt in to the dynamic shared memory explicitly: the default 48 KB limit covers static + dynamic together.
@@ -485,7 +637,7 @@ cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool c
                           uint32_t flags, uint32_t substeps, uint32_t pend, uint32_t start, cudaStream_t st) {
     const void* fn = solver_kernel_fn(solver, block);
     if (!fn) return cudaErrorInvalidValue;
-    const size_t dyn = solver_dyn_smem(solver, block);
+    const size_t dyn = solver_dyn_smem(solver, block, W);
     if (!set_smem_attr(fn, dyn)) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
@@ -500,7 +652,7 @@ cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool c
         cfg.numAttrs = 1;
     }
     XpbdWorld w = W;
-    if (solver == 0) {
+    if (solver != 1) {
         void* args[] = {&w, &flags, &substeps, &pend, &start};
         return cudaLaunchKernelExC(&cfg, fn, args);
     }
@@ -508,9 +660,9 @@ cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool c
     return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
-int max_blocks_per_sm(uint32_t solver, uint32_t block) {
+int max_blocks_per_sm(uint32_t solver, uint32_t block, const XpbdWorld& W) {
     const void* fn = solver_kernel_fn(solver, block);
-    const size_t dyn = solver_dyn_smem(solver, block);
+    const size_t dyn = solver_dyn_smem(solver, block, W);
     int nb = 0;
     if (!fn || !set_smem_attr(fn, dyn)) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, (int)block, dyn) != cudaSuccess) return 0;

@@ -53,6 +53,23 @@ struct XpbdTile {
     uint16_t cloth;  // cloth index (palette row)
 };
 
+// Spatial patch of the Jacobi solve: `np` owned particles (a recursive-coordinate-bisection block of one cloth) and
+// `nh` halo particles read by its constraints. Local particle index: owned [0, np), halo [np, np+nh).
+//   parts[parts_off ...]      np owned then nh halo global particle indices
+//   con[con_off ...]          nc records {li | lj<<12 | palette<<24, rest bits}: every constraint with an owned
+//                             endpoint (not both pinned), each solved once per patch per iteration
+//   gofs[gofs_off ... + np]   per owned particle: range in `slots` of its incidences in neighbour-table order;
+//                             slot = local constraint index | 0x8000 when the particle is the constraint's j
+struct XpbdPatch {
+    uint32_t parts_off, con_off, gofs_off;
+    uint16_t np, nh;
+    uint16_t nc_hi, cloth;  // nc = nc_hi << 16 | nc_lo
+    uint16_t nc_lo, pad;
+};
+#define XPBD_PATCH_LOCAL_BITS 12
+#define XPBD_PATCH_MAX_LOCAL (1u << XPBD_PATCH_LOCAL_BITS)
+#define XPBD_PATCH_MAX_CON 32767u
+
 struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     uint32_t n, e, n_inc, n_tiles, n_colors, n_cloths;
     float4* x;
@@ -71,4 +88,12 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     const XpbdDevParams* params;
     int* status;
     XpbdGridSync* sync;
+    // patch-staged Jacobi
+    uint32_t n_patches, patch_max_local, patch_max_con, patch_con_total;
+    const XpbdPatch* patches;
+    const uint32_t* patch_parts;
+    const uint2* patch_con;
+    const uint32_t* patch_gofs;
+    const uint16_t* patch_slots;
+    float* patch_lambda;
 };

@@ -10,9 +10,9 @@ namespace xpbd {
 constexpr uint32_t kBeginFinalize = 1u;  // finalize positions waiting in jac[pend] before predicting
 constexpr uint32_t kEndFinalize = 2u;    // finalize the launch's last substep in place
 
-// ---- solver (solver_kernels.cu)
+// ---- solver (solver_kernels.cu); kernel id: 0 Jacobi warp tiles, 1 Gauss–Seidel, 2 Jacobi spatial patches
 const void* solver_kernel_fn(uint32_t solver, uint32_t block);
-int max_blocks_per_sm(uint32_t solver, uint32_t block);
+int max_blocks_per_sm(uint32_t solver, uint32_t block, const XpbdWorld& W);
 cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool cooperative, const XpbdWorld& W,
                           uint32_t flags, uint32_t substeps, uint32_t pend, uint32_t start, cudaStream_t st);
 cudaError_t launch_finalize(const XpbdWorld& W, uint32_t pend, int sms, cudaStream_t st);

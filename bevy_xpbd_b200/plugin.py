@@ -120,6 +120,7 @@ class ClothSimConfig:
     blocks_per_sm: int = 0
     warm_start: bool = False
     cluster_ctas: int = 0
+    jacobi_kernel: int = 0
 
     def to_c(self) -> N.SolverOpts:
         o = N.SolverOpts()
@@ -132,6 +133,7 @@ class ClothSimConfig:
         o.use_graphs, o.barrier_timeout_ms = int(self.use_graphs), self.barrier_timeout_ms
         o.block_threads, o.blocks_per_sm, o.warm_start = self.block_threads, self.blocks_per_sm, int(self.warm_start)
         o.cluster_ctas = self.cluster_ctas
+        o.jacobi_kernel = self.jacobi_kernel
         return o
 
 
@@ -298,6 +300,7 @@ class ClothComputePlugin:
         self._check(self._L.xpbd_autotune(self._h, frames, C.byref(o)))
         self.config.block_threads, self.config.blocks_per_sm = o.block_threads, o.blocks_per_sm
         self.config.cluster_ctas = o.cluster_ctas
+        self.config.jacobi_kernel = o.jacobi_kernel
         return self.config
 
     # ---- collision introspection
