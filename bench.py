@@ -297,7 +297,7 @@ def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks:
     mean_ms = total_ms / steps
     cloth_steps = w["total_cloths"] * steps
     kernel = {0: "jacobi_persistent_kernel", 1: "gs_persistent_kernel", 2: "jacobi_patch_kernel",
-              3: "gs_cluster_kernel"}[st["solver_kernel"]]
+              3: "gs_cluster_kernel", 5: "jacobi_row_kernel"}[st["solver_kernel"]]
     res = {
         "value": round(cloth_steps / (total_ms * 1e-3), 2),
         "ms_per_step": round(mean_ms, 4),

@@ -444,6 +444,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     ALLOC(inc_d, uint2, inc.size());
     ALLOC(lam_inc, float, inc.size());
     ALLOC(tiles_d, XpbdTile, tiles.size());
+    uint16_t* rcloth_d;
+    ALLOC(rcloth_d, uint16_t, N);
     ALLOC(pal_d, float, palette.size());
     ALLOC(con_d, uint4, E);
     ALLOC(lam_con, float, E);
@@ -465,6 +467,13 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     if (!inc.empty()) H2D(inc_d, inc.data(), inc.size() * sizeof(uint2));
     CK(cudaMemsetAsync(lam_inc, 0, std::max<size_t>(inc.size(), 1) * sizeof(float), st), "memset");
     H2D(tiles_d, tiles.data(), tiles.size() * sizeof(XpbdTile));
+    {
+        std::vector<uint16_t> rc(N);
+        for (uint32_t k = 0; k < C; ++k)
+            for (uint32_t i = 0; i < ctx->cloths[k].n; ++i) rc[ctx->cloths[k].vtx_off + i] = (uint16_t)k;
+        H2D(rcloth_d, rc.data(), N * sizeof(uint16_t));
+        CK(cudaStreamSynchronize(st), "commit sync");
+    }
     H2D(pal_d, palette.data(), palette.size() * sizeof(float));
     if (E) {
         H2D(con_d, con.data(), E * sizeof(uint4));
@@ -477,47 +486,64 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     CK(cudaMemsetAsync(status, 0, 4 * sizeof(int), st), "memset");
     ctx->patches_ok = patches_ok && !patch_arrays.header.empty();
     if (ctx->patches_ok) {
+        // one contiguous 16-byte aligned blob per patch: parts | con | gofs (patch-relative) | slots
         const size_t np_ = patch_arrays.header.size() / 6;
         std::vector<XpbdPatch> ph(np_);
+        std::vector<uint32_t> words;  // blob storage in u32 words (16-byte = 4 words granularity)
+        uint32_t max_blob = 0;
+        auto pad16 = [&]() {
+            while (words.size() % 4) words.push_back(0);
+        };
         for (size_t k = 0; k < np_; ++k) {
             const uint32_t* h = &patch_arrays.header[6 * k];
-            ph[k].parts_off = h[0];
-            ph[k].con_off = h[1];
-            ph[k].gofs_off = h[2];
-            ph[k].np = (uint16_t)(h[3] & 0xFFFF);
-            ph[k].nh = (uint16_t)(h[3] >> 16);
-            ph[k].nc_hi = (uint16_t)(h[4] >> 16);
-            ph[k].nc_lo = (uint16_t)(h[4] & 0xFFFF);
+            const uint32_t parts_off = h[0], con_off = h[1], gofs_off = h[2];
+            const uint32_t npo = h[3] & 0xFFFF, nh = h[3] >> 16, nc = h[4];
+            const size_t start_w = words.size();
+            for (uint32_t t = 0; t < npo + nh; ++t) words.push_back(patch_arrays.parts[parts_off + t]);
+            pad16();
+            for (uint32_t c = 0; c < nc; ++c) {
+                words.push_back(patch_arrays.con[2 * (con_off + c)]);
+                words.push_back(patch_arrays.con[2 * (con_off + c) + 1]);
+            }
+            pad16();
+            const uint32_t s0 = patch_arrays.gofs[gofs_off], s1 = patch_arrays.gofs[gofs_off + npo];
+            for (uint32_t t = 0; t <= npo; ++t) words.push_back(patch_arrays.gofs[gofs_off + t] - s0);
+            pad16();
+            for (uint32_t q = s0; q < s1; q += 2) {
+                const uint32_t lo = patch_arrays.slots[q];
+                const uint32_t hi = (q + 1 < s1) ? patch_arrays.slots[q + 1] : 0u;
+                words.push_back(lo | (hi << 16));
+            }
+            pad16();
+            const uint32_t bytes = (uint32_t)((words.size() - start_w) * 4);
+            ph[k].off16 = (uint32_t)(start_w / 4);
+            ph[k].bytes = bytes;
+            ph[k].nc = nc;
+            ph[k].lam_off = con_off;
+            ph[k].np = (uint16_t)npo;
+            ph[k].nh = (uint16_t)nh;
             ph[k].cloth = (uint16_t)h[5];
             ph[k].pad = 0;
+            max_blob = std::max(max_blob, bytes);
         }
         XpbdPatch* d_ph;
-        uint32_t *d_parts, *d_gofs;
-        uint2* d_pcon;
-        uint16_t* d_slots;
+        uint4* d_blob;
         float* d_plam;
         const size_t ncon = patch_arrays.con.size() / 2;
         ALLOC(d_ph, XpbdPatch, np_);
-        ALLOC(d_parts, uint32_t, patch_arrays.parts.size());
-        ALLOC(d_pcon, uint2, ncon);
-        ALLOC(d_gofs, uint32_t, patch_arrays.gofs.size());
-        ALLOC(d_slots, uint16_t, patch_arrays.slots.size());
+        ALLOC(d_blob, uint4, words.size() / 4);
         ALLOC(d_plam, float, ncon);
         H2D(d_ph, ph.data(), np_ * sizeof(XpbdPatch));
-        H2D(d_parts, patch_arrays.parts.data(), patch_arrays.parts.size() * 4);
-        if (ncon) H2D(d_pcon, patch_arrays.con.data(), ncon * 8);
-        H2D(d_gofs, patch_arrays.gofs.data(), patch_arrays.gofs.size() * 4);
-        if (!patch_arrays.slots.empty()) H2D(d_slots, patch_arrays.slots.data(), patch_arrays.slots.size() * 2);
+        H2D(d_blob, words.data(), words.size() * 4);
         CK(cudaMemsetAsync(d_plam, 0, std::max<size_t>(ncon, 1) * 4, st), "memset");
+        CK(cudaStreamSynchronize(st), "commit sync");
         W.n_patches = (uint32_t)np_;
         W.patch_max_local = patch_arrays.max_local;
         W.patch_max_con = std::max<uint32_t>(patch_arrays.max_con, 1);
         W.patch_con_total = (uint32_t)ncon;
+        W.patch_max_blob = max_blob;
         W.patches = d_ph;
-        W.patch_parts = d_parts;
-        W.patch_con = d_pcon;
-        W.patch_gofs = d_gofs;
-        W.patch_slots = d_slots;
+        W.patch_blob = d_blob;
         W.patch_lambda = d_plam;
     }
     CK(cudaMemsetAsync(sync, 0, sizeof(XpbdGridSync), st), "memset");
@@ -531,6 +557,7 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     W.inc = inc_d;
     W.inc_lambda = lam_inc;
     W.tiles = tiles_d;
+    W.row_cloth = rcloth_d;
     W.palette_comp = pal_d;
     W.con = con_d;
     W.con_lambda = lam_con;
@@ -624,8 +651,12 @@ static void choose_schedule(xpbd_ctx* ctx) {
     }
     if (ctx->opts.solver == XPBD_SOLVER_GAUSS_SEIDEL)
         ctx->kernel = 1;
+    else if (ctx->opts.jacobi_kernel == 1)
+        ctx->kernel = 0;
+    else if (ctx->opts.jacobi_kernel == 3)
+        ctx->kernel = 5;
     else
-        ctx->kernel = (ctx->patches_ok && ctx->opts.jacobi_kernel != 1) ? 2 : 0;
+        ctx->kernel = ctx->patches_ok ? 2 : 5;
     int maxb = max_blocks_per_sm(ctx->kernel, block, ctx->W);
     if (maxb < 1) maxb = 1;
     int bps = ctx->opts.blocks_per_sm ? (int)ctx->opts.blocks_per_sm : maxb;
@@ -634,7 +665,7 @@ static void choose_schedule(xpbd_ctx* ctx) {
     uint64_t need;
     if (ctx->kernel == 0) need = ((uint64_t)ctx->W.n_tiles * 32 + block - 1) / block;
     else if (ctx->kernel == 2) need = ctx->W.n_patches;
-    else need = (ctx->W.n + block - 1) / block;
+    else need = ((uint64_t)ctx->W.n + block - 1) / block;
     uint32_t grid = (uint32_t)ctx->sms * (uint32_t)bps;
     if (grid > need) grid = (uint32_t)std::max<uint64_t>(1, need);
     ctx->block = block;
@@ -985,7 +1016,7 @@ extern "C" int xpbd_read_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out) {
     if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const ClothHost& h = ctx->cloths[cloth_id];
-    const uint32_t kern = ctx->kernel;
+    const uint32_t kern = ctx->kernel == 5 ? 0u : ctx->kernel;  // rows and tiles share the incidence λ table
     const float* src = kern == 0 ? ctx->W.inc_lambda : (kern == 2 ? ctx->W.patch_lambda : ctx->W.con_lambda);
     const size_t cnt = kern == 0 ? ctx->W.n_inc : (kern == 2 ? ctx->W.patch_con_total : ctx->W.e);
     std::vector<float> all(std::max<size_t>(cnt, 1));
@@ -1070,11 +1101,11 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
     };
     std::vector<Cand> cands;
     const uint32_t blocks[] = {128, 256, 512};
-    const uint32_t jks[2] = {2, 1};
+    const uint32_t jks[3] = {2, 3, 1};
     for (uint32_t jk : jks) {
-        if (base.solver != XPBD_SOLVER_JACOBI && jk == 2) continue;
+        if (base.solver != XPBD_SOLVER_JACOBI && jk != 1) continue;
         if (jk == 2 && !ctx->patches_ok) continue;
-        const uint32_t kid = base.solver == XPBD_SOLVER_JACOBI ? (jk == 2 ? 2u : 0u) : 1u;
+        const uint32_t kid = base.solver == XPBD_SOLVER_JACOBI ? (jk == 2 ? 2u : (jk == 3 ? 5u : 0u)) : 1u;
         for (uint32_t blk : blocks) {
             int maxb = max_blocks_per_sm(kid, blk, ctx->W);
             for (int bps = 1; bps <= maxb; bps *= 2) cands.push_back({blk, (uint32_t)bps, 1, jk});

@@ -359,116 +359,99 @@ __global__ void __launch_bounds__(BLOCK) jacobi_persistent_kernel(XpbdWorld W, u
     }
 }
 
-// ---------------------------------------------------------------------------------------------- Jacobi patches
-// One Jacobi iteration for one spatial patch (a CTA): stage the patch's particles and halo in shared memory, solve
-// each of its constraints once (reference jacobi_edges: Δλ and n̂ = (p_i - p_j)/len), then let every owned
-// particle sum its incidences in neighbour-table order (reference jacobi_gather: (±n̂·w)·Δλ) — bit-identical to the
-// reference with each constraint's square root and divisions evaluated once instead of once per endpoint.
-__device__ __forceinline__ void jacobi_patch(const XpbdWorld& W, const XpbdDevParams& P, uint32_t pid,
-                                             const float4* __restrict__ jin, float4* __restrict__ jout, float4* sm,
-                                             TailMode tail) {
-    const XpbdPatch pt = W.patches[pid];
-    const uint32_t np = pt.np, nl = (uint32_t)pt.np + pt.nh;
-    const uint32_t nc = ((uint32_t)pt.nc_hi << 16) | pt.nc_lo;
-    float4* spos = sm;
-    float4* sres = sm + W.patch_max_local;
-    const uint32_t* parts = W.patch_parts + pt.parts_off;
-    for (uint32_t t = threadIdx.x; t < nl; t += blockDim.x) spos[t] = jin[parts[t]];
-    __syncthreads();
-    const float* pal = W.palette_comp + (uint32_t)pt.cloth * XPBD_PALETTE;
+// ---------------------------------------------------------------------------------------------- Jacobi rows
+// Thread per particle over the neighbour table (no shared memory, full occupancy). Each incidence recomputes its
+// constraint's Δλ exactly as jacobi_edges would (identical from either endpoint); the contributions of four
+// consecutive incidences are evaluated as independent dependency chains and then added in neighbour-table order,
+// so the sum is the reference's sequential one.
+__device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevParams& P, uint32_t i,
+                                           const float4* __restrict__ jin, float4* __restrict__ jout,
+                                           TailMode tail) {
+    const float4 ps = jin[i];
+    if (ps.w <= 0.0f) return;
+    const uint32_t rs = W.row_off[i], re = W.row_off[i + 1];
+    // the palette of the particle's cloth is found through the tile table (tiles are 32-particle aligned per cloth)
     const bool persist = P.lambda_mode != 0u;
-    const uint2* con = W.patch_con + pt.con_off;
-    for (uint32_t c = threadIdx.x; c < nc; c += blockDim.x) {
-        const uint2 rec = con[c];
-        const uint32_t li = rec.x & 0xFFFu, lj = (rec.x >> 12) & 0xFFFu;
-        const float4 pi = spos[li], pj = spos[lj];
-        const F3 gv = sub3(f3(pi), f3(pj));
-        const float len = len3(gv);
-        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
-        bool reset_lam = persist && tail == kTailFinalizePredict;
-        if (!(len < 1e-8f)) {
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    const F3 self = f3(ps);
+    for (uint32_t k = rs; k < re; k += 4) {
+        float cx[4], cy[4], cz[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            cx[u] = cy[u] = cz[u] = 0.0f;
+            const uint32_t kk = k + u;
+            if (kk >= re) continue;
+            const uint2 rec = W.inc[kk];
+            const float4 po = jin[rec.x & XPBD_OTHER_MASK];
+            const F3 gv = sub3(self, f3(po));
+            const float len = len3(gv);
+            if (len < 1e-8f) {
+                if (persist && tail == kTailFinalizePredict) W.inc_lambda[kk] = 0.0f;
+                continue;
+            }
             const F3 nrm = div3(gv, len);
             const float C = __fsub_rn(len, __uint_as_float(rec.y));
-            const float alpha_t = __fmul_rn(pal[(rec.x >> 24) & 0xFu], P.inv_dt_sq);
-            const float wsum = __fadd_rn(__fadd_rn(pi.w, pj.w), alpha_t);
+            const float alpha_t = __fmul_rn(W.palette_comp[W.row_cloth[i] * XPBD_PALETTE + (rec.x >> 28)], P.inv_dt_sq);
+            const float wsum = __fadd_rn(__fadd_rn(ps.w, po.w), alpha_t);
             float dlam = 0.0f;
             if (!(wsum < 1e-8f)) {
-                const float lam = persist ? W.patch_lambda[pt.con_off + c] : 0.0f;
+                const float lam = persist ? W.inc_lambda[kk] : 0.0f;
                 dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
-                if (persist) {
-                    W.patch_lambda[pt.con_off + c] = reset_lam ? 0.0f : __fadd_rn(lam, dlam);
-                    reset_lam = false;
-                }
+                if (persist) W.inc_lambda[kk] = (tail == kTailFinalizePredict) ? 0.0f : __fadd_rn(lam, dlam);
+            } else if (persist && tail == kTailFinalizePredict) {
+                W.inc_lambda[kk] = 0.0f;
             }
-            r = make_float4(nrm.x, nrm.y, nrm.z, dlam);
+            cx[u] = __fmul_rn(__fmul_rn(nrm.x, ps.w), dlam);
+            cy[u] = __fmul_rn(__fmul_rn(nrm.y, ps.w), dlam);
+            cz[u] = __fmul_rn(__fmul_rn(nrm.z, ps.w), dlam);
         }
-        if (reset_lam) W.patch_lambda[pt.con_off + c] = 0.0f;
-        sres[c] = r;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u < re) {
+                ax = __fadd_rn(ax, cx[u]);
+                ay = __fadd_rn(ay, cy[u]);
+                az = __fadd_rn(az, cz[u]);
+            }
     }
-    __syncthreads();
-    const uint32_t* gofs = W.patch_gofs + pt.gofs_off;
-    for (uint32_t k = threadIdx.x; k < np; k += blockDim.x) {
-        const float4 ps = spos[k];
-        if (ps.w <= 0.0f) continue;  // pinned: both buffers already hold the fixed position
-        const uint32_t q0 = gofs[k], q1 = gofs[k + 1];
-        float ax = 0.0f, ay = 0.0f, az = 0.0f;
-        for (uint32_t q = q0; q < q1; ++q) {
-            const uint32_t sl = W.patch_slots[q];
-            const float4 r = sres[sl & 0x7FFFu];
-            const float nx = (sl & 0x8000u) ? -r.x : r.x;
-            const float ny = (sl & 0x8000u) ? -r.y : r.y;
-            const float nz = (sl & 0x8000u) ? -r.z : r.z;
-            ax = __fadd_rn(ax, __fmul_rn(__fmul_rn(nx, ps.w), r.w));
-            ay = __fadd_rn(ay, __fmul_rn(__fmul_rn(ny, ps.w), r.w));
-            az = __fadd_rn(az, __fmul_rn(__fmul_rn(nz, ps.w), r.w));
-        }
-        F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
-        if (P.relaxation == 1u && q1 > q0) delta = div3(delta, (float)(q1 - q0));
-        delta = clamp_correction(delta);
-        F3 xn = add3(f3(ps), delta);
-        const uint32_t g = parts[k];
-        if (tail == kTailNone) {
-            jout[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
-            continue;
-        }
-        const F3 xo = f3(W.x[g]);
-        F3 vel = f3(W.v[g]);
-        xn = finalize_particle(xn, xo, vel, P, W.status);
-        W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
-        W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
-        if (tail == kTailFinalizePredict) {
-            const F3 pos = predict_particle(g, xn, vel, P);
-            jout[g] = make_float4(pos.x, pos.y, pos.z, ps.w);
-        } else {
-            jout[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
-        }
+    F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
+    if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
+    delta = clamp_correction(delta);
+    F3 xn = add3(self, delta);
+    if (tail == kTailNone) {
+        jout[i] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        return;
     }
-    __syncthreads();
+    const F3 xo = f3(W.x[i]);
+    F3 vel = f3(W.v[i]);
+    xn = finalize_particle(xn, xo, vel, P, W.status);
+    W.x[i] = make_float4(xn.x, xn.y, xn.z, ps.w);
+    W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+    if (tail == kTailFinalizePredict) {
+        const F3 pos = predict_particle(i, xn, vel, P);
+        jout[i] = make_float4(pos.x, pos.y, pos.z, ps.w);
+    } else {
+        jout[i] = make_float4(xn.x, xn.y, xn.z, ps.w);
+    }
 }
 
-// Persistent Jacobi over spatial patches; same flags / buffer protocol as jacobi_persistent_kernel.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) jacobi_patch_kernel(XpbdWorld W, uint32_t flags, uint32_t substeps,
-                                                             uint32_t pend, uint32_t start) {
-    extern __shared__ float4 s_patch[];
+__global__ void __launch_bounds__(BLOCK) jacobi_row_kernel(XpbdWorld W, uint32_t flags, uint32_t substeps,
+                                                           uint32_t pend, uint32_t start) {
     if (!status_clear(W)) return;
     const XpbdDevParams P = *W.params;
     const bool persist = P.lambda_mode != 0u;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
     predict_phase(W, P, (flags & kBeginFinalize) != 0u, pend, start, true);
-    if (persist) {  // λ of every patch constraint slot starts the substep at zero
-        const uint32_t stride = gridDim.x * blockDim.x;
-        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < W.patch_con_total; k += stride)
-            W.patch_lambda[k] = 0.0f;
-    }
+    if (persist)
+        for (uint32_t k = gtid; k < W.n_inc; k += gstride) W.inc_lambda[k] = 0.0f;
     if (!grid_barrier(W, P)) return;
     uint32_t b = start;
     const uint32_t I = P.iterations;
     for (uint32_t s = 0; s < substeps; ++s) {
         const bool last_sub = (s + 1 == substeps);
         if (I == 0) {
-            const uint32_t stride = gridDim.x * blockDim.x;
             const bool fin = !last_sub || (flags & kEndFinalize);
-            for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n && fin; i += stride) {
+            for (uint32_t i = gtid; i < W.n && fin; i += gstride) {
                 float4 p4 = W.jac[b][i];
                 if (p4.w <= 0.0f) continue;
                 const F3 xo = f3(W.x[i]);
@@ -492,13 +475,268 @@ __global__ void __launch_bounds__(BLOCK) jacobi_patch_kernel(XpbdWorld W, uint32
                 if (!last_sub) tail = kTailFinalizePredict;
                 else if (flags & kEndFinalize) tail = kTailFinalize;
             }
-            for (uint32_t pid = blockIdx.x; pid < W.n_patches; pid += gridDim.x)
-                jacobi_patch(W, P, pid, jin, jout, s_patch, tail);
+            for (uint32_t i = gtid; i < W.n; i += gstride) jacobi_row(W, P, i, jin, jout, tail);
             const bool very_last = last_sub && (k + 1 == I);
             if (!very_last && !grid_barrier(W, P)) return;
         }
         b = (b + I) & 1u;
     }
+}
+
+// ---------------------------------------------------------------------------------------------- Jacobi patches
+// Each CTA walks its patches (pid = blockIdx.x + m*gridDim.x). Per patch: (1) the patch's table blob was fetched into
+// shared memory by one TMA bulk copy issued one patch ahead (cp.async.bulk, completion on an mbarrier, L2 evict-first
+// so the streamed tables do not push the particle buffers out of L2); (2) its particles + halo were gathered into
+// shared memory with cp.async while the previous patch was finishing; (3) every constraint is solved once
+// (reference jacobi_edges: Δλ and n̂ = (p_i - p_j)/len) into shared memory; (4) each owned particle sums its
+// incidences in neighbour-table order (reference jacobi_gather: (±n̂·w)·Δλ) — bit-identical to the reference, with
+// each constraint's square root and divisions evaluated once instead of once per endpoint.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init1(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s_evict_first(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "{\n\t.reg .b64 pol;\n\tcreatepolicy.fractional.L2::evict_first.b64 pol, 1.0;\n\t"
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], pol;"
+        "\n\t}" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+// Bounded wait on phase `parity`; false when the limit was reached.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_addr(bar);
+    for (uint32_t it = 0; it < (1u << 26); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t align16(uint32_t b) { return (b + 15u) & ~15u; }
+
+struct PatchView {
+    const uint32_t* parts;
+    const uint2* con;
+    const uint32_t* gofs;
+    const uint16_t* slots;
+};
+__device__ __forceinline__ PatchView patch_view(const unsigned char* blob, const XpbdPatch& pt) {
+    PatchView v;
+    const uint32_t nl = (uint32_t)pt.np + pt.nh;
+    v.parts = reinterpret_cast<const uint32_t*>(blob);
+    const unsigned char* c = blob + align16(4u * nl);
+    v.con = reinterpret_cast<const uint2*>(c);
+    const unsigned char* g = c + align16(8u * pt.nc);
+    v.gofs = reinterpret_cast<const uint32_t*>(g);
+    v.slots = reinterpret_cast<const uint16_t*>(g + align16(4u * ((uint32_t)pt.np + 1u)));
+    return v;
+}
+
+__device__ __forceinline__ void patch_constraints(const XpbdWorld& W, const XpbdDevParams& P, const XpbdPatch& pt,
+                                                  const PatchView& v, const float4* __restrict__ spos,
+                                                  float4* __restrict__ sres, TailMode tail) {
+    const float* pal = W.palette_comp + (uint32_t)pt.cloth * XPBD_PALETTE;
+    const bool persist = P.lambda_mode != 0u;
+#pragma unroll 2
+    for (uint32_t c = threadIdx.x; c < pt.nc; c += blockDim.x) {
+        const uint2 rec = v.con[c];
+        const float4 pi = spos[rec.x & 0xFFFu], pj = spos[(rec.x >> 12) & 0xFFFu];
+        const F3 gv = sub3(f3(pi), f3(pj));
+        const float len = len3(gv);
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool reset_lam = persist && tail == kTailFinalizePredict;
+        if (!(len < 1e-8f)) {
+            const F3 nrm = div3(gv, len);
+            const float C = __fsub_rn(len, __uint_as_float(rec.y));
+            const float alpha_t = __fmul_rn(pal[(rec.x >> 24) & 0xFu], P.inv_dt_sq);
+            const float wsum = __fadd_rn(__fadd_rn(pi.w, pj.w), alpha_t);
+            float dlam = 0.0f;
+            if (!(wsum < 1e-8f)) {
+                const float lam = persist ? W.patch_lambda[pt.lam_off + c] : 0.0f;
+                dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
+                if (persist) {
+                    W.patch_lambda[pt.lam_off + c] = reset_lam ? 0.0f : __fadd_rn(lam, dlam);
+                    reset_lam = false;
+                }
+            }
+            r = make_float4(nrm.x, nrm.y, nrm.z, dlam);
+        }
+        if (reset_lam) W.patch_lambda[pt.lam_off + c] = 0.0f;
+        sres[c] = r;
+    }
+}
+
+__device__ __forceinline__ void patch_gather(const XpbdWorld& W, const XpbdDevParams& P, const XpbdPatch& pt,
+                                             const PatchView& v, const float4* spos, const float4* sres,
+                                             float4* __restrict__ jout, TailMode tail) {
+    for (uint32_t k = threadIdx.x; k < pt.np; k += blockDim.x) {
+        const float4 ps = spos[k];
+        if (ps.w <= 0.0f) continue;  // pinned: both buffers already hold the fixed position
+        const uint32_t q0 = v.gofs[k], q1 = v.gofs[k + 1];
+        float ax = 0.0f, ay = 0.0f, az = 0.0f;
+        for (uint32_t q = q0; q < q1; ++q) {
+            const uint32_t sl = v.slots[q];
+            const float4 r = sres[sl & 0x7FFFu];
+            const bool neg = (sl & 0x8000u) != 0u;
+            ax = __fadd_rn(ax, __fmul_rn(__fmul_rn(neg ? -r.x : r.x, ps.w), r.w));
+            ay = __fadd_rn(ay, __fmul_rn(__fmul_rn(neg ? -r.y : r.y, ps.w), r.w));
+            az = __fadd_rn(az, __fmul_rn(__fmul_rn(neg ? -r.z : r.z, ps.w), r.w));
+        }
+        F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
+        if (P.relaxation == 1u && q1 > q0) delta = div3(delta, (float)(q1 - q0));
+        delta = clamp_correction(delta);
+        F3 xn = add3(f3(ps), delta);
+        const uint32_t g = v.parts[k];
+        if (tail == kTailNone) {
+            jout[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+            continue;
+        }
+        const F3 xo = f3(W.x[g]);
+        F3 vel = f3(W.v[g]);
+        xn = finalize_particle(xn, xo, vel, P, W.status);
+        W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+        if (tail == kTailFinalizePredict) {
+            const F3 pos = predict_particle(g, xn, vel, P);
+            jout[g] = make_float4(pos.x, pos.y, pos.z, ps.w);
+        } else {
+            jout[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        }
+    }
+}
+
+// Persistent Jacobi over spatial patches; same flags / buffer protocol as jacobi_persistent_kernel. Shared memory:
+// two blob buffers, two particle buffers, one constraint-result buffer, two mbarriers.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) jacobi_patch_kernel(XpbdWorld W, uint32_t flags, uint32_t substeps,
+                                                             uint32_t pend, uint32_t start) {
+    extern __shared__ __align__(128) unsigned char s_dyn[];
+    if (!status_clear(W)) return;
+    const XpbdDevParams P = *W.params;
+    const bool persist = P.lambda_mode != 0u;
+    unsigned char* blob[2] = {s_dyn, s_dyn + W.patch_max_blob};
+    float4* spos[2] = {reinterpret_cast<float4*>(s_dyn + 2 * W.patch_max_blob),
+                       reinterpret_cast<float4*>(s_dyn + 2 * W.patch_max_blob) + W.patch_max_local};
+    float4* sres = spos[1] + W.patch_max_local;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sres + W.patch_max_con);
+    if (threadIdx.x == 0) {
+        mbar_init1(&bars[0]);
+        mbar_init1(&bars[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase[2] = {0u, 0u};
+    bool inflight[2] = {false, false};                   // issued and not yet waited for
+    uint32_t bsel = 0;                                   // blob buffer of the current patch
+    const uint32_t mine = W.n_patches > blockIdx.x ? (W.n_patches - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    auto issue_blob = [&](uint32_t m, uint32_t b) {      // my m-th patch (of any iteration) into buffer b
+        const XpbdPatch& pt = W.patches[blockIdx.x + (m % mine) * gridDim.x];
+        if (threadIdx.x == 0) bulk_g2s_evict_first(blob[b], W.patch_blob + pt.off16, pt.bytes, &bars[b]);
+        inflight[b] = true;
+    };
+    bool failed = false;
+    auto wait_blob = [&](uint32_t b) {
+        if (!mbar_wait_bounded(&bars[b], phase[b])) {
+            failed = true;
+            if (threadIdx.x == 0) set_status(W.status, XPBD_DEV_BARRIER_TIMEOUT);
+        }
+        inflight[b] = false;
+    };
+    if (mine > 0 && (*W.params).iterations > 0 && substeps > 0) issue_blob(0, 0);
+
+    predict_phase(W, P, (flags & kBeginFinalize) != 0u, pend, start, true);
+    if (persist) {  // λ of every patch constraint slot starts the substep at zero
+        const uint32_t stride = gridDim.x * blockDim.x;
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < W.patch_con_total; k += stride)
+            W.patch_lambda[k] = 0.0f;
+    }
+    bool ok = grid_barrier(W, P);
+    uint32_t b = start;
+    const uint32_t I = P.iterations;
+    uint32_t seq = 0;  // running index of my processed patches (blob pipeline position)
+    for (uint32_t s = 0; s < substeps && ok; ++s) {
+        const bool last_sub = (s + 1 == substeps);
+        if (I == 0) {
+            const uint32_t stride = gridDim.x * blockDim.x;
+            const bool fin = !last_sub || (flags & kEndFinalize);
+            for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n && fin; i += stride) {
+                float4 p4 = W.jac[b][i];
+                if (p4.w <= 0.0f) continue;
+                const F3 xo = f3(W.x[i]);
+                F3 vel = f3(W.v[i]);
+                F3 xn = finalize_particle(f3(p4), xo, vel, P, W.status);
+                W.x[i] = make_float4(xn.x, xn.y, xn.z, p4.w);
+                W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+                if (!last_sub) {
+                    F3 pos = predict_particle(i, xn, vel, P);
+                    W.jac[b][i] = make_float4(pos.x, pos.y, pos.z, p4.w);
+                }
+            }
+            if (!last_sub) ok = grid_barrier(W, P);
+            continue;
+        }
+        for (uint32_t k = 0; k < I && ok; ++k) {
+            const float4* jin = W.jac[(b + k) & 1u];
+            float4* jout = W.jac[(b + k + 1) & 1u];
+            TailMode tail = kTailNone;
+            if (k + 1 == I) {
+                if (!last_sub) tail = kTailFinalizePredict;
+                else if (flags & kEndFinalize) tail = kTailFinalize;
+            }
+            const bool very_last = last_sub && (k + 1 == I);
+            uint32_t ps = 0;
+            for (uint32_t m = 0; m < mine && !failed; ++m, ++seq) {
+                const XpbdPatch pt = W.patches[blockIdx.x + m * gridDim.x];
+                const uint32_t nl = (uint32_t)pt.np + pt.nh;
+                wait_blob(bsel);
+                phase[bsel] ^= 1u;
+                const PatchView v = patch_view(blob[bsel], pt);
+                // the next patch's blob (also across the iteration boundary; not after the launch's last patch)
+                const bool more = (m + 1 < mine) || !very_last;
+                if (more) issue_blob(seq + 1, bsel ^ 1u);
+                if (m == 0) {
+                    for (uint32_t t = threadIdx.x; t < nl; t += blockDim.x) spos[ps][t] = jin[v.parts[t]];
+                } else {
+                    cp_async_wait_all();
+                }
+                __syncthreads();
+                patch_constraints(W, P, pt, v, spos[ps], sres, tail);
+                __syncthreads();
+                if (m + 1 < mine) {  // gather the next patch's particles while this one finishes
+                    const XpbdPatch pn = W.patches[blockIdx.x + (m + 1) * gridDim.x];
+                    wait_blob(bsel ^ 1u);
+                    const PatchView vn = patch_view(blob[bsel ^ 1u], pn);
+                    const uint32_t nln = (uint32_t)pn.np + pn.nh;
+                    for (uint32_t t = threadIdx.x; t < nln; t += blockDim.x) cp_async16(&spos[ps ^ 1u][t], jin + vn.parts[t]);
+                    cp_async_commit();
+                }
+                patch_gather(W, P, pt, v, spos[ps], sres, jout, tail);
+                __syncthreads();
+                bsel ^= 1u;
+                ps ^= 1u;
+            }
+            if (failed) break;
+            if (!very_last) ok = grid_barrier(W, P);
+        }
+        b = (b + I) & 1u;
+    }
+    // no copy may still target this CTA's shared memory when it exits (bounded waits)
+    for (uint32_t q = 0; q < 2; ++q)
+        if (inflight[q]) mbar_wait_bounded(&bars[q], phase[q]);
+    cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------------------------- Gauss–Seidel
@@ -600,9 +838,11 @@ static const void* jacobi_fn() { return (const void*)jacobi_persistent_kernel<BL
 template <int BLOCK>
 static const void* patch_fn() { return (const void*)jacobi_patch_kernel<BLOCK>; }
 template <int BLOCK>
+static const void* row_fn() { return (const void*)jacobi_row_kernel<BLOCK>; }
+template <int BLOCK>
 static const void* gs_fn() { return (const void*)gs_persistent_kernel<BLOCK>; }
 
-// solver 0: Jacobi over warp tiles, 1: Gauss–Seidel, 2: Jacobi over spatial patches
+// kernel 0: Jacobi over warp tiles, 1: Gauss–Seidel, 2: Jacobi over spatial patches, 5: Jacobi thread per particle
 const void* solver_kernel_fn(uint32_t solver, uint32_t block) {
     switch (solver * 10000 + block) {
         case 128: return jacobi_fn<128>();
@@ -617,13 +857,18 @@ const void* solver_kernel_fn(uint32_t solver, uint32_t block) {
         case 20256: return patch_fn<256>();
         case 20512: return patch_fn<512>();
         case 21024: return patch_fn<1024>();
+        case 50128: return row_fn<128>();
+        case 50256: return row_fn<256>();
+        case 50512: return row_fn<512>();
+        case 51024: return row_fn<1024>();
     }
     return nullptr;
 }
 
 static size_t solver_dyn_smem(uint32_t solver, uint32_t block, const XpbdWorld& W) {
     if (solver == 0) return (size_t)(block / 32) * 3 * kTileChunk * sizeof(float);
-    if (solver == 2) return ((size_t)W.patch_max_local + W.patch_max_con) * sizeof(float4);
+    if (solver == 2)
+        return 2 * (size_t)W.patch_max_blob + (2 * (size_t)W.patch_max_local + W.patch_max_con) * sizeof(float4) + 16;
     return 0;
 }
 

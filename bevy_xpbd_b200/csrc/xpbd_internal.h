@@ -54,17 +54,20 @@ struct XpbdTile {
 };
 
 // Spatial patch of the Jacobi solve: `np` owned particles (a recursive-coordinate-bisection block of one cloth) and
-// `nh` halo particles read by its constraints. Local particle index: owned [0, np), halo [np, np+nh).
-//   parts[parts_off ...]      np owned then nh halo global particle indices
-//   con[con_off ...]          nc records {li | lj<<12 | palette<<24, rest bits}: every constraint with an owned
-//                             endpoint (not both pinned), each solved once per patch per iteration
-//   gofs[gofs_off ... + np]   per owned particle: range in `slots` of its incidences in neighbour-table order;
-//                             slot = local constraint index | 0x8000 when the particle is the constraint's j
+// `nh` halo particles read by its constraints. Local particle index: owned [0, np), halo [np, np+nh). All tables of
+// a patch form one contiguous 16-byte aligned blob (fetched with one TMA bulk copy), sections 16-byte aligned:
+//   parts[np+nh]   u32 global particle index (owned, then halo)
+//   con[nc]        {li | lj<<12 | palette<<24, rest bits}: every constraint with an owned unpinned endpoint, solved
+//                  once per patch per iteration
+//   gofs[np+1]     per owned particle: range in `slots` of its incidences in neighbour-table order
+//   slots[nslot]   u16 local constraint index | 0x8000 when the particle is the constraint's j endpoint
 struct XpbdPatch {
-    uint32_t parts_off, con_off, gofs_off;
+    uint32_t off16;    // blob offset in 16-byte units
+    uint32_t bytes;    // blob size (multiple of 16)
+    uint32_t nc;       // constraints
+    uint32_t lam_off;  // first λ slot of this patch's constraints
     uint16_t np, nh;
-    uint16_t nc_hi, cloth;  // nc = nc_hi << 16 | nc_lo
-    uint16_t nc_lo, pad;
+    uint16_t cloth, pad;
 };
 #define XPBD_PATCH_LOCAL_BITS 12
 #define XPBD_PATCH_MAX_LOCAL (1u << XPBD_PATCH_LOCAL_BITS)
@@ -80,6 +83,7 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     const uint2* inc;
     float* inc_lambda;
     const XpbdTile* tiles;
+    const uint16_t* row_cloth;      // per particle: cloth index (palette row)
     const float* palette_comp;
     const uint4* con;
     float* con_lambda;
@@ -89,11 +93,8 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     int* status;
     XpbdGridSync* sync;
     // patch-staged Jacobi
-    uint32_t n_patches, patch_max_local, patch_max_con, patch_con_total;
+    uint32_t n_patches, patch_max_local, patch_max_con, patch_con_total, patch_max_blob;
     const XpbdPatch* patches;
-    const uint32_t* patch_parts;
-    const uint2* patch_con;
-    const uint32_t* patch_gofs;
-    const uint16_t* patch_slots;
+    const uint4* patch_blob;
     float* patch_lambda;
 };

@@ -98,7 +98,7 @@ typedef struct xpbd_solver_opts {
     uint32_t blocks_per_sm;           /* 0 = autotuned / default */
     uint32_t warm_start;              /* 1: learned λ warm start (requires XPBD_LAMBDA_PER_SUBSTEP) */
     uint32_t cluster_ctas;            /* Gauss–Seidel in one thread-block cluster: 0 auto, 1 off, 8 or 16 CTAs */
-    uint32_t jacobi_kernel;           /* Jacobi execution: 0 auto, 1 warp tiles, 2 shared-memory spatial patches */
+    uint32_t jacobi_kernel;           /* Jacobi: 0 auto, 1 warp tiles, 2 shared-memory patches, 3 thread per particle */
     uint32_t reserved[4];
 } xpbd_solver_opts;
 
@@ -135,7 +135,8 @@ typedef struct xpbd_stats {
     uint64_t kernel_launches;         /* launches issued by the library so far (graph nodes count once each) */
     uint64_t warm_start_fallbacks;    /* substeps where the learned warm start was rejected */
     uint64_t collision_pairs;         /* pairs found by the last collision pass (when counted) */
-    uint32_t solver_kernel;           /* 0 Jacobi warp tiles, 1 Gauss–Seidel grid, 2 Jacobi patches, 3 GS cluster */
+    uint32_t solver_kernel;           /* 0 Jacobi warp tiles, 1 Gauss–Seidel grid, 2 Jacobi patches, 3 GS cluster,
+                                         5 Jacobi thread per particle */
     uint32_t cluster_ctas;            /* CTAs of the Gauss–Seidel cluster (0 = grid kernel) */
 } xpbd_stats;
 

@@ -331,7 +331,7 @@ def test_gauss_seidel_execution_paths_bit_exact(cluster):
     assert max_abs(plug2.positions(), o2.state()[0]) == 0.0
 
 
-@pytest.mark.parametrize("kernel", [1, 2], ids=["warp_tiles", "spatial_patches"])
+@pytest.mark.parametrize("kernel", [1, 2, 3], ids=["warp_tiles", "spatial_patches", "thread_rows"])
 @pytest.mark.parametrize("lam", [P.LAMBDA_RESET_PER_ITERATION, P.LAMBDA_PER_SUBSTEP], ids=["lambda_reset", "lambda_substep"])
 def test_jacobi_execution_paths_bit_exact(kernel, lam):
     """Both Jacobi executions — warp tiles over the neighbour table and shared-memory spatial patches that solve each
