@@ -31,7 +31,10 @@ EXPORTED = [
     "xpbd_get_stats", "xpbd_get_coloring", "xpbd_autotune", "xpbd_collision_keys", "xpbd_collision_pairs",
     "xpbd_radix_sort_scratch_bytes", "xpbd_radix_sort_pairs", "xpbd_hash_keys", "xpbd_last_error",
     "xpbd_status_string", "xpbd_debug_force_barrier_timeout", "xpbd_color_constraints",
+    "xpbd_radix_sort_pairs_noalloc",
 ]
+NOALLOC_SORT_MAX_KEYS = 1 << 18
+ERR_CAPACITY = -9
 
 
 class TimeStepParams(C.Structure):
@@ -116,6 +119,7 @@ def load():
         "xpbd_status_string": (C.c_char_p, [I]),
         "xpbd_debug_force_barrier_timeout": (I, [P, C.c_float]),
         "xpbd_color_constraints": (I, [U, U, P, P, U, P, P, C.POINTER(U)]),
+        "xpbd_radix_sort_pairs_noalloc": (I, [P, P, P, P, U, U, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -13,6 +13,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
+#include "../../include/xpbd_cuda.h"
 #include "xpbd_internal.h"
 #include "xpbd_kernels.h"
 
@@ -187,6 +190,36 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
         src_v = dv;
     }
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------- sort, no allocation
+// Scratch of the allocation-free sort: a file-scope device array sized for XPBD_NOALLOC_SORT_MAX_KEYS keys (per-tile
+// digit counts + the ping-pong key/value buffers), held by every GPU that loads the library until the process exits.
+constexpr size_t noalloc_scratch_bytes(uint32_t n) {
+    return ((256 * (size_t)((n + kSortTile - 1) / kSortTile) * sizeof(uint32_t) + 255) & ~(size_t)255) +
+           ((2 * (size_t)n * sizeof(uint32_t) + 255) & ~(size_t)255) + 256;
+}
+constexpr size_t kNoAllocScratchBytes = noalloc_scratch_bytes(XPBD_NOALLOC_SORT_MAX_KEYS);
+static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[kNoAllocScratchBytes];
+
+// Device address of the scratch array on the current device. The array's name is only a host-side stand-in, so the
+// address is looked up once per device (with that device current) and cached.
+static cudaError_t noalloc_scratch(void** out) {
+    static std::mutex mu;
+    static void* cache[64] = {nullptr};
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!cache[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
+        if (e != cudaSuccess) return e;
+        cache[dev] = p;
+    }
+    *out = cache[dev];
+    return cudaSuccess;
 }
 
 cudaError_t launch_hash_keys(const float4* x, uint32_t n, float inv_cell, uint32_t bits, uint32_t* keys,
@@ -446,3 +479,19 @@ cudaError_t collision_pairs(const XpbdWorld& W, const float4* pos, const Collisi
 }
 
 }  // namespace xpbd
+
+extern "C" int xpbd_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                             uint32_t* vals_out, uint32_t n, uint32_t passes, void* stream) {
+    if (n && (!keys_in || !vals_in || !keys_out || !vals_out)) return XPBD_ERR_INVALID_ARGUMENT;
+    if (passes < 1 || passes > 4) return XPBD_ERR_INVALID_ARGUMENT;
+    if (keys_in == keys_out || vals_in == vals_out) return XPBD_ERR_INVALID_ARGUMENT;
+    if (n > XPBD_NOALLOC_SORT_MAX_KEYS) return XPBD_ERR_CAPACITY;
+    if (n == 0) return XPBD_OK;
+    void* scratch = nullptr;
+    if (xpbd::noalloc_scratch(&scratch) != cudaSuccess) return XPBD_ERR_CUDA;
+    // nothing in the scratch must start at zero: each pass writes every digit count and every ping-pong word
+    // before reading it, so the previous call's contents are harmless
+    cudaError_t e = xpbd::radix_sort_pairs(keys_in, vals_in, keys_out, vals_out, n, passes, scratch,
+                                           xpbd::kNoAllocScratchBytes, (cudaStream_t)stream, nullptr);
+    return e == cudaSuccess ? XPBD_OK : XPBD_ERR_CUDA;
+}

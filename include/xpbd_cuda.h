@@ -212,6 +212,17 @@ int xpbd_collision_pairs(xpbd_ctx* ctx, uint32_t* pairs, uint64_t cap, uint64_t*
 size_t xpbd_radix_sort_scratch_bytes(uint32_t n);
 int xpbd_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
                           uint32_t n, uint32_t passes, void* scratch, size_t scratch_bytes, void* stream);
+/* The same sort for callers that cannot allocate device memory — e.g. code running where cudaMalloc is forbidden
+ * or would stall (inside a frame budget where its implicit device synchronisation is not acceptable, under a host
+ * application that reserves all device memory through its own pool, or in a plugin that may not grow the process's
+ * footprint). No counterpart in the reference. It allocates nothing: its scratch is a fixed device array built into
+ * the library, sized for at most XPBD_NOALLOC_SORT_MAX_KEYS keys (about 2.2 MB, held on every GPU that loads the
+ * library until the process exits); larger n returns XPBD_ERR_CAPACITY. The first call on a device looks up the
+ * array's device address (make it before any stream capture on that device). Every call shares the one array, so
+ * calls whose work overlaps on the GPU (other streams, other host threads) race; serialise them. */
+#define XPBD_NOALLOC_SORT_MAX_KEYS (1u << 18)
+int xpbd_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                  uint32_t* vals_out, uint32_t n, uint32_t passes, void* stream);
 /* keys[i] = prime-hash(floor(xyz_i * inv_cell)) & (2^bits - 1), positions as float4 (w ignored). */
 int xpbd_hash_keys(const float* xyzw, uint32_t n, float inv_cell, uint32_t table_bits, uint32_t* keys,
                    void* stream);
