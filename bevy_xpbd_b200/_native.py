@@ -31,8 +31,14 @@ EXPORTED = [
     "xpbd_get_stats", "xpbd_get_coloring", "xpbd_autotune", "xpbd_collision_keys", "xpbd_collision_pairs",
     "xpbd_radix_sort_scratch_bytes", "xpbd_radix_sort_pairs", "xpbd_hash_keys", "xpbd_last_error",
     "xpbd_status_string", "xpbd_debug_force_barrier_timeout", "xpbd_color_constraints",
-    "xpbd_radix_sort_pairs_noalloc",
+    "xpbd_radix_sort_pairs_noalloc", "xpbd_set_warm_lambda", "xpbd_mlp_init", "xpbd_mlp_set_params",
+    "xpbd_mlp_get_params", "xpbd_mlp_collect", "xpbd_mlp_dataset_size", "xpbd_mlp_dataset_read",
+    "xpbd_mlp_fit_normalization", "xpbd_mlp_train", "xpbd_mlp_eval", "xpbd_mlp_gradients", "xpbd_mlp_predict_lambda",
+    "xpbd_converge_history",
 ]
+MLP_PARAMS = 4865
+MLP_NORM = 20
+MLP_FEATURES = 9
 NOALLOC_SORT_MAX_KEYS = 1 << 18
 ERR_CAPACITY = -9
 
@@ -53,7 +59,7 @@ class SolverOpts(C.Structure):
         ("ring_depth", C.c_uint32), ("ground_enabled", C.c_uint32), ("ground_y", C.c_float),
         ("use_graphs", C.c_uint32), ("barrier_timeout_ms", C.c_float), ("block_threads", C.c_uint32),
         ("blocks_per_sm", C.c_uint32), ("warm_start", C.c_uint32), ("cluster_ctas", C.c_uint32),
-        ("jacobi_kernel", C.c_uint32), ("reserved", C.c_uint32 * 4),
+        ("jacobi_kernel", C.c_uint32), ("tolerance", C.c_float), ("reserved", C.c_uint32 * 3),
     ]
 
 
@@ -74,6 +80,8 @@ class Stats(C.Structure):
         ("grid_blocks", C.c_uint32), ("block_threads", C.c_uint32), ("graph_captured", C.c_uint32),
         ("cooperative_launch", C.c_uint32), ("kernel_launches", C.c_uint64), ("warm_start_fallbacks", C.c_uint64),
         ("collision_pairs", C.c_uint64), ("solver_kernel", C.c_uint32), ("cluster_ctas", C.c_uint32),
+        ("converge_iterations", C.c_uint64), ("converge_substeps", C.c_uint64),
+        ("converge_max_iterations", C.c_uint32), ("pad", C.c_uint32),
     ]
 
 
@@ -120,6 +128,19 @@ def load():
         "xpbd_debug_force_barrier_timeout": (I, [P, C.c_float]),
         "xpbd_color_constraints": (I, [U, U, P, P, U, P, P, C.POINTER(U)]),
         "xpbd_radix_sort_pairs_noalloc": (I, [P, P, P, P, U, U, P]),
+        "xpbd_set_warm_lambda": (I, [P, U, P]),
+        "xpbd_mlp_init": (I, [P, C.c_uint64, U]),
+        "xpbd_mlp_set_params": (I, [P, P, P]),
+        "xpbd_mlp_get_params": (I, [P, P, P]),
+        "xpbd_mlp_collect": (I, [P, U, U]),
+        "xpbd_mlp_dataset_size": (I, [P, C.POINTER(U)]),
+        "xpbd_mlp_dataset_read": (I, [P, U, P, P, C.POINTER(U)]),
+        "xpbd_mlp_fit_normalization": (I, [P]),
+        "xpbd_mlp_train": (I, [P, U, U, C.c_float, C.c_uint64, P]),
+        "xpbd_mlp_eval": (I, [P, P, U, P]),
+        "xpbd_mlp_gradients": (I, [P, P, P, U, P, P]),
+        "xpbd_mlp_predict_lambda": (I, [P, U, P]),
+        "xpbd_converge_history": (I, [P, P, U, C.POINTER(U)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -38,6 +38,7 @@ struct ClothHost {
     std::vector<uint32_t> lambda_inc;  // per input constraint: incidence holding its λ (Jacobi), or UINT32_MAX
     std::vector<uint32_t> lambda_gs;   // per input constraint: position in the color-major table
     std::vector<uint32_t> lambda_patch;  // per input constraint: patch slot holding its λ, or UINT32_MAX
+    std::vector<uint32_t> inc_i, inc_j;  // per input constraint: incidence in the i / j particle's row (or MAX)
 };
 
 struct DeviceBuf {
@@ -46,6 +47,9 @@ struct DeviceBuf {
 };
 
 }  // namespace
+
+// bench.py counts this block as the per-step host→device bytes of the end-to-end path
+static_assert(sizeof(XpbdDevParams) == 120, "update DEV_PARAMS_BYTES in bench.py");
 
 struct xpbd_ctx {
     int device = 0;
@@ -87,6 +91,14 @@ struct xpbd_ctx {
     int* d_status_copy = nullptr;
     xpbd_stats stats{};
     std::string last_error;
+    // warm-start MLP
+    XpbdMlp* d_mlp = nullptr;
+    float *d_master = nullptr, *d_m1 = nullptr, *d_m2 = nullptr, *d_grads = nullptr, *d_loss = nullptr;
+    float *d_feat = nullptr, *d_scale = nullptr, *d_target = nullptr;
+    uint32_t* d_idx = nullptr;
+    uint32_t idx_cap = 0, ds_count = 0, ds_cap = 0, collect_offset = 0;
+    uint64_t adam_step = 0;
+    float norm[XPBD_MLP_NORM] = {0};
     float forced_timeout_ms = 0.f;
 };
 
@@ -156,6 +168,9 @@ static void fill_dev_params(xpbd_ctx* ctx) {
     float tmo = ctx->forced_timeout_ms > 0.f ? ctx->forced_timeout_ms
                                              : (o.barrier_timeout_ms > 0.f ? o.barrier_timeout_ms : 2000.f);
     p.barrier_timeout_ns = (unsigned long long)((double)tmo * 1e6);
+    p.tolerance = o.tolerance;
+    p.max_iterations = t.inner_iterations;
+    if (o.tolerance > 0.f || o.warm_start) p.lambda_mode = XPBD_LAMBDA_PER_SUBSTEP;
 }
 
 extern "C" void xpbd_default_opts(xpbd_solver_opts* o) {
@@ -366,6 +381,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
                 for (uint32_t k = 0; k < c.e; ++k) c.lambda_patch[c.perm[k]] = slot[k];
         }
         c.lambda_inc.assign(c.e, 0xFFFFFFFFu);
+        c.inc_i.assign(c.e, 0xFFFFFFFFu);
+        c.inc_j.assign(c.e, 0xFFFFFFFFu);
         for (uint32_t i = 0; i < c.n; ++i) {
             const uint32_t g = c.vtx_off + i;
             row_off[g] = (uint32_t)inc.size();
@@ -375,6 +392,7 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
                 uint32_t rb;
                 memcpy(&rb, &c.rest[e_in], 4);
                 if (c.lambda_inc[e_in] == 0xFFFFFFFFu) c.lambda_inc[e_in] = (uint32_t)inc.size();
+                (c.ci[e_in] == i ? c.inc_i : c.inc_j)[e_in] = (uint32_t)inc.size();
                 inc.push_back(make_uint2((other[k] + c.vtx_off) | (pidx[e_in] << 28), rb));
             }
         }
@@ -451,10 +469,21 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     ALLOC(lam_con, float, E);
     ALLOC(color_d, uint32_t, max_colors + 1);
     ALLOC(con_in_d, uint4, E);
+    uint8_t* con_type_d;
+    ALLOC(con_type_d, uint8_t, E);
     ALLOC(ctx->dparams, XpbdDevParams, 1);
     ALLOC(status, int, 4);
     ALLOC(sync, XpbdGridSync, 1);
     ALLOC(ctx->d_xyz, float, 3 * (size_t)N);
+    float* warm_inc;
+    uint32_t* inc_of_con_d;
+    unsigned *cloth_res_d, *iter_res_d;
+    XpbdConvergeStats* cstats_d;
+    ALLOC(warm_inc, float, inc.size());
+    ALLOC(inc_of_con_d, uint32_t, 2 * (size_t)E);
+    ALLOC(cloth_res_d, unsigned, 2 * (size_t)C);
+    ALLOC(iter_res_d, unsigned, XPBD_MAX_CONVERGE_ITERS);
+    ALLOC(cstats_d, XpbdConvergeStats, 1);
     ALLOC(ctx->d_resid, unsigned, 4);
     cudaStream_t st = ctx->stream;
 #define H2D(dst, src, bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), "upload")
@@ -475,15 +504,32 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
         CK(cudaStreamSynchronize(st), "commit sync");
     }
     H2D(pal_d, palette.data(), palette.size() * sizeof(float));
+    std::vector<uint8_t> ctypes(E);
+    for (auto& c : ctx->cloths)
+        for (uint32_t e = 0; e < c.e; ++e) ctypes[c.con_off + e] = (uint8_t)std::min<uint32_t>(c.ctype[e], 2);
     if (E) {
         H2D(con_d, con.data(), E * sizeof(uint4));
         H2D(con_in_d, con_in.data(), E * sizeof(uint4));
+        H2D(con_type_d, ctypes.data(), E);
+        CK(cudaStreamSynchronize(st), "commit sync");
     }
     CK(cudaMemsetAsync(lam_con, 0, std::max<size_t>(E, 1) * sizeof(float), st), "memset");
     H2D(color_d, color_off.data(), color_off.size() * sizeof(uint32_t));
     ctx->con_host = con;
     ctx->color_off_host = color_off;
     CK(cudaMemsetAsync(status, 0, 4 * sizeof(int), st), "memset");
+    CK(cudaMemsetAsync(warm_inc, 0, std::max<size_t>(inc.size(), 1) * 4, st), "memset");
+    CK(cudaMemsetAsync(cstats_d, 0, sizeof(XpbdConvergeStats), st), "memset");
+    {
+        std::vector<uint32_t> ioc(2 * (size_t)E);
+        for (auto& c : ctx->cloths)
+            for (uint32_t e = 0; e < c.e; ++e) {
+                ioc[2 * ((size_t)c.con_off + e)] = c.inc_i[e];
+                ioc[2 * ((size_t)c.con_off + e) + 1] = c.inc_j[e];
+            }
+        if (E) H2D(inc_of_con_d, ioc.data(), ioc.size() * 4);
+        CK(cudaStreamSynchronize(st), "commit sync");
+    }
     ctx->patches_ok = patches_ok && !patch_arrays.header.empty();
     if (ctx->patches_ok) {
         // one contiguous 16-byte aligned blob per patch: parts | con | gofs (patch-relative) | slots
@@ -563,9 +609,15 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     W.con_lambda = lam_con;
     W.color_off = color_d;
     W.con_in = con_in_d;
+    W.con_type = con_type_d;
     W.params = ctx->dparams;
     W.status = status;
     W.sync = sync;
+    W.warm_lam_inc = warm_inc;
+    W.inc_of_con = inc_of_con_d;
+    W.cloth_res = cloth_res_d;
+    W.iter_res = iter_res_d;
+    W.cstats = cstats_d;
     ensure_pinned(ctx, 16 * (size_t)N);
     ctx->committed = true;
     ctx->stats.num_particles = N;
@@ -649,7 +701,9 @@ static void choose_schedule(xpbd_ctx* ctx) {
         ctx->stats.cluster_ctas = ctx->cl;
         return;
     }
-    if (ctx->opts.solver == XPBD_SOLVER_GAUSS_SEIDEL)
+    if (ctx->opts.solver == XPBD_SOLVER_JACOBI && (ctx->opts.tolerance > 0.f || ctx->opts.warm_start))
+        ctx->kernel = 6;
+    else if (ctx->opts.solver == XPBD_SOLVER_GAUSS_SEIDEL)
         ctx->kernel = 1;
     else if (ctx->opts.jacobi_kernel == 1)
         ctx->kernel = 0;
@@ -665,7 +719,7 @@ static void choose_schedule(xpbd_ctx* ctx) {
     uint64_t need;
     if (ctx->kernel == 0) need = ((uint64_t)ctx->W.n_tiles * 32 + block - 1) / block;
     else if (ctx->kernel == 2) need = ctx->W.n_patches;
-    else need = ((uint64_t)ctx->W.n + block - 1) / block;
+    else need = ((uint64_t)ctx->W.n + block - 1) / block;  // rows / convergence solve: thread per particle
     uint32_t grid = (uint32_t)ctx->sms * (uint32_t)bps;
     if (grid > need) grid = (uint32_t)std::max<uint64_t>(1, need);
     ctx->block = block;
@@ -725,6 +779,9 @@ static int ensure_collision_buffers(xpbd_ctx* ctx) {
     return XPBD_OK;
 }
 
+// Learned warm start: features → MLP → λ0 per incidence (defined with the MLP host code below).
+cudaError_t launch_mlp_warm_start(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launches);
+
 // Enqueues one frame (opts.substeps substeps) on `st`. Returns the number of kernel launches.
 static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launches) {
     const xpbd_solver_opts& o = ctx->opts;
@@ -735,6 +792,26 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
     const uint32_t every = std::max<uint32_t>(1, o.collision_every_n_substeps);
     const float inv_cell = ctx->hp.inv_cell;
     cudaError_t e;
+    if (ctx->kernel == 6) {  // convergence solve: per substep predict, [λ0], solve-to-tolerance + finalize
+        const uint32_t warm = o.warm_start;
+        for (uint32_t s = 0; s < S; ++s) {
+            e = launch_converge_predict(ctx->W, ctx->sms, st);
+            *launches += 1;
+            if (e != cudaSuccess) return e;
+            if (warm == XPBD_WARM_PREVIOUS && ctx->W.n_inc) {
+                e = cudaMemcpyAsync(ctx->W.warm_lam_inc, ctx->W.inc_lambda, (size_t)ctx->W.n_inc * 4,
+                                    cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) return e;
+            } else if (warm == XPBD_WARM_LEARNED) {
+                e = launch_mlp_warm_start(ctx, st, launches);
+                if (e != cudaSuccess) return e;
+            }
+            e = launch_solver(6, ctx->block, ctx->grid, ctx->coop, ctx->W, warm ? 1u : 0u, 1, 0, 0, st);
+            *launches += 1;
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
     if (!coll) {
         e = launch_substeps(ctx, kEndFinalize, S, 0, 0, st);
         *launches += 1;
@@ -773,11 +850,14 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
 static std::string schedule_key(xpbd_ctx* ctx) {
     const xpbd_solver_opts& o = ctx->opts;
     char buf[256];
-    snprintf(buf, sizeof(buf), "%u/%u/%u/%u/%u/%u/%u/%u/%d/%p/%u/%u/%u/%u", o.solver, o.substeps, o.collision,
+    snprintf(buf, sizeof(buf), "%u/%u/%u/%u/%u/%u/%u/%u/%d/%p/%u/%u/%u/%u/%u", o.solver, o.substeps, o.collision,
              o.collision_every_n_substeps, ctx->tsp.inner_iterations, ctx->block, ctx->grid, (int)ctx->coop,
-             (int)(o.coll_scale > 1e-12f), (void*)ctx->stream, o.hash_table_bits, o.ring_depth, ctx->cl, ctx->kernel);
+             (int)(o.coll_scale > 1e-12f), (void*)ctx->stream, o.hash_table_bits, o.ring_depth, ctx->cl, ctx->kernel,
+             o.warm_start);
     return buf;
 }
+
+bool mlp_ready(xpbd_ctx* ctx);
 
 static int check_ready(xpbd_ctx* ctx) {
     if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
@@ -797,7 +877,16 @@ extern "C" int xpbd_set_params(xpbd_ctx* ctx, const xpbd_time_step_params* param
             return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "unknown solver option value");
         if (opts->collision != XPBD_COLLISION_NONE && !(opts->hash_cell >= opts->thickness))
             return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "hash_cell must be >= thickness");
-        if (opts->warm_start) return fail(ctx, XPBD_ERR_UNSUPPORTED, "learned warm start is not built yet");
+        if (opts->warm_start > XPBD_WARM_PREVIOUS) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad warm_start");
+        const bool converge = opts->tolerance > 0.f || opts->warm_start;
+        if (converge && opts->solver != XPBD_SOLVER_JACOBI)
+            return fail(ctx, XPBD_ERR_UNSUPPORTED, "the convergence solve is a Jacobi solve");
+        if (converge && opts->collision != XPBD_COLLISION_NONE)
+            return fail(ctx, XPBD_ERR_UNSUPPORTED, "the convergence solve has no collision pass");
+        if (converge && params->inner_iterations > XPBD_MAX_CONVERGE_ITERS)
+            return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "convergence solve: at most 4096 iterations per substep");
+        if (opts->warm_start == XPBD_WARM_LEARNED && !mlp_ready(ctx))
+            return fail(ctx, XPBD_ERR_STATE, "learned warm start needs a trained or loaded MLP (xpbd_mlp_*)");
         ctx->opts = *opts;
     }
     ctx->tsp = *params;
@@ -1016,7 +1105,7 @@ extern "C" int xpbd_read_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out) {
     if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const ClothHost& h = ctx->cloths[cloth_id];
-    const uint32_t kern = ctx->kernel == 5 ? 0u : ctx->kernel;  // rows and tiles share the incidence λ table
+    const uint32_t kern = (ctx->kernel == 5 || ctx->kernel == 6) ? 0u : ctx->kernel;  // incidence λ table
     const float* src = kern == 0 ? ctx->W.inc_lambda : (kern == 2 ? ctx->W.patch_lambda : ctx->W.con_lambda);
     const size_t cnt = kern == 0 ? ctx->W.n_inc : (kern == 2 ? ctx->W.patch_con_total : ctx->W.e);
     std::vector<float> all(std::max<size_t>(cnt, 1));
@@ -1048,7 +1137,50 @@ extern "C" int xpbd_strain_residual(xpbd_ctx* ctx, uint32_t cloth_id, float* out
 
 extern "C" int xpbd_get_stats(xpbd_ctx* ctx, xpbd_stats* out) {
     if (!ctx || !out) return XPBD_ERR_INVALID_ARGUMENT;
+    if (ctx->committed) {
+        XpbdConvergeStats cs{};
+        CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+        CK(cudaMemcpyAsync(&cs, ctx->W.cstats, sizeof(cs), cudaMemcpyDeviceToHost, ctx->stream), "stats");
+        CK(cudaStreamSynchronize(ctx->stream), "stats");
+        ctx->stats.converge_iterations = cs.iterations;
+        ctx->stats.converge_substeps = cs.substeps;
+        ctx->stats.converge_max_iterations = cs.max_iterations;
+        ctx->stats.warm_start_fallbacks = cs.fallbacks;
+    }
     *out = ctx->stats;
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_converge_history(xpbd_ctx* ctx, float* residuals, uint32_t max_count, uint32_t* count) {
+    if (!ctx || !count || (max_count && !residuals)) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    XpbdConvergeStats cs{};
+    CK(cudaMemcpyAsync(&cs, ctx->W.cstats, sizeof(cs), cudaMemcpyDeviceToHost, ctx->stream), "stats");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    *count = cs.last_iterations;
+    const uint32_t n = std::min(max_count, cs.last_iterations);
+    if (n) {
+        CK(cudaMemcpyAsync(residuals, ctx->W.iter_res, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "history");
+        CK(cudaStreamSynchronize(ctx->stream), "sync");
+    }
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_set_warm_lambda(xpbd_ctx* ctx, uint32_t cloth_id, const float* lambda0) {
+    if (!ctx || !lambda0) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const ClothHost& h = ctx->cloths[cloth_id];
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    std::vector<float> all(std::max<uint32_t>(ctx->W.n_inc, 1));
+    CK(cudaMemcpy(all.data(), ctx->W.warm_lam_inc, all.size() * 4, cudaMemcpyDeviceToHost), "readback");
+    for (uint32_t e = 0; e < h.e; ++e) {
+        if (h.inc_i[e] != 0xFFFFFFFFu) all[h.inc_i[e]] = lambda0[e];
+        if (h.inc_j[e] != 0xFFFFFFFFu) all[h.inc_j[e]] = lambda0[e];
+    }
+    CK(cudaMemcpy(ctx->W.warm_lam_inc, all.data(), all.size() * 4, cudaMemcpyHostToDevice), "upload");
     return XPBD_OK;
 }
 
@@ -1224,6 +1356,307 @@ extern "C" int xpbd_hash_keys(const float* xyzw, uint32_t n, float inv_cell, uin
     cudaError_t e = launch_hash_keys((const float4*)xyzw, n, inv_cell, table_bits, keys, nullptr,
                                      (cudaStream_t)stream);
     return e == cudaSuccess ? XPBD_OK : XPBD_ERR_CUDA;
+}
+
+// ------------------------------------------------------------------------------------------------- warm-start MLP
+bool mlp_ready(xpbd_ctx* ctx) { return ctx && ctx->d_mlp != nullptr; }
+
+cudaError_t launch_mlp_warm_start(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launches) {
+    *launches += 1;
+    return launch_mlp_infer(ctx->W, ctx->d_mlp, ctx->sms, st);
+}
+
+static int mlp_upload_norm(xpbd_ctx* ctx) {
+    XpbdMlp* m = ctx->d_mlp;
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    CK(cudaMemcpy(m->fmean, ctx->norm, 9 * 4, cudaMemcpyHostToDevice), "norm");
+    CK(cudaMemcpy(m->fstd, ctx->norm + 9, 9 * 4, cudaMemcpyHostToDevice), "norm");
+    CK(cudaMemcpy(&m->tmean, ctx->norm + 18, 4, cudaMemcpyHostToDevice), "norm");
+    CK(cudaMemcpy(&m->tstd, ctx->norm + 19, 4, cudaMemcpyHostToDevice), "norm");
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_mlp_init(xpbd_ctx* ctx, uint64_t seed, uint32_t capacity) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaError_t err = cudaSuccess;
+    if (!ctx->d_mlp) {
+        ctx->d_mlp = dev_alloc<XpbdMlp>(ctx, 1, &err);
+        if (err == cudaSuccess) ctx->d_master = dev_alloc<float>(ctx, XPBD_MLP_PARAMS, &err);
+        if (err == cudaSuccess) ctx->d_m1 = dev_alloc<float>(ctx, XPBD_MLP_PARAMS, &err);
+        if (err == cudaSuccess) ctx->d_m2 = dev_alloc<float>(ctx, XPBD_MLP_PARAMS, &err);
+        if (err == cudaSuccess) ctx->d_grads = dev_alloc<float>(ctx, XPBD_MLP_PARAMS, &err);
+        if (err == cudaSuccess) ctx->d_loss = dev_alloc<float>(ctx, 4096, &err);
+        if (err != cudaSuccess) return cuda_fail(ctx, err, "mlp buffers");
+    }
+    if (capacity > ctx->ds_cap) {
+        ctx->d_feat = dev_alloc<float>(ctx, (size_t)capacity * 9, &err);
+        if (err == cudaSuccess) ctx->d_scale = dev_alloc<float>(ctx, capacity, &err);
+        if (err == cudaSuccess) ctx->d_target = dev_alloc<float>(ctx, capacity, &err);
+        if (err != cudaSuccess) return cuda_fail(ctx, err, "mlp dataset");
+        ctx->ds_cap = capacity;
+    }
+    ctx->ds_count = 0;
+    ctx->adam_step = 0;
+    // seeded uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights, zero biases (splitmix64 stream)
+    std::vector<float> p(XPBD_MLP_PARAMS, 0.f);
+    uint64_t z = seed ? seed : 0x9E3779B97F4A7C15ull;
+    auto rnd = [&]() {
+        z += 0x9E3779B97F4A7C15ull;
+        uint64_t x = z;
+        x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+        x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+        x ^= x >> 31;
+        return (float)((double)(x >> 11) * (1.0 / 9007199254740992.0)) * 2.f - 1.f;
+    };
+    for (int k = 0; k < 576; ++k) p[k] = rnd() / sqrtf(9.f);
+    for (int k = 0; k < 4096; ++k) p[640 + k] = rnd() / sqrtf(64.f);
+    for (int k = 0; k < 64; ++k) p[640 + 4096 + 64 + k] = rnd() / sqrtf(64.f);
+    CK(cudaMemcpy(ctx->d_master, p.data(), XPBD_MLP_PARAMS * 4, cudaMemcpyHostToDevice), "mlp init");
+    CK(cudaMemset(ctx->d_m1, 0, XPBD_MLP_PARAMS * 4), "mlp init");
+    CK(cudaMemset(ctx->d_m2, 0, XPBD_MLP_PARAMS * 4), "mlp init");
+    for (int k = 0; k < 9; ++k) {
+        ctx->norm[k] = 0.f;
+        ctx->norm[9 + k] = 1.f;
+    }
+    ctx->norm[18] = 0.f;
+    ctx->norm[19] = 1.f;
+    int r = mlp_upload_norm(ctx);
+    if (r != XPBD_OK) return r;
+    CK(launch_mlp_publish(ctx->d_master, ctx->d_mlp, ctx->stream), "mlp publish");
+    CK(cudaStreamSynchronize(ctx->stream), "mlp init");
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_mlp_set_params(xpbd_ctx* ctx, const float* params, const float* norm) {
+    if (!ctx || !params) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->d_mlp) return fail(ctx, XPBD_ERR_STATE, "xpbd_mlp_init first");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    CK(cudaMemcpy(ctx->d_master, params, XPBD_MLP_PARAMS * 4, cudaMemcpyHostToDevice), "mlp params");
+    if (norm) {
+        memcpy(ctx->norm, norm, sizeof(ctx->norm));
+        int r = mlp_upload_norm(ctx);
+        if (r != XPBD_OK) return r;
+    }
+    CK(launch_mlp_publish(ctx->d_master, ctx->d_mlp, ctx->stream), "mlp publish");
+    CK(cudaStreamSynchronize(ctx->stream), "mlp params");
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_mlp_get_params(xpbd_ctx* ctx, float* params, float* norm) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->d_mlp) return fail(ctx, XPBD_ERR_STATE, "xpbd_mlp_init first");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    if (params) CK(cudaMemcpy(params, ctx->d_master, XPBD_MLP_PARAMS * 4, cudaMemcpyDeviceToHost), "mlp params");
+    if (norm) memcpy(norm, ctx->norm, sizeof(ctx->norm));
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_mlp_predict_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out) {
+    int r = check_ready(ctx);
+    if (r != XPBD_OK) return r;
+    if (!out) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->d_mlp) return fail(ctx, XPBD_ERR_STATE, "xpbd_mlp_init first");
+    if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(launch_converge_predict(ctx->W, ctx->sms, ctx->stream), "predict");
+    CK(launch_mlp_infer(ctx->W, ctx->d_mlp, ctx->sms, ctx->stream), "infer");
+    ctx->stats.kernel_launches += 2;
+    std::vector<float> all(std::max<uint32_t>(ctx->W.n_inc, 1));
+    if (ctx->W.n_inc)
+        CK(cudaMemcpyAsync(all.data(), ctx->W.warm_lam_inc, ctx->W.n_inc * 4, cudaMemcpyDeviceToHost, ctx->stream),
+           "readback");
+    r = read_status(ctx);
+    const ClothHost& h = ctx->cloths[cloth_id];
+    for (uint32_t e = 0; e < h.e; ++e)
+        out[e] = h.inc_i[e] != 0xFFFFFFFFu ? all[h.inc_i[e]] : (h.inc_j[e] != 0xFFFFFFFFu ? all[h.inc_j[e]] : 0.f);
+    return r;
+}
+
+extern "C" int xpbd_mlp_collect(xpbd_ctx* ctx, uint32_t substeps, uint32_t stride) {
+    int r = check_ready(ctx);
+    if (r != XPBD_OK) return r;
+    if (!ctx->d_mlp) return fail(ctx, XPBD_ERR_STATE, "xpbd_mlp_init first");
+    if (stride == 0) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "stride must be >= 1");
+    if (ctx->opts.solver != XPBD_SOLVER_JACOBI || ctx->opts.collision != XPBD_COLLISION_NONE)
+        return fail(ctx, XPBD_ERR_UNSUPPORTED, "collection runs the Jacobi convergence solve without collision");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    // the convergence solve's schedule, whatever the configured one
+    xpbd_solver_opts saved = ctx->opts;
+    ctx->opts.warm_start = XPBD_WARM_NONE;
+    if (!(ctx->opts.tolerance > 0.f)) ctx->opts.tolerance = 1e-30f;
+    fill_dev_params(ctx);
+    CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream), "p");
+    choose_schedule(ctx);
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = cudaSuccess;
+    for (uint32_t s = 0; s < substeps && e == cudaSuccess; ++s) {
+        const uint32_t offset = ctx->collect_offset++ % stride;
+        const uint32_t avail = ctx->W.e > offset ? (ctx->W.e - offset + stride - 1) / stride : 0;
+        const uint32_t take = std::min(avail, ctx->ds_cap - ctx->ds_count);
+        e = launch_converge_predict(ctx->W, ctx->sms, st);
+        if (e == cudaSuccess && take)
+            e = launch_mlp_collect_features(ctx->W, stride, offset, ctx->d_feat, ctx->d_scale, ctx->ds_count,
+                                            ctx->ds_count + take, st);
+        if (e == cudaSuccess) e = launch_solver(6, ctx->block, ctx->grid, ctx->coop, ctx->W, 0u, 1, 0, 0, st);
+        if (e == cudaSuccess && take)
+            e = launch_mlp_collect_targets(ctx->W, stride, offset, ctx->d_scale, ctx->d_target, ctx->ds_count,
+                                           ctx->ds_count + take, st);
+        ctx->ds_count += take;
+        ctx->stats.kernel_launches += take ? 4 : 2;
+    }
+    ctx->opts = saved;
+    fill_dev_params(ctx);
+    CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream), "p");
+    choose_schedule(ctx);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "collect");
+    return read_status(ctx);
+}
+
+extern "C" int xpbd_mlp_dataset_size(xpbd_ctx* ctx, uint32_t* count) {
+    if (!ctx || !count) return XPBD_ERR_INVALID_ARGUMENT;
+    *count = ctx->ds_count;
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_mlp_dataset_read(xpbd_ctx* ctx, uint32_t max_rows, float* features, float* targets,
+                                     uint32_t* rows) {
+    if (!ctx || !rows) return XPBD_ERR_INVALID_ARGUMENT;
+    const uint32_t n = std::min(max_rows, ctx->ds_count);
+    *rows = n;
+    if (!n) return XPBD_OK;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    if (features) CK(cudaMemcpy(features, ctx->d_feat, (size_t)n * 9 * 4, cudaMemcpyDeviceToHost), "read");
+    if (targets) CK(cudaMemcpy(targets, ctx->d_target, (size_t)n * 4, cudaMemcpyDeviceToHost), "read");
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_mlp_fit_normalization(xpbd_ctx* ctx) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->d_mlp || ctx->ds_count == 0) return fail(ctx, XPBD_ERR_STATE, "no stored samples");
+    const uint32_t n = std::min<uint32_t>(ctx->ds_count, 1u << 20);
+    std::vector<float> f((size_t)n * 9), t(n);
+    uint32_t rows = 0;
+    int r = xpbd_mlp_dataset_read(ctx, n, f.data(), t.data(), &rows);
+    if (r != XPBD_OK) return r;
+    for (int k = 0; k < 5; ++k) {
+        double s = 0, s2 = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            s += f[(size_t)i * 9 + k];
+            s2 += (double)f[(size_t)i * 9 + k] * f[(size_t)i * 9 + k];
+        }
+        const double mean = s / n, var = std::max(s2 / n - mean * mean, 0.0);
+        ctx->norm[k] = (float)mean;
+        ctx->norm[9 + k] = (float)std::max(std::sqrt(var), 1e-12);
+    }
+    for (int k = 5; k < 9; ++k) {
+        ctx->norm[k] = 0.f;
+        ctx->norm[9 + k] = 1.f;
+    }
+    double s = 0, s2 = 0;  // of the learned quantity, the change t - f1
+    for (uint32_t i = 0; i < n; ++i) {
+        const double d = (double)t[i] - f[(size_t)i * 9 + 1];
+        s += d;
+        s2 += d * d;
+    }
+    const double mean = s / n, var = std::max(s2 / n - mean * mean, 0.0);
+    ctx->norm[18] = (float)mean;
+    ctx->norm[19] = (float)std::max(std::sqrt(var), 1e-12);
+    return mlp_upload_norm(ctx);
+}
+
+extern "C" int xpbd_mlp_train(xpbd_ctx* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses) {
+    if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->d_mlp || ctx->ds_count == 0) return fail(ctx, XPBD_ERR_STATE, "no stored samples");
+    if (batch == 0 || steps == 0 || steps > 4096) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "steps in [1, 4096]");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const size_t need = (size_t)steps * batch;
+    if (need > ctx->idx_cap) {
+        cudaError_t err = cudaSuccess;
+        ctx->d_idx = dev_alloc<uint32_t>(ctx, need, &err);
+        if (err != cudaSuccess) return cuda_fail(ctx, err, "batch indices");
+        ctx->idx_cap = (uint32_t)need;
+    }
+    std::vector<uint32_t> idx(need);
+    uint64_t z = seed ^ 0xD1B54A32D192ED03ull;
+    for (size_t k = 0; k < need; ++k) {
+        z ^= z << 13;
+        z ^= z >> 7;
+        z ^= z << 17;
+        idx[k] = (uint32_t)(z % ctx->ds_count);
+    }
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->d_idx, idx.data(), need * 4, cudaMemcpyHostToDevice, st), "indices");
+    CK(cudaMemsetAsync(ctx->d_loss, 0, steps * 4, st), "memset");
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (uint32_t s = 0; s < steps; ++s) {
+        ++ctx->adam_step;
+        CK(cudaMemsetAsync(ctx->d_grads, 0, XPBD_MLP_PARAMS * 4, st), "memset");
+        CK(launch_mlp_train(ctx->d_mlp, ctx->d_feat, ctx->d_target, ctx->d_idx + (size_t)s * batch, batch,
+                            ctx->d_grads, ctx->d_loss + s, st), "train");
+        const float bc1 = 1.f - powf(b1, (float)ctx->adam_step), bc2 = 1.f - powf(b2, (float)ctx->adam_step);
+        CK(launch_mlp_adam(ctx->d_master, ctx->d_m1, ctx->d_m2, ctx->d_grads, lr, b1, b2, eps, bc1, bc2, ctx->d_mlp,
+                           st), "adam");
+        ctx->stats.kernel_launches += 3;
+    }
+    if (losses) {
+        CK(cudaMemcpyAsync(losses, ctx->d_loss, steps * 4, cudaMemcpyDeviceToHost, st), "losses");
+        CK(cudaStreamSynchronize(st), "sync");
+        for (uint32_t s = 0; s < steps; ++s) losses[s] /= (float)batch;
+    }
+    return read_status(ctx);
+}
+
+extern "C" int xpbd_mlp_eval(xpbd_ctx* ctx, const float* features, uint32_t n, float* out) {
+    if (!ctx || (n && (!features || !out))) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->d_mlp) return fail(ctx, XPBD_ERR_STATE, "xpbd_mlp_init first");
+    if (!n) return XPBD_OK;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    float *df = nullptr, *dout = nullptr;
+    CK(cudaMalloc(&df, (size_t)n * 9 * 4), "eval");
+    cudaError_t e = cudaMalloc(&dout, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(df, features, (size_t)n * 9 * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_mlp_eval(ctx->d_mlp, df, n, dout, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(df);
+    if (dout) cudaFree(dout);
+    return e == cudaSuccess ? XPBD_OK : cuda_fail(ctx, e, "eval");
+}
+
+extern "C" int xpbd_mlp_gradients(xpbd_ctx* ctx, const float* features, const float* targets, uint32_t n,
+                                  float* grads, float* loss) {
+    if (!ctx || !n || !features || !targets || !grads) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->d_mlp) return fail(ctx, XPBD_ERR_STATE, "xpbd_mlp_init first");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    float *df = nullptr, *dt = nullptr, *dg = nullptr, *dl = nullptr;
+    uint32_t* di = nullptr;
+    std::vector<uint32_t> idx(n);
+    for (uint32_t k = 0; k < n; ++k) idx[k] = k;
+    cudaError_t e = cudaMalloc(&df, (size_t)n * 9 * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dt, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&di, (size_t)n * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dg, XPBD_MLP_PARAMS * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&dl, 4);
+    cudaStream_t st = ctx->stream;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(df, features, (size_t)n * 36, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, targets, (size_t)n * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(di, idx.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, XPBD_MLP_PARAMS * 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dl, 0, 4, st);
+    if (e == cudaSuccess) e = launch_mlp_train(ctx->d_mlp, df, dt, di, n, dg, dl, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(grads, dg, XPBD_MLP_PARAMS * 4, cudaMemcpyDeviceToHost, st);
+    float lsum = 0.f;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&lsum, dl, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    for (void* p : {(void*)df, (void*)dt, (void*)di, (void*)dg, (void*)dl})
+        if (p) cudaFree(p);
+    if (loss) *loss = lsum / (float)n;
+    return e == cudaSuccess ? XPBD_OK : cuda_fail(ctx, e, "gradients");
 }
 
 // ------------------------------------------------------------------------------------------------- diagnostics

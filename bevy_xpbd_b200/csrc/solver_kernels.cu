@@ -483,6 +483,180 @@ __global__ void __launch_bounds__(BLOCK) jacobi_row_kernel(XpbdWorld W, uint32_t
     }
 }
 
+// ---------------------------------------------------------------------------------------------- convergence solve
+// Jacobi substep with λ kept over the substep, iterated until the pre-update residual max |C + α̃λ|/rest <= tolerance
+// (at most max_iterations passes), optionally warm-started from λ0: positions move by the reference gather with Δλ
+// replaced by λ0 and λ starts at λ0, unless that leaves a cloth's residual above its plain (λ = 0) start — then the
+// cloth falls back to the plain start for this substep. Thread per particle (row), fixed particle→thread mapping
+// across phases, so a particle's own incidences (and their λ copies) are only touched by its thread.
+__device__ __forceinline__ float residual_of(float len, float rest, float alpha_t, float lam) {
+    return __fdiv_rn(fabsf(__fadd_rn(__fsub_rn(len, rest), __fmul_rn(alpha_t, lam))), rest);
+}
+
+__device__ __forceinline__ void block_max_atomic(float v, unsigned* dst) {
+    __shared__ float s_max[32];
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) s_max[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < (blockDim.x >> 5) ? s_max[lane] : 0.0f;
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+        if (lane == 0 && v > 0.0f) atomicMax(dst, __float_as_uint(v));
+    }
+}
+
+// Predict into jac[0] (pinned: both buffers) and clear the per-substep residual slots.
+__global__ void converge_predict_kernel(XpbdWorld W) {
+    const XpbdDevParams P = *W.params;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    for (uint32_t k = gtid; k < 2 * W.n_cloths; k += gstride) W.cloth_res[k] = 0u;
+    for (uint32_t k = gtid; k < XPBD_MAX_CONVERGE_ITERS; k += gstride) W.iter_res[k] = 0u;
+    for (uint32_t i = gtid; i < W.n; i += gstride) {
+        const float4 x4 = W.x[i];
+        if (x4.w <= 0.0f) {
+            W.jac[0][i] = x4;
+            W.jac[1][i] = x4;
+            continue;
+        }
+        F3 vel = f3(W.v[i]);
+        const F3 pos = predict_particle(i, f3(x4), vel, P);
+        W.jac[0][i] = make_float4(pos.x, pos.y, pos.z, x4.w);
+    }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) jacobi_converge_kernel(XpbdWorld W, uint32_t warm) {
+    if (!status_clear(W)) return;
+    const XpbdDevParams P = *W.params;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    const float* lam0 = W.warm_lam_inc;
+    if (warm) {
+        // plain start residual (λ = 0) per cloth, and the warm-started positions into jac[1]
+        for (uint32_t i = gtid; i < W.n; i += gstride) {
+            const float4 ps = W.jac[0][i];
+            if (ps.w <= 0.0f) continue;
+            const uint32_t rs = W.row_off[i], re = W.row_off[i + 1];
+            const float* pal = W.palette_comp + (uint32_t)W.row_cloth[i] * XPBD_PALETTE;
+            float rmax = 0.0f, ax = 0.0f, ay = 0.0f, az = 0.0f;
+            for (uint32_t k = rs; k < re; ++k) {
+                const uint2 rec = W.inc[k];
+                const float4 po = W.jac[0][rec.x & XPBD_OTHER_MASK];
+                const F3 gv = sub3(f3(ps), f3(po));
+                const float len = len3(gv);
+                const float alpha_t = __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq);
+                rmax = fmaxf(rmax, residual_of(len, __uint_as_float(rec.y), alpha_t, 0.0f));
+                if (len < 1e-8f) continue;
+                const F3 nrm = div3(gv, len);
+                const float l0 = lam0[k];
+                ax = __fadd_rn(ax, __fmul_rn(__fmul_rn(nrm.x, ps.w), l0));
+                ay = __fadd_rn(ay, __fmul_rn(__fmul_rn(nrm.y, ps.w), l0));
+                az = __fadd_rn(az, __fmul_rn(__fmul_rn(nrm.z, ps.w), l0));
+            }
+            if (rmax > 0.0f) atomicMax(&W.cloth_res[2 * W.row_cloth[i]], __float_as_uint(rmax));
+            F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
+            if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
+            delta = clamp_correction(delta);
+            const F3 xn = add3(f3(ps), delta);
+            W.jac[1][i] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        }
+        if (!grid_barrier(W, P)) return;
+        // warm start residual per cloth (positions jac[1], λ = λ0)
+        for (uint32_t i = gtid; i < W.n; i += gstride) {
+            const float4 ps = W.jac[1][i];
+            if (ps.w <= 0.0f) continue;
+            const uint32_t rs = W.row_off[i], re = W.row_off[i + 1];
+            const float* pal = W.palette_comp + (uint32_t)W.row_cloth[i] * XPBD_PALETTE;
+            float rmax = 0.0f;
+            for (uint32_t k = rs; k < re; ++k) {
+                const uint2 rec = W.inc[k];
+                const float len = len3(sub3(f3(ps), f3(W.jac[1][rec.x & XPBD_OTHER_MASK])));
+                const float alpha_t = __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq);
+                rmax = fmaxf(rmax, residual_of(len, __uint_as_float(rec.y), alpha_t, lam0[k]));
+            }
+            if (rmax > 0.0f) atomicMax(&W.cloth_res[2 * W.row_cloth[i] + 1], __float_as_uint(rmax));
+        }
+        if (!grid_barrier(W, P)) return;
+        // keep the warm start where it does not raise the cloth's residual
+        for (uint32_t c = gtid; c < W.n_cloths; c += gstride)
+            if (__uint_as_float(W.cloth_res[2 * c + 1]) > __uint_as_float(W.cloth_res[2 * c]))
+                atomicAdd(&W.cstats->fallbacks, 1ull);
+        for (uint32_t i = gtid; i < W.n; i += gstride) {
+            const uint32_t c = W.row_cloth[i];
+            const bool keep = !(__uint_as_float(W.cloth_res[2 * c + 1]) > __uint_as_float(W.cloth_res[2 * c]));
+            if (keep) W.jac[0][i] = W.jac[1][i];
+            const uint32_t rs = W.row_off[i], re = W.row_off[i + 1];
+            for (uint32_t k = rs; k < re; ++k) W.inc_lambda[k] = keep ? lam0[k] : 0.0f;
+        }
+    } else {
+        for (uint32_t k = gtid; k < W.n_inc; k += gstride) W.inc_lambda[k] = 0.0f;
+    }
+    if (!grid_barrier(W, P)) return;
+    // iterations: residual of the state before each update pass, checked after the pass
+    uint32_t cur = 0, it = 0;
+    const uint32_t maxit = min(P.max_iterations, (uint32_t)XPBD_MAX_CONVERGE_ITERS);
+    while (it < maxit) {
+        const float4* jin = W.jac[cur];
+        float4* jout = W.jac[cur ^ 1u];
+        float rmax = 0.0f;
+        for (uint32_t i = gtid; i < W.n; i += gstride) {
+            const float4 ps = jin[i];
+            if (ps.w <= 0.0f) continue;
+            const uint32_t rs = W.row_off[i], re = W.row_off[i + 1];
+            const float* pal = W.palette_comp + (uint32_t)W.row_cloth[i] * XPBD_PALETTE;
+            float ax = 0.0f, ay = 0.0f, az = 0.0f;
+            for (uint32_t k = rs; k < re; ++k) {
+                const uint2 rec = W.inc[k];
+                const float4 po = jin[rec.x & XPBD_OTHER_MASK];
+                const F3 gv = sub3(f3(ps), f3(po));
+                const float len = len3(gv);
+                const float rest = __uint_as_float(rec.y);
+                const float alpha_t = __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq);
+                const float lam = W.inc_lambda[k];
+                rmax = fmaxf(rmax, residual_of(len, rest, alpha_t, lam));
+                if (len < 1e-8f) continue;
+                const F3 nrm = div3(gv, len);
+                const float C = __fsub_rn(len, rest);
+                const float wsum = __fadd_rn(__fadd_rn(ps.w, po.w), alpha_t);
+                if (wsum < 1e-8f) continue;
+                const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
+                W.inc_lambda[k] = __fadd_rn(lam, dlam);
+                ax = __fadd_rn(ax, __fmul_rn(__fmul_rn(nrm.x, ps.w), dlam));
+                ay = __fadd_rn(ay, __fmul_rn(__fmul_rn(nrm.y, ps.w), dlam));
+                az = __fadd_rn(az, __fmul_rn(__fmul_rn(nrm.z, ps.w), dlam));
+            }
+            F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
+            if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
+            delta = clamp_correction(delta);
+            const F3 xn = add3(f3(ps), delta);
+            jout[i] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        }
+        block_max_atomic(rmax, &W.iter_res[it]);
+        if (!grid_barrier(W, P)) return;
+        const float res = __uint_as_float(*(volatile unsigned*)&W.iter_res[it]);
+        cur ^= 1u;
+        ++it;
+        if (res <= P.tolerance) break;
+    }
+    if (gtid == 0) {
+        atomicAdd(&W.cstats->iterations, (unsigned long long)it);
+        atomicAdd(&W.cstats->substeps, 1ull);
+        atomicMax(&W.cstats->max_iterations, it);
+        W.cstats->last_iterations = it;
+    }
+    // finalize (post_velocity) from the final iterate; pinned particles keep x, v
+    for (uint32_t i = gtid; i < W.n; i += gstride) {
+        const float4 p4 = W.jac[cur][i];
+        if (p4.w <= 0.0f) continue;
+        const F3 xo = f3(W.x[i]);
+        F3 vel = f3(W.v[i]);
+        const F3 xn = finalize_particle(f3(p4), xo, vel, P, W.status);
+        W.x[i] = make_float4(xn.x, xn.y, xn.z, p4.w);
+        W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+    }
+}
+
 // ---------------------------------------------------------------------------------------------- Jacobi patches
 // Each CTA walks its patches (pid = blockIdx.x + m*gridDim.x). Per patch: (1) the patch's table blob was fetched into
 // shared memory by one TMA bulk copy issued one patch ahead (cp.async.bulk, completion on an mbarrier, L2 evict-first
@@ -840,6 +1014,8 @@ static const void* patch_fn() { return (const void*)jacobi_patch_kernel<BLOCK>; 
 template <int BLOCK>
 static const void* row_fn() { return (const void*)jacobi_row_kernel<BLOCK>; }
 template <int BLOCK>
+static const void* converge_fn() { return (const void*)jacobi_converge_kernel<BLOCK>; }
+template <int BLOCK>
 static const void* gs_fn() { return (const void*)gs_persistent_kernel<BLOCK>; }
 
 // kernel 0: Jacobi over warp tiles, 1: Gauss–Seidel, 2: Jacobi over spatial patches, 5: Jacobi thread per particle
@@ -861,6 +1037,10 @@ const void* solver_kernel_fn(uint32_t solver, uint32_t block) {
         case 50256: return row_fn<256>();
         case 50512: return row_fn<512>();
         case 51024: return row_fn<1024>();
+        case 60128: return converge_fn<128>();
+        case 60256: return converge_fn<256>();
+        case 60512: return converge_fn<512>();
+        case 61024: return converge_fn<1024>();
     }
     return nullptr;
 }
@@ -897,6 +1077,10 @@ cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool c
         cfg.numAttrs = 1;
     }
     XpbdWorld w = W;
+    if (solver == 6) {  // convergence solve: `flags` carries the warm-start switch
+        void* args[] = {&w, &flags};
+        return cudaLaunchKernelExC(&cfg, fn, args);
+    }
     if (solver != 1) {
         void* args[] = {&w, &flags, &substeps, &pend, &start};
         return cudaLaunchKernelExC(&cfg, fn, args);
@@ -912,6 +1096,14 @@ int max_blocks_per_sm(uint32_t solver, uint32_t block, const XpbdWorld& W) {
     if (!fn || !set_smem_attr(fn, dyn)) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, (int)block, dyn) != cudaSuccess) return 0;
     return nb;
+}
+
+cudaError_t launch_converge_predict(const XpbdWorld& W, int sms, cudaStream_t st) {
+    uint32_t grid = (W.n + 255) / 256;
+    if (grid > (uint32_t)sms * 8) grid = (uint32_t)sms * 8;
+    if (grid < 16) grid = 16;
+    converge_predict_kernel<<<grid, 256, 0, st>>>(W);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(const XpbdWorld& W, uint32_t pend, int sms, cudaStream_t st) {

@@ -38,6 +38,31 @@ struct XpbdDevParams {  // the per-call uniform block (ClothSimParamsGpu, cloth_
     float thickness, coll_scale, inv_cell, ground_y;
     uint32_t ground_enabled, collision, table_bits, warm_start;
     unsigned long long barrier_timeout_ns;
+    float tolerance;       // convergence solve: stop when max |C + α̃λ|/rest of the pre-update state <= tolerance
+    uint32_t max_iterations;
+};
+
+#define XPBD_MLP_IN 9
+#define XPBD_MLP_PARAMS 4865  // w1 64x9, b1 64, w2 64x64, b2 64, w3 64, b3 1 (fp32 master layout)
+#define XPBD_MLP_NORM 20      // feature mean[9], std[9], target mean, std
+
+// Working copy of the warm-start MLP read by the kernels: bf16 weights ([out][in], layer-1 inputs padded 9 → 16),
+// fp32 biases, input/target standardisation.
+struct XpbdMlp {
+    uint16_t w1[64 * 16];
+    uint16_t w2[64 * 64];
+    uint16_t w3[64];
+    float b1[64], b2[64], b3;
+    float fmean[XPBD_MLP_IN], fstd[XPBD_MLP_IN], tmean, tstd;
+};
+
+#define XPBD_MAX_CONVERGE_ITERS 4096
+struct XpbdConvergeStats {  // device counters of the convergence solve
+    unsigned long long iterations;  // update passes summed over substeps
+    unsigned long long substeps;
+    unsigned long long fallbacks;   // cloth-substeps whose warm start was rejected
+    unsigned int max_iterations;
+    unsigned int last_iterations;   // update passes of the most recent substep (its residuals stay in iter_res)
 };
 
 struct XpbdGridSync {
@@ -89,6 +114,7 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     float* con_lambda;
     const uint32_t* color_off;
     const uint4* con_in;            // constraints in input order, cloths contiguous (residual)
+    const uint8_t* con_type;        // constraint type per packed input-order constraint
     const XpbdDevParams* params;
     int* status;
     XpbdGridSync* sync;
@@ -97,4 +123,10 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     const XpbdPatch* patches;
     const uint4* patch_blob;
     float* patch_lambda;
+    // convergence solve
+    float* warm_lam_inc;            // λ0 per incidence
+    const uint32_t* inc_of_con;     // per constraint (input order, packed): incidence of the i / j side (2 entries)
+    unsigned* cloth_res;            // 2 per cloth: plain / warm start residual (float bits)
+    unsigned* iter_res;             // per iteration of a substep: residual (float bits)
+    XpbdConvergeStats* cstats;
 };

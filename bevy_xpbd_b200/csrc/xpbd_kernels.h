@@ -10,14 +10,29 @@ namespace xpbd {
 constexpr uint32_t kBeginFinalize = 1u;  // finalize positions waiting in jac[pend] before predicting
 constexpr uint32_t kEndFinalize = 2u;    // finalize the launch's last substep in place
 
-// ---- solver (solver_kernels.cu); kernel id: 0 Jacobi warp tiles, 1 Gauss–Seidel, 2 Jacobi spatial patches
+// ---- solver (solver_kernels.cu); kernel id: 0 Jacobi warp tiles, 1 Gauss–Seidel, 2 Jacobi spatial patches,
+//      5 Jacobi thread per particle, 6 Jacobi convergence solve
 const void* solver_kernel_fn(uint32_t solver, uint32_t block);
 int max_blocks_per_sm(uint32_t solver, uint32_t block, const XpbdWorld& W);
 cudaError_t launch_solver(uint32_t solver, uint32_t block, uint32_t grid, bool cooperative, const XpbdWorld& W,
                           uint32_t flags, uint32_t substeps, uint32_t pend, uint32_t start, cudaStream_t st);
 cudaError_t launch_finalize(const XpbdWorld& W, uint32_t pend, int sms, cudaStream_t st);
+cudaError_t launch_converge_predict(const XpbdWorld& W, int sms, cudaStream_t st);
 cudaError_t launch_strain_residual(const XpbdWorld& W, uint32_t e0, uint32_t e1, unsigned* out_bits, int sms,
                                    cudaStream_t st);
+
+// ---- warm-start MLP (mlp.cu)
+cudaError_t launch_mlp_infer(const XpbdWorld& W, const XpbdMlp* mlp, int sms, cudaStream_t st);
+cudaError_t launch_mlp_eval(const XpbdMlp* mlp, const float* feat, uint32_t n, float* out, cudaStream_t st);
+cudaError_t launch_mlp_collect_features(const XpbdWorld& W, uint32_t stride, uint32_t offset, float* feat,
+                                        float* scale, uint32_t base, uint32_t cap, cudaStream_t st);
+cudaError_t launch_mlp_collect_targets(const XpbdWorld& W, uint32_t stride, uint32_t offset, const float* scale,
+                                       float* target, uint32_t base, uint32_t cap, cudaStream_t st);
+cudaError_t launch_mlp_train(const XpbdMlp* mlp, const float* feat, const float* target, const uint32_t* idx,
+                             uint32_t nrows, float* grads, float* loss, cudaStream_t st);
+cudaError_t launch_mlp_adam(float* master, float* m1, float* m2, const float* grads, float lr, float beta1,
+                            float beta2, float eps, float bc1, float bc2, XpbdMlp* mlp, cudaStream_t st);
+cudaError_t launch_mlp_publish(const float* master, XpbdMlp* mlp, cudaStream_t st);
 
 // ---- cluster Gauss–Seidel (cluster_gs.cu)
 struct ClusterTable {

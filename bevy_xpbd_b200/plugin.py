@@ -33,6 +33,7 @@ RELAX_OMEGA, RELAX_AVERAGE = 0, 1
 LAMBDA_RESET_PER_ITERATION, LAMBDA_PER_SUBSTEP = 0, 1
 COLLISION_NONE, COLLISION_REST_FILTER, COLLISION_RING_FILTER = 0, 1, 2
 ORDER_COLOR_REFERENCE, ORDER_COLOR_INDEX, ORDER_PRESORTED = 0, 1, 2
+WARM_NONE, WARM_LEARNED, WARM_GIVEN, WARM_PREVIOUS = 0, 1, 2, 3
 ALL = 0xFFFFFFFF
 
 
@@ -118,9 +119,10 @@ class ClothSimConfig:
     barrier_timeout_ms: float = 2000.0
     block_threads: int = 0
     blocks_per_sm: int = 0
-    warm_start: bool = False
+    warm_start: int = WARM_NONE
     cluster_ctas: int = 0
     jacobi_kernel: int = 0
+    tolerance: float = 0.0
 
     def to_c(self) -> N.SolverOpts:
         o = N.SolverOpts()
@@ -134,6 +136,7 @@ class ClothSimConfig:
         o.block_threads, o.blocks_per_sm, o.warm_start = self.block_threads, self.blocks_per_sm, int(self.warm_start)
         o.cluster_ctas = self.cluster_ctas
         o.jacobi_kernel = self.jacobi_kernel
+        o.tolerance = self.tolerance
         return o
 
 
@@ -276,6 +279,82 @@ class ClothComputePlugin:
         out = np.empty(self._cloths[cloth][1], np.float32)
         self._check(self._L.xpbd_read_lambda(self._h, cloth, _ptr(out)))
         return out
+
+    def set_warm_lambda(self, lambda0, cloth: int = 0):
+        """λ0 per constraint (input order) for the WARM_GIVEN start of the convergence solve."""
+        self._warm = _f32(lambda0)
+        self._check(self._L.xpbd_set_warm_lambda(self._h, cloth, _ptr(self._warm)))
+
+    def converge_history(self, max_count: int = 4096) -> np.ndarray:
+        """Max residual |C + α̃λ|/rest before each update pass of the most recent convergence-solve substep."""
+        out = np.zeros(max_count, np.float32)
+        c = C.c_uint32(0)
+        self._check(self._L.xpbd_converge_history(self._h, _ptr(out), max_count, C.byref(c)))
+        return out[: min(int(c.value), max_count)]
+
+    # ---- learned warm start (extension) ------------------------------------------------------------------------
+    def mlp_init(self, seed: int = 0, capacity: int = 1 << 20):
+        """Allocates the warm-start MLP (seeded initialisation) and room for `capacity` training samples."""
+        self._check(self._L.xpbd_mlp_init(self._h, seed, capacity))
+
+    def mlp_params(self) -> tuple[np.ndarray, np.ndarray]:
+        """(fp32 parameters [w1 64x9, b1, w2 64x64, b2, w3, b3], normalisation [fmean 9, fstd 9, tmean, tstd])."""
+        p = np.zeros(N.MLP_PARAMS, np.float32)
+        n = np.zeros(N.MLP_NORM, np.float32)
+        self._check(self._L.xpbd_mlp_get_params(self._h, _ptr(p), _ptr(n)))
+        return p, n
+
+    def mlp_set_params(self, params, norm=None):
+        p = _f32(params)
+        n = None if norm is None else _f32(norm)
+        self._check(self._L.xpbd_mlp_set_params(self._h, _ptr(p), None if n is None else _ptr(n)))
+
+    def mlp_predict_lambda(self, cloth: int = 0) -> np.ndarray:
+        """λ0 the learned warm start gives the next substep (input order); the state is unchanged."""
+        n_con = self.cloth_size(cloth)[1]
+        out = np.zeros(n_con, np.float32)
+        self._check(self._L.xpbd_mlp_predict_lambda(self._h, cloth, _ptr(out)))
+        return out
+
+    def mlp_collect(self, substeps: int, stride: int = 1) -> int:
+        """Runs `substeps` plain convergence-solve substeps and stores (features, final λ target) samples."""
+        self._check(self._L.xpbd_mlp_collect(self._h, substeps, stride))
+        c = C.c_uint32(0)
+        self._check(self._L.xpbd_mlp_dataset_size(self._h, C.byref(c)))
+        return int(c.value)
+
+    def mlp_dataset(self, max_rows: int | None = None) -> tuple[np.ndarray, np.ndarray]:
+        c = C.c_uint32(0)
+        self._check(self._L.xpbd_mlp_dataset_size(self._h, C.byref(c)))
+        n = int(c.value) if max_rows is None else min(int(c.value), max_rows)
+        f = np.zeros((n, N.MLP_FEATURES), np.float32)
+        t = np.zeros(n, np.float32)
+        rows = C.c_uint32(0)
+        self._check(self._L.xpbd_mlp_dataset_read(self._h, n, _ptr(f), _ptr(t), C.byref(rows)))
+        return f[: rows.value], t[: rows.value]
+
+    def mlp_fit_normalization(self):
+        self._check(self._L.xpbd_mlp_fit_normalization(self._h))
+
+    def mlp_train(self, steps: int, batch: int = 4096, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+        losses = np.zeros(steps, np.float32)
+        self._check(self._L.xpbd_mlp_train(self._h, steps, batch, C.c_float(lr), seed, _ptr(losses)))
+        return losses
+
+    def mlp_eval(self, features) -> np.ndarray:
+        f = _f32(features)
+        n = f.size // N.MLP_FEATURES
+        out = np.zeros(n, np.float32)
+        self._check(self._L.xpbd_mlp_eval(self._h, _ptr(f), n, _ptr(out)))
+        return out
+
+    def mlp_gradients(self, features, targets) -> tuple[np.ndarray, float]:
+        f = _f32(features)
+        t = _f32(targets)
+        g = np.zeros(N.MLP_PARAMS, np.float32)
+        loss = C.c_float(0)
+        self._check(self._L.xpbd_mlp_gradients(self._h, _ptr(f), _ptr(t), t.size, _ptr(g), C.byref(loss)))
+        return g, float(loss.value)
 
     def strain_residual(self, cloth: int | None = None) -> float:
         v = C.c_float()

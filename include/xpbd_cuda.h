@@ -54,6 +54,11 @@ extern "C" {
 #define XPBD_ORDER_COLOR_INDEX 1     /* recolor greedily in plain constraint-index order */
 #define XPBD_ORDER_PRESORTED 2       /* constraints already batch-sorted by the caller; use its batch offsets */
 
+#define XPBD_WARM_NONE 0      /* plain start: λ = 0, predicted positions */
+#define XPBD_WARM_LEARNED 1   /* λ0 from the context's MLP (xpbd_mlp_*) */
+#define XPBD_WARM_GIVEN 2     /* λ0 set with xpbd_set_warm_lambda */
+#define XPBD_WARM_PREVIOUS 3  /* λ0 = the previous substep's final λ */
+
 #define XPBD_CONSTRAINT_STRETCH 0
 #define XPBD_CONSTRAINT_SHEAR 1
 #define XPBD_CONSTRAINT_BEND 2
@@ -96,10 +101,12 @@ typedef struct xpbd_solver_opts {
     float barrier_timeout_ms;         /* bound on every grid-barrier wait (default 2000) */
     uint32_t block_threads;           /* 0 = autotuned / default */
     uint32_t blocks_per_sm;           /* 0 = autotuned / default */
-    uint32_t warm_start;              /* 1: learned λ warm start (requires XPBD_LAMBDA_PER_SUBSTEP) */
+    uint32_t warm_start;              /* convergence solve start: XPBD_WARM_* (0 = plain, λ = 0) */
     uint32_t cluster_ctas;            /* Gauss–Seidel in one thread-block cluster: 0 auto, 1 off, 8 or 16 CTAs */
     uint32_t jacobi_kernel;           /* Jacobi: 0 auto, 1 warp tiles, 2 shared-memory patches, 3 thread per particle */
-    uint32_t reserved[4];
+    float tolerance;                  /* > 0 (or warm_start != 0): convergence solve — Jacobi, λ kept per substep,
+                                         iterate until max |C + α̃λ|/rest <= tolerance, at most inner_iterations */
+    uint32_t reserved[3];
 } xpbd_solver_opts;
 
 /* One cloth: the arrays of ClothMeshData / ClothSimConfig (mesh_prep.rs:103-131, cloth_compute.rs:140-179). All
@@ -136,8 +143,12 @@ typedef struct xpbd_stats {
     uint64_t warm_start_fallbacks;    /* substeps where the learned warm start was rejected */
     uint64_t collision_pairs;         /* pairs found by the last collision pass (when counted) */
     uint32_t solver_kernel;           /* 0 Jacobi warp tiles, 1 Gauss–Seidel grid, 2 Jacobi patches, 3 GS cluster,
-                                         5 Jacobi thread per particle */
+                                         5 Jacobi thread per particle, 6 Jacobi convergence solve */
     uint32_t cluster_ctas;            /* CTAs of the Gauss–Seidel cluster (0 = grid kernel) */
+    uint64_t converge_iterations;     /* convergence solve: update passes summed over substeps */
+    uint64_t converge_substeps;
+    uint32_t converge_max_iterations;
+    uint32_t pad;
 } xpbd_stats;
 
 typedef struct xpbd_ctx xpbd_ctx;
@@ -179,6 +190,11 @@ int xpbd_write_state(xpbd_ctx* ctx, uint32_t cloth_id, const float* xyz, const f
 int xpbd_reset(xpbd_ctx* ctx);
 /* Per-constraint λ after the last substep, in the cloth's input constraint order (extension). */
 int xpbd_read_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out);
+/* Convergence solve: the max pre-update residual max|C + α̃λ|/rest of each update pass of the most recent substep
+ * (`count` = its number of passes; up to max_count values are copied). Extension: no reference counterpart. */
+int xpbd_converge_history(xpbd_ctx* ctx, float* residuals, uint32_t max_count, uint32_t* count);
+/* Warm-start λ0 per constraint of a cloth (input order) for XPBD_WARM_GIVEN — extension. */
+int xpbd_set_warm_lambda(xpbd_ctx* ctx, uint32_t cloth_id, const float* lambda0);
 /* Max strain residual |‖xi−xj‖−rest|/rest over the constraints of a cloth (UINT32_MAX = all) — extension. */
 int xpbd_strain_residual(xpbd_ctx* ctx, uint32_t cloth_id, float* out);
 int xpbd_get_stats(xpbd_ctx* ctx, xpbd_stats* out);
@@ -226,6 +242,39 @@ int xpbd_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_
 /* keys[i] = prime-hash(floor(xyz_i * inv_cell)) & (2^bits - 1), positions as float4 (w ignored). */
 int xpbd_hash_keys(const float* xyzw, uint32_t n, float inv_cell, uint32_t table_bits, uint32_t* keys,
                    void* stream);
+
+/* ---- learned warm start (extension: no reference counterpart) -------------------------------------------------
+ * A 9→64→64→1 MLP (SiLU; BF16 tensor-core tiles, FP32 accumulation) predicting each constraint's initial λ for the
+ * convergence solve (XPBD_WARM_LEARNED). Parameters: XPBD_MLP_PARAMS fp32 values in the order w1[64][9], b1[64],
+ * w2[64][64], b2[64], w3[64], b3, plus XPBD_MLP_NORM normalisation values (feature mean[9], std[9], target mean,
+ * std; features f0..f4 are standardised; the target is t = λ·(wi+wj+α̃)/rest and the network predicts its change over
+ * the previous substep, t - f1, standardised with the target mean/std). */
+#define XPBD_MLP_PARAMS 4865
+#define XPBD_MLP_NORM 20
+#define XPBD_MLP_FEATURES 9
+/* Allocates the MLP (seeded initialisation) and a training set of `capacity` samples. */
+int xpbd_mlp_init(xpbd_ctx* ctx, uint64_t seed, uint32_t capacity);
+int xpbd_mlp_set_params(xpbd_ctx* ctx, const float* params, const float* norm);
+int xpbd_mlp_get_params(xpbd_ctx* ctx, float* params, float* norm);
+/* λ0 the learned warm start would give cloth `cloth`'s constraints (input order) at the next substep's predicted
+ * positions; the simulation state is unchanged. */
+int xpbd_mlp_predict_lambda(xpbd_ctx* ctx, uint32_t cloth, float* lambda0);
+/* Runs `substeps` substeps of the convergence solve (plain start; inner_iterations / tolerance as set) and stores, for
+ * every `stride`-th constraint, its features at the substep's predicted positions and its final λ as the target. */
+int xpbd_mlp_collect(xpbd_ctx* ctx, uint32_t substeps, uint32_t stride);
+int xpbd_mlp_dataset_size(xpbd_ctx* ctx, uint32_t* count);
+/* Copies up to `max_rows` stored samples (raw features n x 9, targets t) to the host. */
+int xpbd_mlp_dataset_read(xpbd_ctx* ctx, uint32_t max_rows, float* features, float* targets, uint32_t* rows);
+/* Sets the standardisation from the stored samples. */
+int xpbd_mlp_fit_normalization(xpbd_ctx* ctx);
+/* `steps` Adam steps on minibatches of `batch` samples drawn (seeded) from the stored set; losses[steps] (may be NULL)
+ * receives each step's mean squared error of the standardised target. */
+int xpbd_mlp_train(xpbd_ctx* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses);
+/* Standardised prediction for n raw feature rows (host arrays). */
+int xpbd_mlp_eval(xpbd_ctx* ctx, const float* features, uint32_t n, float* out);
+/* Gradient of mean((y - (t - f1 - tmean)/tstd)^2) over n rows w.r.t. the XPBD_MLP_PARAMS parameters (host arrays). */
+int xpbd_mlp_gradients(xpbd_ctx* ctx, const float* features, const float* targets, uint32_t n, float* grads,
+                       float* loss);
 
 /* ---- diagnostics ------------------------------------------------------------------------------------------- */
 const char* xpbd_last_error(xpbd_ctx* ctx);

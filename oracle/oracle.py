@@ -36,6 +36,7 @@ class OracleParams(C.Structure):
         ("solver", C.c_uint32), ("relaxation", C.c_uint32), ("lambda_mode", C.c_uint32),
         ("collision", C.c_uint32), ("thickness", C.c_float), ("coll_scale", C.c_float),
         ("hash_cell", C.c_float), ("ground_enabled", C.c_uint32), ("ground_y", C.c_float), ("damp", C.c_float),
+        ("tolerance", C.c_float), ("warm_start", C.c_uint32),
     ]
 
 
@@ -82,6 +83,8 @@ def lib():
         L.oracle_sim_collision_pairs.argtypes = [P, u32p, C.c_uint64]
         L.oracle_sim_set_batches.argtypes = [P, C.c_void_p, C.c_uint32]
         L.oracle_threads.restype = C.c_int
+        L.oracle_sim_substeps_converge.argtypes = [P, C.c_uint32, C.c_void_p, C.c_void_p]
+        L.oracle_sim_predicted.argtypes = [P, f64p]
         _lib = L
     return _lib
 
@@ -193,6 +196,13 @@ class OracleSim:
     def substeps(self, count: int, brute_force: bool = False):
         lib().oracle_sim_substeps(self.h, count, int(brute_force))
 
+    def substeps_converge(self, count: int):
+        """Convergence solve (extension); returns (update passes, fallback flag) per substep."""
+        it = np.zeros(count, np.uint32)
+        fb = np.zeros(count, np.uint32)
+        lib().oracle_sim_substeps_converge(self.h, count, _ptr(it), _ptr(fb))
+        return it, fb
+
     def state(self):
         x = np.zeros((self.n, 3), np.float64)
         v = np.zeros((self.n, 3), np.float64)
@@ -203,6 +213,12 @@ class OracleSim:
         xx = None if x is None else np.ascontiguousarray(x, np.float32).reshape(-1)
         vv = None if v is None else np.ascontiguousarray(v, np.float32).reshape(-1)
         lib().oracle_sim_set_state(self.h, _ptr(xx), _ptr(vv))
+
+    def predicted(self):
+        """Positions after the next substep's prediction step (xpbd_cpu.rs:251-260), state unchanged."""
+        out = np.zeros((self.n, 3), np.float64)
+        lib().oracle_sim_predicted(self.h, out.reshape(-1))
+        return out
 
     def lambdas(self):
         out = np.zeros(self.e, np.float64)

@@ -230,6 +230,26 @@ void oracle_sim_get_lambda(void* h, double* out) {
     else
         for (size_t e = 0; e < s->f.lambda.size(); ++e) out[e] = (double)s->f.lambda[e];
 }
+// Positions the next substep's prediction step would produce (state unchanged).
+void oracle_sim_predicted(void* h, double* x) {
+    auto* s = (OracleSim*)h;
+    auto run = [&](auto& sim) {
+        for (uint32_t i = 0; i < sim.n; ++i) {
+            auto pos = sim.sim_pos[i];
+            if (sim.inv_mass[i] > 0) {
+                auto v = sim.vel[i];
+                pos = sim.predict_particle(i, sim.sim_pos[i], v);
+            }
+            x[3 * i] = (double)pos.x;
+            x[3 * i + 1] = (double)pos.y;
+            x[3 * i + 2] = (double)pos.z;
+        }
+    };
+    if (s->fp64)
+        run(s->d);
+    else
+        run(s->f);
+}
 void oracle_sim_set_warm_lambda(void* h, const float* lam) {
     auto* s = (OracleSim*)h;
     if (!lam) {
@@ -241,6 +261,21 @@ void oracle_sim_set_warm_lambda(void* h, const float* lam) {
     s->f.warm_lambda.assign(lam, lam + e);
     s->d.warm_lambda.resize(e);
     for (size_t k = 0; k < e; ++k) s->d.warm_lambda[k] = lam[k];
+}
+// Extension convergence solve (Jacobi, per-substep λ, optional warm start from oracle_sim_set_warm_lambda).
+void oracle_sim_substeps_converge(void* h, uint32_t count, uint32_t* iterations_out, uint32_t* fallback_out) {
+    auto* s = (OracleSim*)h;
+    for (uint32_t k = 0; k < count; ++k) {
+        if (s->fp64) {
+            s->d.substep_converge();
+            if (iterations_out) iterations_out[k] = s->d.last_iterations;
+            if (fallback_out) fallback_out[k] = s->d.last_fallback;
+        } else {
+            s->f.substep_converge();
+            if (iterations_out) iterations_out[k] = s->f.last_iterations;
+            if (fallback_out) fallback_out[k] = s->f.last_fallback;
+        }
+    }
 }
 void oracle_sim_set_batches(void* h, const uint32_t* offsets, uint32_t count) {
     auto* s = (OracleSim*)h;

@@ -512,6 +512,8 @@ struct Params {  // XpbdCpuTimeStepParams, xpbd_cpu.rs:11-26, plus the extension
     uint32_t ground_enabled;
     float ground_y;
     float damp;            // exp(-k·dt) evaluated once on the host (xpbd_cpu.rs:402)
+    float tolerance;       // extension: stop when the pre-update residual max|C+α̃λ|/rest <= tolerance (0 = off)
+    uint32_t warm_start;   // extension: 1 = start from the given λ0 (warm_lambda) when it lowers the residual
 };
 
 template <typename T>
@@ -530,6 +532,8 @@ struct Sim {
     std::vector<uint32_t> ring_off, ring_idx;
     Params p{};
     uint64_t collision_pairs_last = 0;
+    uint32_t last_iterations = 0;  // convergence solve: update passes of the last substep
+    uint32_t last_fallback = 0;    // convergence solve: 1 if the warm start was rejected in the last substep
 
     static V cvt(const float* a, size_t i) { return {(T)a[3 * i], (T)a[3 * i + 1], (T)a[3 * i + 2]}; }
 
@@ -691,6 +695,66 @@ struct Sim {
             }
         }
         for (uint32_t i = 0; i < n; ++i) sim_pos[i] = jw[i];
+    }
+
+    // Extension: residual of constraint e at positions `pos` with multiplier `lam`: |C + α̃λ| / rest.
+    T constraint_residual(const std::vector<V>& pos, size_t e, T lam, T inv_dt_sq) const {
+        T len = length(pos[ci[e]] - pos[cj[e]]);
+        T c = len - rest[e];
+        T alpha_t = comp[e] * inv_dt_sq;
+        return std::fabs(c + alpha_t * lam) / rest[e];
+    }
+    // Extension: the gather of jacobi_gather_particle with Δλ replaced by `dl` (per constraint), from `src`.
+    void gather_with(const std::vector<V>& src, const std::vector<T>& dl, std::vector<V>& dst) {
+        std::vector<T> saved = delta_lambda;
+        delta_lambda = dl;
+        for (uint32_t i = 0; i < n; ++i) dst[i] = jacobi_gather_particle(i, src);
+        delta_lambda = saved;
+    }
+    // Extension: Jacobi substep (per-substep λ) iterating until the pre-update residual <= tolerance, at most
+    // p.inner_iterations passes. Warm start: positions move by the gather of λ0 (warm_lambda) and λ starts at λ0 —
+    // kept only if the resulting residual is not above the plain start's (otherwise plain: λ = 0).
+    void substep_converge() {
+        T inv_dt_sq = (T)p.inv_dt * (T)p.inv_dt;
+        predict_all();
+        std::vector<V>& start = jac_b;
+        for (uint32_t i = 0; i < n; ++i) start[i] = sim_pos[i];
+        std::fill(lambda.begin(), lambda.end(), (T)0);
+        last_fallback = 0;
+        if (p.warm_start && warm_lambda.size() == lambda.size()) {
+            T plain = 0;
+            for (size_t e = 0; e < ci.size(); ++e)
+                if (!(inv_mass[ci[e]] <= (T)0 && inv_mass[cj[e]] <= (T)0))
+                    plain = std::max(plain, constraint_residual(start, e, (T)0, inv_dt_sq));
+            gather_with(start, warm_lambda, jac_a);
+            T warm = 0;
+            for (size_t e = 0; e < ci.size(); ++e)
+                if (!(inv_mass[ci[e]] <= (T)0 && inv_mass[cj[e]] <= (T)0))
+                    warm = std::max(warm, constraint_residual(jac_a, e, warm_lambda[e], inv_dt_sq));
+            if (warm <= plain) {
+                for (uint32_t i = 0; i < n; ++i) start[i] = jac_a[i];
+                lambda = warm_lambda;
+            } else {
+                last_fallback = 1;
+            }
+        }
+        uint32_t it = 0;
+        std::vector<V>* cur = &jac_b;
+        std::vector<V>* nxt = &jac_a;
+        while (it < p.inner_iterations) {
+            T res = 0;
+            for (size_t e = 0; e < ci.size(); ++e)
+                if (!(inv_mass[ci[e]] <= (T)0 && inv_mass[cj[e]] <= (T)0))
+                    res = std::max(res, constraint_residual(*cur, e, lambda[e], inv_dt_sq));
+            jacobi_edges_pass(*cur, inv_dt_sq);
+            for (uint32_t i = 0; i < n; ++i) (*nxt)[i] = jacobi_gather_particle(i, *cur);
+            std::swap(cur, nxt);
+            ++it;
+            if (res <= (T)p.tolerance) break;
+        }
+        last_iterations = it;
+        for (uint32_t i = 0; i < n; ++i) sim_pos[i] = (*cur)[i];
+        post_velocity();
     }
 
     // Narrow phase of one pair (a<b), xpbd_cpu.rs:84-121. filter 1: reference rest-distance test (:94-100);

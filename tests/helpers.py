@@ -12,7 +12,8 @@ def oracle_params(params: P.XpbdCpuTimeStepParams, cfg: P.ClothSimConfig) -> dic
     d["grab_active"] = int(bool(d["grab_active"]))
     d.update(solver=cfg.solver, relaxation=cfg.relaxation, lambda_mode=cfg.lambda_mode, collision=cfg.collision,
              thickness=cfg.thickness, coll_scale=cfg.coll_scale, hash_cell=cfg.hash_cell,
-             ground_enabled=int(cfg.ground_enabled), ground_y=cfg.ground_y)
+             ground_enabled=int(cfg.ground_enabled), ground_y=cfg.ground_y, tolerance=cfg.tolerance,
+             warm_start=int(cfg.warm_start != 0))
     return d
 
 
