@@ -41,7 +41,7 @@ DEV_PARAMS_BYTES = 120  # sizeof(XpbdDevParams): the per-call parameter block up
 
 
 # ------------------------------------------------------------------------------------------------ workloads
-def make_workload(name: str, rank: int = 0, world: int = 1) -> dict:
+def make_workload(name: str, rank: int = 0, world: int = 1, c3_cloths: int = 0) -> dict:
     from bevy_xpbd_b200 import plugin as P
     from bevy_xpbd_b200 import workloads as wl
     dt, inv_dt = wl.substep_dt(10)
@@ -68,11 +68,14 @@ def make_workload(name: str, rank: int = 0, world: int = 1) -> dict:
         total_cloths = world
     elif name == "c3":
         allspecs = wl.config3_batch()
+        if c3_cloths:
+            allspecs = allspecs[:c3_cloths]
         specs = [s for k, s in enumerate(allspecs) if k % world == rank]
         prm = P.XpbdCpuTimeStepParams(float(dt), float(inv_dt), 1.0, 10)
         cfg = P.ClothSimConfig(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
-        desc = ("c3: 256 cloths, sides seeded uniform 16..192 vertices, random pins and stretch compliance, packed into "
-                "one persistent launch per frame, plain Jacobi (degree-averaged), 10 substeps x 10 iterations")
+        desc = (f"c3: {len(allspecs)} cloths, sides seeded uniform 16..192 vertices, random pins and stretch compliance, "
+                "packed into one persistent launch per frame, plain Jacobi (degree-averaged), 10 substeps x 10 "
+                "iterations")
         total_cloths = len(allspecs)
     else:
         raise ValueError(name)
@@ -285,19 +288,41 @@ def roofline(w: dict, mean_ms: float, kernel: str, peaks: dict) -> dict:
             "alg_bytes_per_launch": int(w["bytes_per_frame"]), "traffic": traffic}
 
 
+def fixed_schedule(args) -> bool:
+    return (args.no_autotune or args.jacobi_kernel is not None or args.block is not None or args.bps is not None
+            or args.cluster is not None)
+
+
+def apply_schedule(w: dict, plug, args):
+    """Autotuned schedule, or the one given on the command line (profiling runs pin it)."""
+    if not fixed_schedule(args):
+        return plug.autotune(frames=2)
+    cfg = w["cfg"]
+    if args.jacobi_kernel is not None:
+        cfg.jacobi_kernel = args.jacobi_kernel
+    if args.block is not None:
+        cfg.block_threads = args.block
+    if args.bps is not None:
+        cfg.blocks_per_sm = args.bps
+    if args.cluster is not None:
+        cfg.cluster_ctas = args.cluster
+    plug.set_params(w["params"], cfg)
+    return cfg
+
+
 def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks: dict, with_e2e: bool) -> dict:
-    w = make_workload(name, rank, world)
+    w = make_workload(name, rank, world, args.c3_cloths if name == "c3" else 0)
     t0 = time.time()
     plug = build_plugin(w, device)
     setup_s = time.time() - t0
-    tuned = plug.autotune(frames=2)
+    tuned = apply_schedule(w, plug, args)
     flush = working_set_bytes(w) < L2_BYTES
     steps = args.steps if name == args.workload else args.batched_steps
     total_ms, per, launches, clocks, st = time_device(w, plug, steps, args.warmup, world, device, flush)
     mean_ms = total_ms / steps
     cloth_steps = w["total_cloths"] * steps
     kernel = {0: "jacobi_persistent_kernel", 1: "gs_persistent_kernel", 2: "jacobi_patch_kernel",
-              3: "gs_cluster_kernel", 5: "jacobi_row_kernel"}[st["solver_kernel"]]
+              3: "gs_cluster_kernel", 5: "jacobi_row_kernel", 6: "jacobi_converge_kernel"}[st["solver_kernel"]]
     res = {
         "value": round(cloth_steps / (total_ms * 1e-3), 2),
         "ms_per_step": round(mean_ms, 4),
@@ -324,6 +349,95 @@ def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks:
     plug.close()
     res["_w"] = w
     return res
+
+
+# ------------------------------------------------------------------------------------------------ warm-start leg
+def run_warm_leg(args, device: int) -> dict:
+    """Convergence solve, learned vs plain (and previous-substep λ) warm start.
+
+    Per substep, Jacobi (degree-averaged) iterates each cloth until its max residual |C + α̃λ|/rest — the strain
+    |‖xi−xj‖−rest|/rest for the rigid (α = 0) constraints — is at or below 1e-4, capped at 1024 passes. Cloths: the
+    config-3 generator (sides 16..96, random pins, stretch compliance 10^U(-8,-3)), 48 for training (seed 31) and a
+    different 48 for the measurement (seed 32). Training data: 60 plain substeps of the training batch, every 28th
+    constraint; the MLP (BF16 tensor-core kernels) is fitted with 4000 Adam steps of 4096 samples. Measurement:
+    `warm_frames` frames (10 substeps each) per mode from the same initial state after one untimed frame; mean passes
+    per cloth-substep, fraction of cloth-substeps that hit the cap, and cloth-steps/s timed with CUDA events."""
+    import torch
+
+    from bevy_xpbd_b200 import plugin as P
+    from bevy_xpbd_b200 import workloads as wl
+    cap, tol = 1024, 1e-4
+    dt, inv_dt = wl.substep_dt(10)
+    prm = P.XpbdCpuTimeStepParams(float(dt), float(inv_dt), 1.0, cap, linear_drag_per_sec=0.01)
+
+    def cfg(warm):
+        return P.ClothSimConfig(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10,
+                                tolerance=tol, warm_start=warm)
+
+    train = wl.config3_batch(seed=31, count=48, side_lo=16, side_hi=96)
+    test = wl.config3_batch(seed=32, count=48, side_lo=16, side_hi=96)
+    t0 = time.time()
+    tr = P.ClothComputePlugin(device)
+    for sp in train:
+        tr.add_spec(sp)
+    tr.commit()
+    tr.set_params(prm, cfg(P.WARM_NONE))
+    tr.mlp_init(seed=1, capacity=1 << 21)
+    samples = tr.mlp_collect(60, stride=28)
+    tr.mlp_fit_normalization()
+    t1 = time.time()
+    l1 = tr.mlp_train(3000, batch=4096, lr=2e-3, seed=3)
+    l2 = tr.mlp_train(1000, batch=4096, lr=3e-4, seed=4)
+    torch.cuda.synchronize()
+    t2 = time.time()
+    params, norm = tr.mlp_params()
+    tr.close()
+    out = {"workload": "48 config-3 cloths (sides 16..96, seed 32; trained on another 48, seed 31), "
+                       f"tolerance {tol:g} on max |C + a~lambda|/rest, cap {cap} passes per substep, 10 substeps",
+           "train": {"samples": samples, "collect_s": round(t1 - t0, 2), "train_s": round(t2 - t1, 2),
+                     "adam_steps": 4000, "batch": 4096, "loss_first10": round(float(l1[:10].mean()), 4),
+                     "loss_last50": round(float(l2[-50:].mean()), 4)}}
+    n = sum(sp.num_particles for sp in test)
+    for name, warm in (("plain", P.WARM_NONE), ("previous", P.WARM_PREVIOUS), ("learned", P.WARM_LEARNED)):
+        q = P.ClothComputePlugin(device)
+        for sp in test:
+            q.add_spec(sp)
+        q.commit()
+        q.mlp_init(seed=0, capacity=16)
+        q.mlp_set_params(params, norm)
+        q.set_params(prm, cfg(warm))
+        stream = torch.cuda.Stream()
+        q.set_stream(stream.cuda_stream)
+        q.step(frames=1)
+        q.sync()
+        s0 = q.stats()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.warm_frames)]
+        per = []
+        for a, b in evs:
+            a.record(stream)
+            q.step(frames=1)
+            b.record(stream)
+            per.append(q.converge_cloth_iterations().astype(np.int64))  # last substep of the frame
+        torch.cuda.synchronize()
+        s1 = q.stats()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        its = s1["converge_iterations"] - s0["converge_iterations"]
+        cs = s1["converge_substeps"] - s0["converge_substeps"]
+        last = np.array(per)
+        out[name] = {"passes_per_cloth_substep": round(its / max(cs, 1), 2),
+                     "capped_frac_last_substeps": round(float((last >= cap).mean()), 4),
+                     "fallbacks": int(s1["warm_start_fallbacks"] - s0["warm_start_fallbacks"]),
+                     "cloth_steps_per_s": round(len(test) * args.warm_frames / (ms * 1e-3), 2),
+                     "ms_per_frame": round(ms / args.warm_frames, 3), "gpu_launches":
+                         int(s1["kernel_launches"] - s0["kernel_launches"]), "particles": n}
+        q.set_stream(None)
+        q.close()
+    p, l_ = out["plain"], out["learned"]
+    out["iteration_ratio_plain_over_learned"] = round(p["passes_per_cloth_substep"] /
+                                                      max(l_["passes_per_cloth_substep"], 1e-9), 3)
+    out["speed_ratio_learned_over_plain"] = round(l_["cloth_steps_per_s"] / max(p["cloth_steps_per_s"], 1e-9), 3)
+    return out
 
 
 # ------------------------------------------------------------------------------------------------ CPU arm
@@ -393,6 +507,15 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-warm", action="store_true", help="skip the learned-vs-plain convergence leg")
+    ap.add_argument("--warm-frames", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--c3-cloths", type=int, default=0, help="first K cloths of c3 only (profiling cases)")
+    ap.add_argument("--no-autotune", action="store_true", help="library default schedule")
+    ap.add_argument("--jacobi-kernel", type=int, default=None, help="1 warp tiles, 2 spatial patches, 3 rows")
+    ap.add_argument("--block", type=int, default=None)
+    ap.add_argument("--bps", type=int, default=None)
+    ap.add_argument("--cluster", type=int, default=None, help="Gauss-Seidel cluster size (0 = grid kernel)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -403,13 +526,13 @@ def main():
     import torch
     torch.cuda.set_device(local)
     peaks = load_peaks()
-    main_res = run_gpu_workload(args.workload, args, rank, world, local, peaks, with_e2e=True)
+    main_res = run_gpu_workload(args.workload, args, rank, world, local, peaks, with_e2e=not args.no_e2e)
     w = main_res.pop("_w")
     line = {"metric": METRIC, "value": main_res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": main_res["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded procedural sheets (no dataset)", "config": main_res["config"],
-            "roofline": main_res["roofline"], "e2e": main_res["e2e"], "gpu_launches": main_res["gpu_launches"],
+            "roofline": main_res["roofline"], "e2e": main_res.get("e2e"), "gpu_launches": main_res["gpu_launches"],
             "clocks": main_res["clocks"], "step_ms_min_max": main_res["step_ms_min_max"]}
     line["config"]["parallelism"] = ("replicas" if args.workload != "c3" else "cloth shards") + f" x{world}"
     if not args.no_batched and args.workload != "c3":
@@ -418,6 +541,8 @@ def main():
         line["batched"] = {"value": b["value"], "unit": UNIT, "ms_per_step": b["ms_per_step"], "steps": b["steps"],
                            "config": b["config"], "roofline": b["roofline"], "gpu_launches": b["gpu_launches"],
                            "clocks": b["clocks"]}
+    if rank == 0 and world == 1 and not args.no_warm:
+        line["warm_start"] = run_warm_leg(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_oracle_run(w, args.cpu_seconds, max_cloths=16 if args.workload == "c3" else None)
         line["cpu_baseline"] = {"value": round(r["value"], 4), "unit": UNIT, "cores": r["cores"], "kind": "port",

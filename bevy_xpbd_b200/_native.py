@@ -34,7 +34,7 @@ EXPORTED = [
     "xpbd_radix_sort_pairs_noalloc", "xpbd_set_warm_lambda", "xpbd_mlp_init", "xpbd_mlp_set_params",
     "xpbd_mlp_get_params", "xpbd_mlp_collect", "xpbd_mlp_dataset_size", "xpbd_mlp_dataset_read",
     "xpbd_mlp_fit_normalization", "xpbd_mlp_train", "xpbd_mlp_eval", "xpbd_mlp_gradients", "xpbd_mlp_predict_lambda",
-    "xpbd_converge_history",
+    "xpbd_converge_history", "xpbd_converge_cloth_iterations", "xpbd_selftest_division",
 ]
 MLP_PARAMS = 4865
 MLP_NORM = 20
@@ -141,6 +141,8 @@ def load():
         "xpbd_mlp_gradients": (I, [P, P, P, U, P, P]),
         "xpbd_mlp_predict_lambda": (I, [P, U, P]),
         "xpbd_converge_history": (I, [P, P, U, C.POINTER(U)]),
+        "xpbd_converge_cloth_iterations": (I, [P, P]),
+        "xpbd_selftest_division": (I, [I, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

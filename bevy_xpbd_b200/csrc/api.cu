@@ -477,12 +477,14 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     ALLOC(ctx->d_xyz, float, 3 * (size_t)N);
     float* warm_inc;
     uint32_t* inc_of_con_d;
-    unsigned *cloth_res_d, *iter_res_d;
+    unsigned *cloth_res_d, *iter_res_d, *cloth_ires_d, *cloth_iters_d;
     XpbdConvergeStats* cstats_d;
     ALLOC(warm_inc, float, inc.size());
     ALLOC(inc_of_con_d, uint32_t, 2 * (size_t)E);
     ALLOC(cloth_res_d, unsigned, 2 * (size_t)C);
     ALLOC(iter_res_d, unsigned, XPBD_MAX_CONVERGE_ITERS);
+    ALLOC(cloth_ires_d, unsigned, 3 * (size_t)C);
+    ALLOC(cloth_iters_d, unsigned, C);
     ALLOC(cstats_d, XpbdConvergeStats, 1);
     ALLOC(ctx->d_resid, unsigned, 4);
     cudaStream_t st = ctx->stream;
@@ -617,6 +619,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     W.inc_of_con = inc_of_con_d;
     W.cloth_res = cloth_res_d;
     W.iter_res = iter_res_d;
+    W.cloth_ires = cloth_ires_d;
+    W.cloth_iters = cloth_iters_d;
     W.cstats = cstats_d;
     ensure_pinned(ctx, 16 * (size_t)N);
     ctx->committed = true;
@@ -1105,7 +1109,7 @@ extern "C" int xpbd_read_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out) {
     if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const ClothHost& h = ctx->cloths[cloth_id];
-    const uint32_t kern = (ctx->kernel == 5 || ctx->kernel == 6) ? 0u : ctx->kernel;  // incidence λ table
+    const uint32_t kern = (ctx->kernel >= 5) ? 0u : ctx->kernel;  // rows / convergence solve: incidence λ
     const float* src = kern == 0 ? ctx->W.inc_lambda : (kern == 2 ? ctx->W.patch_lambda : ctx->W.con_lambda);
     const size_t cnt = kern == 0 ? ctx->W.n_inc : (kern == 2 ? ctx->W.patch_con_total : ctx->W.e);
     std::vector<float> all(std::max<size_t>(cnt, 1));
@@ -1164,6 +1168,16 @@ extern "C" int xpbd_converge_history(xpbd_ctx* ctx, float* residuals, uint32_t m
         CK(cudaMemcpyAsync(residuals, ctx->W.iter_res, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "history");
         CK(cudaStreamSynchronize(ctx->stream), "sync");
     }
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_converge_cloth_iterations(xpbd_ctx* ctx, uint32_t* out) {
+    if (!ctx || !out) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const uint32_t nc = (uint32_t)ctx->cloths.size();
+    if (nc) CK(cudaMemcpyAsync(out, ctx->W.cloth_iters, nc * 4, cudaMemcpyDeviceToHost, ctx->stream), "iters");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
     return XPBD_OK;
 }
 
@@ -1481,37 +1495,42 @@ extern "C" int xpbd_mlp_collect(xpbd_ctx* ctx, uint32_t substeps, uint32_t strid
     if (r != XPBD_OK) return r;
     if (!ctx->d_mlp) return fail(ctx, XPBD_ERR_STATE, "xpbd_mlp_init first");
     if (stride == 0) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "stride must be >= 1");
-    if (ctx->opts.solver != XPBD_SOLVER_JACOBI || ctx->opts.collision != XPBD_COLLISION_NONE)
-        return fail(ctx, XPBD_ERR_UNSUPPORTED, "collection runs the Jacobi convergence solve without collision");
+    if (ctx->kernel != 6) return fail(ctx, XPBD_ERR_STATE, "collection runs the convergence solve: set tolerance > 0");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
-    // the convergence solve's schedule, whatever the configured one
-    xpbd_solver_opts saved = ctx->opts;
-    ctx->opts.warm_start = XPBD_WARM_NONE;
-    if (!(ctx->opts.tolerance > 0.f)) ctx->opts.tolerance = 1e-30f;
-    fill_dev_params(ctx);
-    CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream), "p");
-    choose_schedule(ctx);
     cudaStream_t st = ctx->stream;
+    const uint32_t warm = ctx->opts.warm_start;
     cudaError_t e = cudaSuccess;
     for (uint32_t s = 0; s < substeps && e == cudaSuccess; ++s) {
         const uint32_t offset = ctx->collect_offset++ % stride;
         const uint32_t avail = ctx->W.e > offset ? (ctx->W.e - offset + stride - 1) / stride : 0;
         const uint32_t take = std::min(avail, ctx->ds_cap - ctx->ds_count);
+        uint64_t launches = 0;
         e = launch_converge_predict(ctx->W, ctx->sms, st);
-        if (e == cudaSuccess && take)
+        ++launches;
+        // features see the predicted positions and the previous substep's λ, before any warm start
+        if (e == cudaSuccess && take) {
             e = launch_mlp_collect_features(ctx->W, stride, offset, ctx->d_feat, ctx->d_scale, ctx->ds_count,
                                             ctx->ds_count + take, st);
-        if (e == cudaSuccess) e = launch_solver(6, ctx->block, ctx->grid, ctx->coop, ctx->W, 0u, 1, 0, 0, st);
-        if (e == cudaSuccess && take)
+            ++launches;
+        }
+        if (e == cudaSuccess && warm == XPBD_WARM_PREVIOUS && ctx->W.n_inc)
+            e = cudaMemcpyAsync(ctx->W.warm_lam_inc, ctx->W.inc_lambda, (size_t)ctx->W.n_inc * 4,
+                                cudaMemcpyDeviceToDevice, st);
+        else if (e == cudaSuccess && warm == XPBD_WARM_LEARNED)
+            e = launch_mlp_warm_start(ctx, st, &launches);
+        if (e == cudaSuccess) {
+            e = launch_solver(6, ctx->block, ctx->grid, ctx->coop, ctx->W, warm ? 1u : 0u, 1, 0, 0, st);
+            ++launches;
+        }
+        if (e == cudaSuccess && take) {
             e = launch_mlp_collect_targets(ctx->W, stride, offset, ctx->d_scale, ctx->d_target, ctx->ds_count,
                                            ctx->ds_count + take, st);
+            ++launches;
+        }
         ctx->ds_count += take;
-        ctx->stats.kernel_launches += take ? 4 : 2;
+        ctx->stats.kernel_launches += launches;
+        ctx->stats.substeps += 1;
     }
-    ctx->opts = saved;
-    fill_dev_params(ctx);
-    CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream), "p");
-    choose_schedule(ctx);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "collect");
     return read_status(ctx);
 }
@@ -1660,6 +1679,22 @@ extern "C" int xpbd_mlp_gradients(xpbd_ctx* ctx, const float* features, const fl
 }
 
 // ------------------------------------------------------------------------------------------------- diagnostics
+extern "C" int xpbd_selftest_division(int device, uint64_t count, uint64_t seed, uint64_t* mismatches) {
+    if (!mismatches) return XPBD_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return XPBD_ERR_NO_DEVICE;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return XPBD_ERR_CUDA;
+    unsigned long long* d = nullptr;
+    if (cudaMalloc(&d, sizeof(*d)) != cudaSuccess) return XPBD_ERR_OUT_OF_MEMORY;
+    cudaError_t e = cudaMemset(d, 0, sizeof(*d));
+    if (e == cudaSuccess) e = launch_division_selftest(count, seed, d, sms, 0);
+    unsigned long long h = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    *mismatches = h;
+    return e == cudaSuccess ? XPBD_OK : XPBD_ERR_CUDA;
+}
+
 extern "C" const char* xpbd_last_error(xpbd_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
 
 extern "C" const char* xpbd_status_string(int s) {

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "xpbd_fpdiv.h"
 #include "xpbd_internal.h"
 #include "xpbd_kernels.h"
 
@@ -31,7 +32,11 @@ __device__ __forceinline__ V3 v3(float4 a) { return {a.x, a.y, a.z}; }
 __device__ __forceinline__ V3 vadd(V3 a, V3 b) { return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)}; }
 __device__ __forceinline__ V3 vsub(V3 a, V3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
 __device__ __forceinline__ V3 vmul(V3 a, float s) { return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)}; }
-__device__ __forceinline__ V3 vdiv(V3 a, float s) { return {__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s)}; }
+__device__ __forceinline__ V3 vdiv(V3 a, float s) {  // correctly rounded, one shared reciprocal (xpbd_fpdiv.h)
+    V3 q;
+    fpdiv3(a.x, a.y, a.z, s, q.x, q.y, q.z);
+    return q;
+}
 __device__ __forceinline__ float vlen(V3 a) {
     return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)), __fmul_rn(a.z, a.z)));
 }

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "xpbd_fpdiv.h"
 #include "xpbd_internal.h"
 #include "xpbd_kernels.h"
 
@@ -37,7 +38,11 @@ __device__ __forceinline__ F3 f3(float4 a) { return {a.x, a.y, a.z}; }
 __device__ __forceinline__ F3 add3(F3 a, F3 b) { return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)}; }
 __device__ __forceinline__ F3 sub3(F3 a, F3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
 __device__ __forceinline__ F3 mul3(F3 a, float s) { return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)}; }
-__device__ __forceinline__ F3 div3(F3 a, float s) { return {__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s)}; }
+__device__ __forceinline__ F3 div3(F3 a, float s) {  // correctly rounded, one shared reciprocal (xpbd_fpdiv.h)
+    F3 q;
+    fpdiv3(a.x, a.y, a.z, s, q.x, q.y, q.z);
+    return q;
+}
 __device__ __forceinline__ F3 neg3(F3 a) { return {-a.x, -a.y, -a.z}; }
 // glam dot: (x*x' + y*y') + z*z'; length = sqrt(dot)
 __device__ __forceinline__ float dot3(F3 a, F3 b) {
@@ -364,54 +369,100 @@ __global__ void __launch_bounds__(BLOCK) jacobi_persistent_kernel(XpbdWorld W, u
 // constraint's Δλ exactly as jacobi_edges would (identical from either endpoint); the contributions of four
 // consecutive incidences are evaluated as independent dependency chains and then added in neighbour-table order,
 // so the sum is the reference's sequential one.
+// One incidence of row i (reference jacobi_edges recomputed from this endpoint, then its jacobi_gather term): the
+// correction (n̂·w_i)·Δλ, or zero where the reference skips the constraint (|d| < 1e-8) or has Δλ = 0 (w sum < 1e-8).
+// Branch-free: a skipped term is selected as +0, which leaves the running sum unchanged (the sum starts at +0 and
+// adding terms never yields -0).
+__device__ __forceinline__ F3 row_term(const F3 self, float wi, const float4 po, float rest, float alpha_t) {
+    const F3 gv = sub3(self, f3(po));
+    const float len = len3(gv);
+    const F3 nrm = div3(gv, len);
+    const float C = __fsub_rn(len, rest);
+    const float wsum = __fadd_rn(__fadd_rn(wi, po.w), alpha_t);
+    const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
+    const bool use = !(len < 1e-8f) && !(wsum < 1e-8f);
+    return {use ? __fmul_rn(__fmul_rn(nrm.x, wi), dlam) : 0.0f, use ? __fmul_rn(__fmul_rn(nrm.y, wi), dlam) : 0.0f,
+            use ? __fmul_rn(__fmul_rn(nrm.z, wi), dlam) : 0.0f};
+}
+
 __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevParams& P, uint32_t i,
                                            const float4* __restrict__ jin, float4* __restrict__ jout,
                                            TailMode tail) {
     const float4 ps = jin[i];
     if (ps.w <= 0.0f) return;
     const uint32_t rs = W.row_off[i], re = W.row_off[i + 1];
-    // the palette of the particle's cloth is found through the tile table (tiles are 32-particle aligned per cloth)
     const bool persist = P.lambda_mode != 0u;
+    const float* __restrict__ pal = W.palette_comp + (uint32_t)W.row_cloth[i] * XPBD_PALETTE;
+    const uint2* __restrict__ recs = W.inc;
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
     const F3 self = f3(ps);
-    for (uint32_t k = rs; k < re; k += 4) {
-        float cx[4], cy[4], cz[4];
+    if (!persist) {
+        // λ = 0 at every pass (reference mode): groups of four independent terms, then the remainder, summed in
+        // incidence order
+        uint32_t k = rs;
+        for (; k + 4 <= re; k += 4) {
+            F3 c[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            cx[u] = cy[u] = cz[u] = 0.0f;
-            const uint32_t kk = k + u;
-            if (kk >= re) continue;
-            const uint2 rec = W.inc[kk];
-            const float4 po = jin[rec.x & XPBD_OTHER_MASK];
-            const F3 gv = sub3(self, f3(po));
-            const float len = len3(gv);
-            if (len < 1e-8f) {
-                if (persist && tail == kTailFinalizePredict) W.inc_lambda[kk] = 0.0f;
-                continue;
+            for (int u = 0; u < 4; ++u) {
+                const uint2 rec = recs[k + u];
+                c[u] = row_term(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
+                                __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq));
             }
-            const F3 nrm = div3(gv, len);
-            const float C = __fsub_rn(len, __uint_as_float(rec.y));
-            const float alpha_t = __fmul_rn(W.palette_comp[W.row_cloth[i] * XPBD_PALETTE + (rec.x >> 28)], P.inv_dt_sq);
-            const float wsum = __fadd_rn(__fadd_rn(ps.w, po.w), alpha_t);
-            float dlam = 0.0f;
-            if (!(wsum < 1e-8f)) {
-                const float lam = persist ? W.inc_lambda[kk] : 0.0f;
-                dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
-                if (persist) W.inc_lambda[kk] = (tail == kTailFinalizePredict) ? 0.0f : __fadd_rn(lam, dlam);
-            } else if (persist && tail == kTailFinalizePredict) {
-                W.inc_lambda[kk] = 0.0f;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                ax = __fadd_rn(ax, c[u].x);
+                ay = __fadd_rn(ay, c[u].y);
+                az = __fadd_rn(az, c[u].z);
             }
-            cx[u] = __fmul_rn(__fmul_rn(nrm.x, ps.w), dlam);
-            cy[u] = __fmul_rn(__fmul_rn(nrm.y, ps.w), dlam);
-            cz[u] = __fmul_rn(__fmul_rn(nrm.z, ps.w), dlam);
         }
+        for (; k < re; ++k) {
+            const uint2 rec = recs[k];
+            const F3 c = row_term(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
+                                  __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq));
+            ax = __fadd_rn(ax, c.x);
+            ay = __fadd_rn(ay, c.y);
+            az = __fadd_rn(az, c.z);
+        }
+    } else {
+        for (uint32_t k = rs; k < re; k += 4) {
+            float cx[4], cy[4], cz[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (k + u < re) {
-                ax = __fadd_rn(ax, cx[u]);
-                ay = __fadd_rn(ay, cy[u]);
-                az = __fadd_rn(az, cz[u]);
+            for (int u = 0; u < 4; ++u) {
+                cx[u] = cy[u] = cz[u] = 0.0f;
+                const uint32_t kk = k + u;
+                if (kk >= re) continue;
+                const uint2 rec = recs[kk];
+                const float4 po = jin[rec.x & XPBD_OTHER_MASK];
+                const F3 gv = sub3(self, f3(po));
+                const float len = len3(gv);
+                if (len < 1e-8f) {
+                    if (tail == kTailFinalizePredict) W.inc_lambda[kk] = 0.0f;
+                    continue;
+                }
+                const F3 nrm = div3(gv, len);
+                const float C = __fsub_rn(len, __uint_as_float(rec.y));
+                const float alpha_t = __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq);
+                const float wsum = __fadd_rn(__fadd_rn(ps.w, po.w), alpha_t);
+                float dlam = 0.0f;
+                if (!(wsum < 1e-8f)) {
+                    const float lam = W.inc_lambda[kk];
+                    dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
+                    W.inc_lambda[kk] = (tail == kTailFinalizePredict) ? 0.0f : __fadd_rn(lam, dlam);
+                } else if (tail == kTailFinalizePredict) {
+                    W.inc_lambda[kk] = 0.0f;
+                }
+                cx[u] = __fmul_rn(__fmul_rn(nrm.x, ps.w), dlam);
+                cy[u] = __fmul_rn(__fmul_rn(nrm.y, ps.w), dlam);
+                cz[u] = __fmul_rn(__fmul_rn(nrm.z, ps.w), dlam);
             }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k + u < re) {
+                    ax = __fadd_rn(ax, cx[u]);
+                    ay = __fadd_rn(ay, cy[u]);
+                    az = __fadd_rn(az, cz[u]);
+                }
+        }
     }
     F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
     if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
@@ -435,8 +486,8 @@ __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevPara
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) jacobi_row_kernel(XpbdWorld W, uint32_t flags, uint32_t substeps,
-                                                           uint32_t pend, uint32_t start) {
+__device__ __forceinline__ void jacobi_rows_body(const XpbdWorld& W, uint32_t flags, uint32_t substeps, uint32_t pend,
+                                                 uint32_t start) {
     if (!status_clear(W)) return;
     const XpbdDevParams P = *W.params;
     const bool persist = P.lambda_mode != 0u;
@@ -483,6 +534,13 @@ __global__ void __launch_bounds__(BLOCK) jacobi_row_kernel(XpbdWorld W, uint32_t
     }
 }
 
+// Thread per particle over the row-ordered incidence table (kernel id 5).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) jacobi_row_kernel(XpbdWorld W, uint32_t flags, uint32_t substeps,
+                                                           uint32_t pend, uint32_t start) {
+    jacobi_rows_body<BLOCK>(W, flags, substeps, pend, start);
+}
+
 // ---------------------------------------------------------------------------------------------- convergence solve
 // Jacobi substep with λ kept over the substep, iterated until the pre-update residual max |C + α̃λ|/rest <= tolerance
 // (at most max_iterations passes), optionally warm-started from λ0: positions move by the reference gather with Δλ
@@ -512,6 +570,8 @@ __global__ void converge_predict_kernel(XpbdWorld W) {
     const XpbdDevParams P = *W.params;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
     for (uint32_t k = gtid; k < 2 * W.n_cloths; k += gstride) W.cloth_res[k] = 0u;
+    for (uint32_t k = gtid; k < 3 * W.n_cloths; k += gstride) W.cloth_ires[k] = 0u;
+    for (uint32_t k = gtid; k < W.n_cloths; k += gstride) W.cloth_iters[k] = 0u;
     for (uint32_t k = gtid; k < XPBD_MAX_CONVERGE_ITERS; k += gstride) W.iter_res[k] = 0u;
     for (uint32_t i = gtid; i < W.n; i += gstride) {
         const float4 x4 = W.x[i];
@@ -593,44 +653,73 @@ __global__ void __launch_bounds__(BLOCK) jacobi_converge_kernel(XpbdWorld W, uin
         for (uint32_t k = gtid; k < W.n_inc; k += gstride) W.inc_lambda[k] = 0.0f;
     }
     if (!grid_barrier(W, P)) return;
-    // iterations: residual of the state before each update pass, checked after the pass
+    // Iterations, per cloth: residual of the state before each update pass, checked after the pass; a cloth whose
+    // residual was at or below the tolerance stops (its iterate is carried over unchanged) and the loop ends when no
+    // cloth is left — each cloth takes the passes it would take alone. Per-cloth residuals rotate over three slots:
+    // slot it%3 is written in iteration it, read after its barrier, and cleared in iteration it+2.
     uint32_t cur = 0, it = 0;
     const uint32_t maxit = min(P.max_iterations, (uint32_t)XPBD_MAX_CONVERGE_ITERS);
+    const uint32_t nc = W.n_cloths, lane = threadIdx.x & 31u;
     while (it < maxit) {
         const float4* jin = W.jac[cur];
         float4* jout = W.jac[cur ^ 1u];
+        const unsigned* prev_res = W.cloth_ires + ((it + 2u) % 3u) * nc;
+        unsigned* cur_res = W.cloth_ires + (it % 3u) * nc;
         float rmax = 0.0f;
-        for (uint32_t i = gtid; i < W.n; i += gstride) {
-            const float4 ps = jin[i];
-            if (ps.w <= 0.0f) continue;
-            const uint32_t rs = W.row_off[i], re = W.row_off[i + 1];
-            const float* pal = W.palette_comp + (uint32_t)W.row_cloth[i] * XPBD_PALETTE;
-            float ax = 0.0f, ay = 0.0f, az = 0.0f;
-            for (uint32_t k = rs; k < re; ++k) {
-                const uint2 rec = W.inc[k];
-                const float4 po = jin[rec.x & XPBD_OTHER_MASK];
-                const F3 gv = sub3(f3(ps), f3(po));
-                const float len = len3(gv);
-                const float rest = __uint_as_float(rec.y);
-                const float alpha_t = __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq);
-                const float lam = W.inc_lambda[k];
-                rmax = fmaxf(rmax, residual_of(len, rest, alpha_t, lam));
-                if (len < 1e-8f) continue;
-                const F3 nrm = div3(gv, len);
-                const float C = __fsub_rn(len, rest);
-                const float wsum = __fadd_rn(__fadd_rn(ps.w, po.w), alpha_t);
-                if (wsum < 1e-8f) continue;
-                const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
-                W.inc_lambda[k] = __fadd_rn(lam, dlam);
-                ax = __fadd_rn(ax, __fmul_rn(__fmul_rn(nrm.x, ps.w), dlam));
-                ay = __fadd_rn(ay, __fmul_rn(__fmul_rn(nrm.y, ps.w), dlam));
-                az = __fadd_rn(az, __fmul_rn(__fmul_rn(nrm.z, ps.w), dlam));
+        for (uint32_t base = gtid - lane; base < W.n; base += gstride) {  // warp-uniform trip count
+            const uint32_t i = base + lane;
+            float ri = 0.0f;
+            uint32_t ci = 0u;
+            if (i < W.n) {
+                const float4 ps = jin[i];
+                ci = W.row_cloth[i];
+                const bool active = it == 0u || __uint_as_float(prev_res[ci]) > P.tolerance;
+                if (!active) {
+                    jout[i] = ps;
+                } else if (ps.w > 0.0f) {
+                    const uint32_t rs = W.row_off[i], re = W.row_off[i + 1];
+                    const float* pal = W.palette_comp + ci * XPBD_PALETTE;
+                    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+                    for (uint32_t k = rs; k < re; ++k) {
+                        const uint2 rec = W.inc[k];
+                        const float4 po = jin[rec.x & XPBD_OTHER_MASK];
+                        const F3 gv = sub3(f3(ps), f3(po));
+                        const float len = len3(gv);
+                        const float rest = __uint_as_float(rec.y);
+                        const float alpha_t = __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq);
+                        const float lam = W.inc_lambda[k];
+                        ri = fmaxf(ri, residual_of(len, rest, alpha_t, lam));
+                        if (len < 1e-8f) continue;
+                        const F3 nrm = div3(gv, len);
+                        const float C = __fsub_rn(len, rest);
+                        const float wsum = __fadd_rn(__fadd_rn(ps.w, po.w), alpha_t);
+                        if (wsum < 1e-8f) continue;
+                        const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, lam)), wsum);
+                        W.inc_lambda[k] = __fadd_rn(lam, dlam);
+                        ax = __fadd_rn(ax, __fmul_rn(__fmul_rn(nrm.x, ps.w), dlam));
+                        ay = __fadd_rn(ay, __fmul_rn(__fmul_rn(nrm.y, ps.w), dlam));
+                        az = __fadd_rn(az, __fmul_rn(__fmul_rn(nrm.z, ps.w), dlam));
+                    }
+                    F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
+                    if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
+                    delta = clamp_correction(delta);
+                    const F3 xn = add3(f3(ps), delta);
+                    jout[i] = make_float4(xn.x, xn.y, xn.z, ps.w);
+                }
             }
-            F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
-            if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
-            delta = clamp_correction(delta);
-            const F3 xn = add3(f3(ps), delta);
-            jout[i] = make_float4(xn.x, xn.y, xn.z, ps.w);
+            // per-cloth max: one atomic per cloth present in the warp
+            const bool has = ri > 0.0f;
+            const unsigned hm = __ballot_sync(kFull, has);
+            if (has) {
+                const unsigned grp = __match_any_sync(hm, ci);
+                const unsigned m = __reduce_max_sync(grp, __float_as_uint(ri));
+                if (lane == (uint32_t)(__ffs(grp) - 1)) atomicMax(&cur_res[ci], m);
+            }
+            rmax = fmaxf(rmax, ri);
+        }
+        for (uint32_t c = gtid; c < nc; c += gstride) {
+            W.cloth_ires[((it + 1u) % 3u) * nc + c] = 0u;
+            if (it == 0u || __uint_as_float(prev_res[c]) > P.tolerance) W.cloth_iters[c] += 1u;
         }
         block_max_atomic(rmax, &W.iter_res[it]);
         if (!grid_barrier(W, P)) return;
@@ -639,10 +728,12 @@ __global__ void __launch_bounds__(BLOCK) jacobi_converge_kernel(XpbdWorld W, uin
         ++it;
         if (res <= P.tolerance) break;
     }
+    for (uint32_t c = gtid; c < nc; c += gstride) {
+        atomicAdd(&W.cstats->iterations, (unsigned long long)W.cloth_iters[c]);
+        atomicMax(&W.cstats->max_iterations, W.cloth_iters[c]);
+    }
     if (gtid == 0) {
-        atomicAdd(&W.cstats->iterations, (unsigned long long)it);
-        atomicAdd(&W.cstats->substeps, 1ull);
-        atomicMax(&W.cstats->max_iterations, it);
+        atomicAdd(&W.cstats->substeps, (unsigned long long)nc);
         W.cstats->last_iterations = it;
     }
     // finalize (post_velocity) from the final iterate; pinned particles keep x, v
@@ -1013,12 +1104,14 @@ template <int BLOCK>
 static const void* patch_fn() { return (const void*)jacobi_patch_kernel<BLOCK>; }
 template <int BLOCK>
 static const void* row_fn() { return (const void*)jacobi_row_kernel<BLOCK>; }
+
 template <int BLOCK>
 static const void* converge_fn() { return (const void*)jacobi_converge_kernel<BLOCK>; }
 template <int BLOCK>
 static const void* gs_fn() { return (const void*)gs_persistent_kernel<BLOCK>; }
 
-// kernel 0: Jacobi over warp tiles, 1: Gauss–Seidel, 2: Jacobi over spatial patches, 5: Jacobi thread per particle
+// kernel 0: Jacobi over warp tiles, 1: Gauss–Seidel, 2: Jacobi over spatial patches, 5: Jacobi thread per particle,
+// 6: convergence solve
 const void* solver_kernel_fn(uint32_t solver, uint32_t block) {
     switch (solver * 10000 + block) {
         case 128: return jacobi_fn<128>();
@@ -1041,6 +1134,7 @@ const void* solver_kernel_fn(uint32_t solver, uint32_t block) {
         case 60256: return converge_fn<256>();
         case 60512: return converge_fn<512>();
         case 61024: return converge_fn<1024>();
+
     }
     return nullptr;
 }
@@ -1121,6 +1215,50 @@ cudaError_t launch_strain_residual(const XpbdWorld& W, uint32_t e0, uint32_t e1,
     if (grid > (uint32_t)sms * 4) grid = (uint32_t)sms * 4;
     if (grid == 0) grid = 1;
     strain_residual_kernel<<<grid, 256, 0, st>>>(W, e0, e1, out_bits);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------- self test
+// The shared-reciprocal division against the ordinary correctly rounded division on `count` operand triples drawn
+// (splitmix64 of the index) over all finite float bit patterns for the numerators and for the divisor.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ float finite_bits(uint32_t u) {
+    const float f = __uint_as_float(u);
+    return isfinite(f) ? f : __uint_as_float(u & 0xBF7FFFFFu);  // clear an exponent bit: finite
+}
+__global__ void division_selftest_kernel(uint64_t count, uint64_t seed, unsigned long long* mismatches) {
+    unsigned long long bad = 0;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < count;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r0 = splitmix64(seed ^ (2 * k)), r1 = splitmix64(seed ^ (2 * k + 1));
+        float ax = finite_bits((uint32_t)r0), ay = finite_bits((uint32_t)(r0 >> 32)), az = finite_bits((uint32_t)r1);
+        float b = finite_bits((uint32_t)(r1 >> 32));
+        // half the samples: operands of a cloth step (differences of nearby positions over their length)
+        if (k & 1ull) {
+            b = fabsf(b);
+            const float e = __uint_as_float(0x3F800000u | ((uint32_t)r1 & 0x7FFFFFu));  // [1, 2)
+            b = __fmul_rn(e, __uint_as_float((uint32_t)(((r1 >> 23) % 60u) + 97u) << 23));  // ~1e-9 .. 1e9
+            ax = __fmul_rn(b, __fmul_rn(__uint_as_float(0x3F800000u | ((uint32_t)r0 & 0x7FFFFFu)), -0.7f));
+            ay = __fmul_rn(b, __uint_as_float((uint32_t)(r0 >> 40) | 0x3E000000u));
+        }
+        float qx, qy, qz;
+        fpdiv3(ax, ay, az, b, qx, qy, qz);
+        const float rx = __fdiv_rn(ax, b), ry = __fdiv_rn(ay, b), rz = __fdiv_rn(az, b);
+        bad += (__float_as_uint(qx) != __float_as_uint(rx) && !(isnan(qx) && isnan(rx)));
+        bad += (__float_as_uint(qy) != __float_as_uint(ry) && !(isnan(qy) && isnan(ry)));
+        bad += (__float_as_uint(qz) != __float_as_uint(rz) && !(isnan(qz) && isnan(rz)));
+    }
+    for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(kFull, bad, o);
+    if ((threadIdx.x & 31u) == 0 && bad) atomicAdd(mismatches, bad);
+}
+cudaError_t launch_division_selftest(uint64_t count, uint64_t seed, unsigned long long* mismatches, int sms,
+                                     cudaStream_t st) {
+    division_selftest_kernel<<<sms * 8, 256, 0, st>>>(count, seed, mismatches);
     return cudaGetLastError();
 }
 

@@ -58,11 +58,11 @@ struct XpbdMlp {
 
 #define XPBD_MAX_CONVERGE_ITERS 4096
 struct XpbdConvergeStats {  // device counters of the convergence solve
-    unsigned long long iterations;  // update passes summed over substeps
-    unsigned long long substeps;
+    unsigned long long iterations;  // update passes summed over cloth-substeps
+    unsigned long long substeps;    // cloth-substeps
     unsigned long long fallbacks;   // cloth-substeps whose warm start was rejected
     unsigned int max_iterations;
-    unsigned int last_iterations;   // update passes of the most recent substep (its residuals stay in iter_res)
+    unsigned int last_iterations;   // passes of the most recent substep, slowest cloth (its residuals stay in iter_res)
 };
 
 struct XpbdGridSync {
@@ -127,6 +127,8 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     float* warm_lam_inc;            // λ0 per incidence
     const uint32_t* inc_of_con;     // per constraint (input order, packed): incidence of the i / j side (2 entries)
     unsigned* cloth_res;            // 2 per cloth: plain / warm start residual (float bits)
-    unsigned* iter_res;             // per iteration of a substep: residual (float bits)
+    unsigned* iter_res;             // per iteration of a substep: residual of the still-active cloths (float bits)
+    unsigned* cloth_ires;           // 3 x n_cloths: per-cloth residual of iterations it % 3 (float bits)
+    unsigned* cloth_iters;          // per cloth: update passes of the current substep
     XpbdConvergeStats* cstats;
 };

@@ -292,6 +292,12 @@ class ClothComputePlugin:
         self._check(self._L.xpbd_converge_history(self._h, _ptr(out), max_count, C.byref(c)))
         return out[: min(int(c.value), max_count)]
 
+    def converge_cloth_iterations(self) -> np.ndarray:
+        """Update passes each cloth took in the most recent convergence-solve substep."""
+        out = np.zeros(len(self._cloths), np.uint32)
+        self._check(self._L.xpbd_converge_cloth_iterations(self._h, _ptr(out)))
+        return out
+
     # ---- learned warm start (extension) ------------------------------------------------------------------------
     def mlp_init(self, seed: int = 0, capacity: int = 1 << 20):
         """Allocates the warm-start MLP (seeded initialisation) and room for `capacity` training samples."""
@@ -317,7 +323,7 @@ class ClothComputePlugin:
         return out
 
     def mlp_collect(self, substeps: int, stride: int = 1) -> int:
-        """Runs `substeps` plain convergence-solve substeps and stores (features, final λ target) samples."""
+        """Runs `substeps` convergence-solve substeps as configured and stores (features, final λ target) samples."""
         self._check(self._L.xpbd_mlp_collect(self._h, substeps, stride))
         c = C.c_uint32(0)
         self._check(self._L.xpbd_mlp_dataset_size(self._h, C.byref(c)))

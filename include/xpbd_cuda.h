@@ -193,6 +193,8 @@ int xpbd_read_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out);
 /* Convergence solve: the max pre-update residual max|C + α̃λ|/rest of each update pass of the most recent substep
  * (`count` = its number of passes; up to max_count values are copied). Extension: no reference counterpart. */
 int xpbd_converge_history(xpbd_ctx* ctx, float* residuals, uint32_t max_count, uint32_t* count);
+/* Convergence solve: update passes each cloth took in the most recent substep (out[num_cloths]). Extension. */
+int xpbd_converge_cloth_iterations(xpbd_ctx* ctx, uint32_t* out);
 /* Warm-start λ0 per constraint of a cloth (input order) for XPBD_WARM_GIVEN — extension. */
 int xpbd_set_warm_lambda(xpbd_ctx* ctx, uint32_t cloth_id, const float* lambda0);
 /* Max strain residual |‖xi−xj‖−rest|/rest over the constraints of a cloth (UINT32_MAX = all) — extension. */
@@ -259,8 +261,9 @@ int xpbd_mlp_get_params(xpbd_ctx* ctx, float* params, float* norm);
 /* λ0 the learned warm start would give cloth `cloth`'s constraints (input order) at the next substep's predicted
  * positions; the simulation state is unchanged. */
 int xpbd_mlp_predict_lambda(xpbd_ctx* ctx, uint32_t cloth, float* lambda0);
-/* Runs `substeps` substeps of the convergence solve (plain start; inner_iterations / tolerance as set) and stores, for
- * every `stride`-th constraint, its features at the substep's predicted positions and its final λ as the target. */
+/* Runs `substeps` substeps of the convergence solve as configured (tolerance > 0; warm start, inner_iterations as set)
+ * and stores, for every `stride`-th constraint (offset rotating per substep), its features at the substep's predicted
+ * positions and its final λ as the target. */
 int xpbd_mlp_collect(xpbd_ctx* ctx, uint32_t substeps, uint32_t stride);
 int xpbd_mlp_dataset_size(xpbd_ctx* ctx, uint32_t* count);
 /* Copies up to `max_rows` stored samples (raw features n x 9, targets t) to the host. */
@@ -282,6 +285,9 @@ const char* xpbd_status_string(int status);
 /* Test hook for failure detection: the next step's first grid barrier expects one block more than the grid has,
  * so it can never complete and times out after `timeout_ms`, setting XPBD_ERR_BARRIER_TIMEOUT. */
 int xpbd_debug_force_barrier_timeout(xpbd_ctx* ctx, float timeout_ms);
+/* Self test of the kernels' shared-reciprocal division (three quotients from one correctly rounded reciprocal) against
+ * the ordinary correctly rounded division on `count` random operand triples: *mismatches = differing quotients. */
+int xpbd_selftest_division(int device, uint64_t count, uint64_t seed, uint64_t* mismatches);
 
 #ifdef __cplusplus
 }

@@ -106,3 +106,32 @@ def test_converge_rejects_unsupported_modes():
         plug.set_params(prm, _cfg(collision=P.COLLISION_REST_FILTER))
     with pytest.raises(P.XpbdError):       # learned start without a network
         plug.set_params(prm, _cfg(warm_start=P.WARM_LEARNED))
+
+
+def test_converge_batched_cloths_stop_independently():
+    """Three cloths in one context: each takes the passes it takes alone (per-cloth early exit), bit-exact."""
+    specs = [wl.make_sheet(s, 1.0, 1.0, "top_edge", seed=5 + s) for s in (12, 24, 16)]
+    prm = params_for(4, 160, 1.0, drag=0.01)
+    for warm in (P.WARM_NONE, P.WARM_PREVIOUS):
+        cfg = _cfg(warm_start=warm)
+        plug = gpu_sim(specs, prm, cfg)
+        oracles = [oracle_sim(sp, prm, cfg) for sp in specs]
+        if warm:
+            for sp, o in zip(specs, oracles):
+                o.set_warm_lambda(np.zeros(len(sp.constraint_i), np.float32))
+        tot, seen = 0, set()
+        for s in range(8):
+            plug.substep(1)
+            per = plug.converge_cloth_iterations()
+            for c, o in enumerate(oracles):
+                it, _ = o.substeps_converge(1)
+                if warm:
+                    o.set_warm_lambda(o.lambdas().astype(np.float32))
+                assert int(per[c]) == int(it[0]), (warm, s, c)
+                tot += int(it[0])
+                seen.add(int(it[0]))
+                assert max_abs(plug.positions(c), o.state()[0]) == 0.0, (warm, s, c)
+        st = plug.stats()
+        assert st["converge_iterations"] == tot
+        assert st["converge_substeps"] == 8 * len(specs)
+        assert len(seen) > 2          # the cloths stopped after different numbers of passes

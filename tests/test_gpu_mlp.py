@@ -211,21 +211,30 @@ def test_learned_warm_start_bit_exact_against_oracle_with_same_lambda0():
 
 
 def test_learned_warm_start_reduces_iterations(record_property):
-    """Train on one run of the sheet, then run the same later substeps plain and learned from identical states."""
-    sp, prm = _sheet(24)
-    cfg = _cfg()
-    plug, losses = _trained(sp, prm, cfg, substeps=32, steps=600)
-    assert losses[-50:].mean() < 0.5 * losses[:10].mean()
+    """Train on one batch of config-3 cloths (varied stiffness), then run a different batch plain and learned from the
+    same initial state: the learned start needs fewer update passes per cloth-substep to reach the tolerance."""
+    cap = 1024
+    prm = params_for(10, cap, 1.0, drag=0.01)
+    cfg = _cfg(solve_substeps=10)
+    train = wl.config3_batch(seed=31, count=48, side_lo=16, side_hi=96)
+    test = wl.config3_batch(seed=32, count=48, side_lo=16, side_hi=96)
+    plug = gpu_sim(train, prm, cfg)
+    plug.mlp_init(seed=11, capacity=1 << 21)
+    plug.mlp_collect(40, stride=28)
+    plug.mlp_fit_normalization()
+    losses = np.concatenate([plug.mlp_train(1500, batch=4096, lr=2e-3, seed=11),
+                             plug.mlp_train(500, batch=4096, lr=3e-4, seed=12)])
+    assert np.all(np.isfinite(losses))
+    assert losses[-200:].mean() < losses[:20].mean()      # per-batch losses are heavy-tailed: compare means
     params, norm = plug.mlp_params()
     runs = {}
     for name, warm in (("plain", P.WARM_NONE), ("previous", P.WARM_PREVIOUS), ("learned", P.WARM_LEARNED)):
-        q = gpu_sim(sp, prm, cfg)
+        q = gpu_sim(test, prm, cfg)
         q.mlp_init(seed=0, capacity=16)
         q.mlp_set_params(params, norm)
-        q.substep(32)                                      # the training trajectory's states
-        q.set_params(prm, _cfg(warm_start=warm))
-        s0 = q.stats()["converge_iterations"]
-        q.substep(16)
-        runs[name] = q.stats()["converge_iterations"] - s0
-        record_property(f"iterations_{name}", runs[name])
+        q.set_params(prm, _cfg(solve_substeps=10, warm_start=warm))
+        q.step(frames=2)
+        st = q.stats()
+        runs[name] = st["converge_iterations"] / st["converge_substeps"]
+        record_property(f"passes_per_cloth_substep_{name}", runs[name])
     assert runs["learned"] < runs["plain"]

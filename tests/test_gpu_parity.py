@@ -334,8 +334,9 @@ def test_gauss_seidel_execution_paths_bit_exact(cluster):
 @pytest.mark.parametrize("kernel", [1, 2, 3], ids=["warp_tiles", "spatial_patches", "thread_rows"])
 @pytest.mark.parametrize("lam", [P.LAMBDA_RESET_PER_ITERATION, P.LAMBDA_PER_SUBSTEP], ids=["lambda_reset", "lambda_substep"])
 def test_jacobi_execution_paths_bit_exact(kernel, lam):
-    """Both Jacobi executions — warp tiles over the neighbour table and shared-memory spatial patches that solve each
-    constraint once — give the reference result on a batch of uneven cloths, in both λ modes."""
+    """Every Jacobi execution — warp tiles over the neighbour table, shared-memory spatial patches that solve each
+    constraint once, thread per particle over the incidence table — gives the reference result on a batch of uneven
+    cloths, in both λ modes."""
     specs = wl.config3_batch(seed=13, count=5, side_lo=20, side_hi=70)
     prm = params_for(10, 10, 1.0)
     cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, lambda_mode=lam, solve_substeps=10,
