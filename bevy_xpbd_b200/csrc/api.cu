@@ -1246,7 +1246,7 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
         uint32_t block, bps, cl, jk;
     };
     std::vector<Cand> cands;
-    const uint32_t blocks[] = {128, 256, 512};
+    const uint32_t blocks[] = {128, 256, 512, 1024};
     const uint32_t jks[3] = {2, 3, 1};
     for (uint32_t jk : jks) {
         if (base.solver != XPBD_SOLVER_JACOBI && jk != 1) continue;
