@@ -64,41 +64,60 @@ __global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(const uint32_t* 
     counts[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Single-block exclusive scan of `m` u32 values in place (each thread scans a contiguous chunk).
-__global__ void __launch_bounds__(1024) exclusive_scan_kernel(uint32_t* __restrict__ a, uint32_t m,
-                                                               uint32_t* __restrict__ total) {
+// Single-block exclusive scan of `m` u32 values in place, in chunks of 4 × blockDim.x: each chunk is loaded
+// coalesced into shared memory, every thread scans 4 consecutive values, a warp-shuffle + shared-memory scan combines
+// the threads, and a running carry links the chunks. Launch with 1024 threads.
+constexpr uint32_t kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) exclusive_scan_kernel(uint32_t* __restrict__ a, uint32_t m,
+                                                                      uint32_t* __restrict__ total) {
+    __shared__ uint32_t s[4 * kScanThreads];
     __shared__ uint32_t ws[32];
-    const uint32_t per = (m + blockDim.x - 1) / blockDim.x;
-    const uint32_t b0 = threadIdx.x * per;
-    const uint32_t b1 = min(b0 + per, m);
-    uint32_t sum = 0;
-    for (uint32_t k = b0; k < b1; ++k) sum += a[k];
-    // block exclusive scan of per-thread sums
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t incl = sum;
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(kFullMask, incl, o);
-        if (lane >= (uint32_t)o) incl += t;
-    }
-    if (lane == 31) ws[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t v = (lane < (blockDim.x >> 5)) ? ws[lane] : 0u;
-        uint32_t inc2 = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(kFullMask, inc2, o);
-            if (lane >= (uint32_t)o) inc2 += t;
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < m; base += 4 * kScanThreads) {
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+            const uint32_t i = base + k * kScanThreads + t;
+            s[k * kScanThreads + t] = i < m ? a[i] : 0u;
         }
-        ws[lane] = inc2 - v;
+        __syncthreads();
+        const uint32_t v0 = s[4 * t], v1 = s[4 * t + 1], v2 = s[4 * t + 2], v3 = s[4 * t + 3];
+        const uint32_t sum = v0 + v1 + v2 + v3;
+        uint32_t incl = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(kFullMask, incl, o);
+            if (lane >= (uint32_t)o) incl += x;
+        }
+        if (lane == 31) ws[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t v = ws[lane];
+            uint32_t inc2 = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t x = __shfl_up_sync(kFullMask, inc2, o);
+                if (lane >= (uint32_t)o) inc2 += x;
+            }
+            ws[lane] = inc2 - v;  // exclusive prefix of the warps' sums
+            if (lane == 31) s[0] = inc2;  // chunk total (s[0] is no longer read: v0 is in registers)
+        }
+        __syncthreads();
+        const uint32_t ex = carry + ws[warp] + incl - sum;
+        const uint32_t chunk_total = s[0];
+        __syncthreads();  // everyone has read s[0] and ws before they are overwritten
+        s[4 * t] = ex;
+        s[4 * t + 1] = ex + v0;
+        s[4 * t + 2] = ex + v0 + v1;
+        s[4 * t + 3] = ex + v0 + v1 + v2;
+        __syncthreads();
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+            const uint32_t i = base + k * kScanThreads + t;
+            if (i < m) a[i] = s[k * kScanThreads + t];
+        }
+        carry += chunk_total;
+        __syncthreads();  // the next chunk's loads overwrite s
     }
-    __syncthreads();
-    uint32_t run = ws[warp] + incl - sum;
-    for (uint32_t k = b0; k < b1; ++k) {
-        uint32_t t = a[k];
-        a[k] = run;
-        run += t;
-    }
-    if (total && threadIdx.x == blockDim.x - 1) *total = run;
+    if (total && t == 0) *total = carry;
 }
 
 __global__ void __launch_bounds__(kSortBlock) radix_scatter_kernel(const uint32_t* __restrict__ keys_in,
@@ -183,7 +202,7 @@ cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, u
         uint32_t* dv = to_out ? vals_out : tmp_v;
         const uint32_t shift = 8u * p;
         radix_hist_kernel<<<tiles, kSortBlock, 0, st>>>(src_k, n, shift, tiles, counts);
-        exclusive_scan_kernel<<<1, 1024, 0, st>>>(counts, 256 * tiles, nullptr);
+        exclusive_scan_kernel<<<1, kScanThreads, 0, st>>>(counts, 256 * tiles, nullptr);
         radix_scatter_kernel<<<tiles, kSortBlock, 0, st>>>(src_k, src_v, dk, dv, n, shift, tiles, counts);
         if (launches) *launches += 3;
         src_k = dk;
@@ -466,7 +485,7 @@ cudaError_t collision_pairs(const XpbdWorld& W, const float4* pos, const Collisi
     pair_count_kernel<<<grid, 128, 0, st>>>(W, pos, B, inv_cell, filter, B.pair_count);
     cudaError_t e = cudaMemsetAsync(B.pair_count + W.n, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    exclusive_scan_kernel<<<1, 1024, 0, st>>>(B.pair_count, W.n + 1, nullptr);
+    exclusive_scan_kernel<<<1, kScanThreads, 0, st>>>(B.pair_count, W.n + 1, nullptr);
     uint32_t h_total = 0;
     e = cudaMemcpyAsync(&h_total, B.pair_count + W.n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return e;
