@@ -223,7 +223,11 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
                         V3 gv = vsub(p_i, p_j);
                         const float len = vlen(gv);
                         if (len < 1e-8f) continue;
-                        gv = vdiv(gv, len);
+                        {
+                            V3 q;
+                            if (!fpdiv3_by_length_fast(gv.x, gv.y, gv.z, len, q.x, q.y, q.z)) q = vdiv(gv, len);
+                            gv = q;
+                        }
                         const float C = __fsub_rn(len, __uint_as_float(cr.z));
                         const float alpha_t = __fmul_rn(__uint_as_float(cr.w), P.inv_dt_sq);
                         const float wsum = __fadd_rn(__fadd_rn(w_i, w_j), alpha_t);

@@ -373,10 +373,16 @@ __global__ void __launch_bounds__(BLOCK) jacobi_persistent_kernel(XpbdWorld W, u
 // correction (n̂·w_i)·Δλ, or zero where the reference skips the constraint (|d| < 1e-8) or has Δλ = 0 (w sum < 1e-8).
 // Branch-free: a skipped term is selected as +0, which leaves the running sum unchanged (the sum starts at +0 and
 // adding terms never yields -0).
-__device__ __forceinline__ F3 row_term(const F3 self, float wi, const float4 po, float rest, float alpha_t) {
+template <bool EXACT_FALLBACK>
+__device__ __forceinline__ F3 row_term(const F3 self, float wi, const float4 po, float rest, float alpha_t, bool& ok) {
     const F3 gv = sub3(self, f3(po));
     const float len = len3(gv);
-    const F3 nrm = div3(gv, len);
+    F3 nrm;
+    if (EXACT_FALLBACK) {
+        nrm = div3(gv, len);
+    } else {
+        ok = fpdiv3_by_length_fast(gv.x, gv.y, gv.z, len, nrm.x, nrm.y, nrm.z) | (len < 1e-8f);  // skipped: fine
+    }
     const float C = __fsub_rn(len, rest);
     const float wsum = __fadd_rn(__fadd_rn(wi, po.w), alpha_t);
     const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
@@ -402,11 +408,23 @@ __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevPara
         uint32_t k = rs;
         for (; k + 4 <= re; k += 4) {
             F3 c[4];
+            bool ok = true;
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const uint2 rec = recs[k + u];
-                c[u] = row_term(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
-                                __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq));
+                bool oku = true;
+                c[u] = row_term<false>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
+                                       __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq), oku);
+                ok &= oku;
+            }
+            if (!ok) {  // an operand outside the shared-reciprocal range (tiny nonzero component): exact division
+#pragma unroll 1
+                for (int u = 0; u < 4; ++u) {
+                    const uint2 rec = recs[k + u];
+                    bool unused = true;
+                    c[u] = row_term<true>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
+                                          __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq), unused);
+                }
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
@@ -417,8 +435,9 @@ __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevPara
         }
         for (; k < re; ++k) {
             const uint2 rec = recs[k];
-            const F3 c = row_term(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
-                                  __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq));
+            bool unused = true;
+            const F3 c = row_term<true>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
+                                        __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq), unused);
             ax = __fadd_rn(ax, c.x);
             ay = __fadd_rn(ay, c.y);
             az = __fadd_rn(az, c.z);
@@ -1245,13 +1264,27 @@ __global__ void division_selftest_kernel(uint64_t count, uint64_t seed, unsigned
             b = __fmul_rn(e, __uint_as_float((uint32_t)(((r1 >> 23) % 60u) + 97u) << 23));  // ~1e-9 .. 1e9
             ax = __fmul_rn(b, __fmul_rn(__uint_as_float(0x3F800000u | ((uint32_t)r0 & 0x7FFFFFu)), -0.7f));
             ay = __fmul_rn(b, __uint_as_float((uint32_t)(r0 >> 40) | 0x3E000000u));
+            if ((k & 6ull) == 2ull) az = 0.0f;                                        // exact zero component
+            if ((k & 6ull) == 4ull) az = __fmul_rn(az, 0x1p-100f);                      // tiny component
         }
         float qx, qy, qz;
         fpdiv3(ax, ay, az, b, qx, qy, qz);
-        const float rx = __fdiv_rn(ax, b), ry = __fdiv_rn(ay, b), rz = __fdiv_rn(az, b);
+        float rx = __fdiv_rn(ax, b), ry = __fdiv_rn(ay, b), rz = __fdiv_rn(az, b);
         bad += (__float_as_uint(qx) != __float_as_uint(rx) && !(isnan(qx) && isnan(rx)));
         bad += (__float_as_uint(qy) != __float_as_uint(ry) && !(isnan(qy) && isnan(ry)));
         bad += (__float_as_uint(qz) != __float_as_uint(rz) && !(isnan(qz) && isnan(rz)));
+        // a vector over its own correctly rounded length: where the fast path reports success it must be exact
+        {
+            const float len = len3(F3{ax, ay, az});
+            if (fpdiv3_by_length_fast(ax, ay, az, len, qx, qy, qz)) {
+                rx = __fdiv_rn(ax, len);
+                ry = __fdiv_rn(ay, len);
+                rz = __fdiv_rn(az, len);
+                bad += (__float_as_uint(qx) != __float_as_uint(rx));
+                bad += (__float_as_uint(qy) != __float_as_uint(ry));
+                bad += (__float_as_uint(qz) != __float_as_uint(rz));
+            }
+        }
     }
     for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(kFull, bad, o);
     if ((threadIdx.x & 31u) == 0 && bad) atomicAdd(mismatches, bad);

@@ -17,13 +17,42 @@ namespace xpbd {
 
 __device__ __forceinline__ bool fpdiv_num_ok(float a) {
     const float m = fabsf(a);
-    return (m >= 0x1p-60f && m <= 0x1p60f) || a == 0.0f;
+    return ((m >= 0x1p-60f) & (m <= 0x1p60f)) | (a == 0.0f);
 }
 
 __device__ __forceinline__ float fpdiv_step(float a, float b, float y) {
     const float q = __fmul_rn(a, y);
     const float r = __fmaf_rn(-b, q, a);
     return a == 0.0f ? q : __fmaf_rn(r, y, q);
+}
+
+// The shared-reciprocal quotients without the fallback branch: returns whether every operand is in the range where
+// they are the correctly rounded ones. Hot loops evaluate this for a group of terms and recompute the rare group with
+// a failing operand through fpdiv3, so the common path carries no branch.
+__device__ __forceinline__ bool fpdiv3_fast(float ax, float ay, float az, float b, float& qx, float& qy, float& qz) {
+    const float y = __frcp_rn(b);
+    qx = fpdiv_step(ax, b, y);
+    qy = fpdiv_step(ay, b, y);
+    qz = fpdiv_step(az, b, y);
+    const float mb = fabsf(b);
+    return (mb >= 0x1p-60f) & (mb <= 0x1p60f) & fpdiv_num_ok(ax) & fpdiv_num_ok(ay) & fpdiv_num_ok(az);
+}
+
+// fpdiv3_fast for the components of a vector divided by its own computed length b = |a| (so |a_k| <= b·(1 + 2^-23)
+// and no quotient can overflow): the range test reduces to 2^-60 <= b <= 2^60 and every a_k zero or >= 2^-60 in
+// magnitude, evaluated on the bit patterns — (bits << 1) - 1 wraps zero to the top, so one unsigned minimum over the
+// three components tests "zero or exponent >= 67" at once.
+__device__ __forceinline__ bool fpdiv3_by_length_fast(float ax, float ay, float az, float b, float& qx, float& qy,
+                                                      float& qz) {
+    const float y = __frcp_rn(b);
+    qx = fpdiv_step(ax, b, y);
+    qy = fpdiv_step(ay, b, y);
+    qz = fpdiv_step(az, b, y);
+    const uint32_t mx = (__float_as_uint(ax) << 1) - 1u, my = (__float_as_uint(ay) << 1) - 1u,
+                   mz = (__float_as_uint(az) << 1) - 1u;
+    const uint32_t mn = min(mx, min(my, mz));
+    const bool b_ok = ((__float_as_uint(b) & 0x7FFFFFFFu) - (67u << 23)) < (120u << 23);  // 2^-60 <= |b| < 2^60
+    return b_ok & (mn >= (67u << 24) - 1u);
 }
 
 // {ax, ay, az} / b, each correctly rounded.
