@@ -441,12 +441,14 @@ def run_warm_leg(args, device: int) -> dict:
 
 
 # ------------------------------------------------------------------------------------------------ CPU arm
-def cpu_oracle_run(w: dict, budget_s: float, max_cloths: int | None = None, min_frames: int = 1):
-    """Times the OpenMP build of the CPU restatement of xpbd_cpu.rs on a bounded sample of workload `w`: every
-    `len/max_cloths`-th cloth, as many whole frames as fit in `budget_s` (at least `min_frames`)."""
+def cpu_oracle_run(w: dict, budget_s: float, max_cloths: int | None = None, min_frames: int = 1,
+                   variant: str = "omp"):
+    """Times the CPU restatement of xpbd_cpu.rs (OpenMP build, or the serial build with the reference's loop order)
+    on a bounded sample of workload `w`: every `len/max_cloths`-th cloth, as many whole frames as fit in `budget_s`
+    (at least `min_frames`)."""
     from oracle import oracle as orc
     from tests.helpers import oracle_params
-    orc.select("omp")
+    orc.select(variant)
     specs = w["specs"]
     if max_cloths is not None and len(specs) > max_cloths:
         specs = specs[:: len(specs) // max_cloths][:max_cloths]
@@ -471,7 +473,7 @@ def cpu_oracle_run(w: dict, budget_s: float, max_cloths: int | None = None, min_
             s.substeps(S)
     t1 = time.perf_counter()
     return dict(value=len(sims) * frames / (t1 - t0), frames=frames, cloths=len(sims), seconds=t1 - t0,
-                cores=orc.threads(), per_frame_s=(t1 - t0) / frames)
+                cores=orc.threads() if variant == "omp" else 1, per_frame_s=(t1 - t0) / frames)
 
 
 def run_reference(args, rank: int, world: int):
@@ -533,12 +535,14 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded procedural sheets (no dataset)", "config": main_res["config"],
             "roofline": main_res["roofline"], "e2e": main_res.get("e2e"), "gpu_launches": main_res["gpu_launches"],
-            "clocks": main_res["clocks"], "step_ms_min_max": main_res["step_ms_min_max"]}
+            "clocks": main_res["clocks"], "step_ms_min_max": main_res["step_ms_min_max"],
+            "substeps_per_s": round(main_res["value"] * w["cfg"].solve_substeps, 1)}
     line["config"]["parallelism"] = ("replicas" if args.workload != "c3" else "cloth shards") + f" x{world}"
     if not args.no_batched and args.workload != "c3":
         b = run_gpu_workload("c3", args, rank, world, local, peaks, with_e2e=False)
         b.pop("_w")
         line["batched"] = {"value": b["value"], "unit": UNIT, "ms_per_step": b["ms_per_step"], "steps": b["steps"],
+                           "substeps_per_s": round(b["value"] * 10, 1),
                            "config": b["config"], "roofline": b["roofline"], "gpu_launches": b["gpu_launches"],
                            "clocks": b["clocks"]}
     if rank == 0 and world == 1 and not args.no_warm:
@@ -548,6 +552,11 @@ def main():
         line["cpu_baseline"] = {"value": round(r["value"], 4), "unit": UNIT, "cores": r["cores"], "kind": "port",
                                 "sample": f"{r['frames']} frames of {r['cloths']} cloth(s) of the workload, "
                                           f"{r['seconds']:.1f} s, OpenMP build of the oracle"}
+        r1 = cpu_oracle_run(w, args.cpu_seconds / 3, max_cloths=16 if args.workload == "c3" else None,
+                            variant="serial")
+        line["cpu_baseline_serial"] = {"value": round(r1["value"], 4), "unit": UNIT, "cores": 1, "kind": "port",
+                                       "sample": f"{r1['frames']} frames of {r1['cloths']} cloth(s), "
+                                                 f"{r1['seconds']:.1f} s, serial build (the reference's loop order)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -1588,6 +1588,18 @@ extern "C" int xpbd_mlp_fit_normalization(xpbd_ctx* ctx) {
     return mlp_upload_norm(ctx);
 }
 
+// Minibatch indices drawn from the stored samples: xorshift64 seeded with `seed`, index = z % count.
+static void draw_indices(uint64_t seed, size_t count, uint32_t n, std::vector<uint32_t>& idx) {
+    idx.resize(count);
+    uint64_t z = seed ^ 0xD1B54A32D192ED03ull;
+    for (size_t k = 0; k < count; ++k) {
+        z ^= z << 13;
+        z ^= z >> 7;
+        z ^= z << 17;
+        idx[k] = (uint32_t)(z % n);
+    }
+}
+
 extern "C" int xpbd_mlp_train(xpbd_ctx* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses) {
     if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
     if (!ctx->d_mlp || ctx->ds_count == 0) return fail(ctx, XPBD_ERR_STATE, "no stored samples");
@@ -1600,14 +1612,8 @@ extern "C" int xpbd_mlp_train(xpbd_ctx* ctx, uint32_t steps, uint32_t batch, flo
         if (err != cudaSuccess) return cuda_fail(ctx, err, "batch indices");
         ctx->idx_cap = (uint32_t)need;
     }
-    std::vector<uint32_t> idx(need);
-    uint64_t z = seed ^ 0xD1B54A32D192ED03ull;
-    for (size_t k = 0; k < need; ++k) {
-        z ^= z << 13;
-        z ^= z >> 7;
-        z ^= z << 17;
-        idx[k] = (uint32_t)(z % ctx->ds_count);
-    }
+    std::vector<uint32_t> idx;
+    draw_indices(seed, need, ctx->ds_count, idx);
     cudaStream_t st = ctx->stream;
     CK(cudaMemcpyAsync(ctx->d_idx, idx.data(), need * 4, cudaMemcpyHostToDevice, st), "indices");
     CK(cudaMemsetAsync(ctx->d_loss, 0, steps * 4, st), "memset");
@@ -1618,7 +1624,7 @@ extern "C" int xpbd_mlp_train(xpbd_ctx* ctx, uint32_t steps, uint32_t batch, flo
         CK(launch_mlp_train(ctx->d_mlp, ctx->d_feat, ctx->d_target, ctx->d_idx + (size_t)s * batch, batch,
                             ctx->d_grads, ctx->d_loss + s, st), "train");
         const float bc1 = 1.f - powf(b1, (float)ctx->adam_step), bc2 = 1.f - powf(b2, (float)ctx->adam_step);
-        CK(launch_mlp_adam(ctx->d_master, ctx->d_m1, ctx->d_m2, ctx->d_grads, lr, b1, b2, eps, bc1, bc2, ctx->d_mlp,
+        CK(launch_mlp_adam(ctx->d_master, ctx->d_m1, ctx->d_m2, ctx->d_grads, 1.0f, lr, b1, b2, eps, bc1, bc2, ctx->d_mlp,
                            st), "adam");
         ctx->stats.kernel_launches += 3;
     }
@@ -1628,6 +1634,43 @@ extern "C" int xpbd_mlp_train(xpbd_ctx* ctx, uint32_t steps, uint32_t batch, flo
         for (uint32_t s = 0; s < steps; ++s) losses[s] /= (float)batch;
     }
     return read_status(ctx);
+}
+
+extern "C" int xpbd_mlp_minibatch_gradients(xpbd_ctx* ctx, uint32_t batch, uint64_t seed, float* grads,
+                                            float* loss) {
+    if (!ctx || !grads || !loss || batch == 0) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->d_mlp || ctx->ds_count == 0) return fail(ctx, XPBD_ERR_STATE, "no stored samples");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (batch > ctx->idx_cap) {
+        cudaError_t err = cudaSuccess;
+        ctx->d_idx = dev_alloc<uint32_t>(ctx, batch, &err);
+        if (err != cudaSuccess) return cuda_fail(ctx, err, "batch indices");
+        ctx->idx_cap = batch;
+    }
+    std::vector<uint32_t> idx;
+    draw_indices(seed, batch, ctx->ds_count, idx);
+    cudaStream_t st = ctx->stream;
+    // the copy must not overwrite indices an earlier launch on this stream still reads
+    CK(cudaStreamSynchronize(st), "sync");
+    CK(cudaMemcpyAsync(ctx->d_idx, idx.data(), (size_t)batch * 4, cudaMemcpyHostToDevice, st), "indices");
+    CK(cudaMemsetAsync(grads, 0, XPBD_MLP_PARAMS * 4, st), "memset");
+    CK(cudaMemsetAsync(loss, 0, 4, st), "memset");
+    CK(launch_mlp_train(ctx->d_mlp, ctx->d_feat, ctx->d_target, ctx->d_idx, batch, grads, loss, st), "train");
+    ctx->stats.kernel_launches += 1;
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_mlp_apply_gradients(xpbd_ctx* ctx, const float* grads, float scale, float lr) {
+    if (!ctx || !grads) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->d_mlp) return fail(ctx, XPBD_ERR_STATE, "xpbd_mlp_init first");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    ++ctx->adam_step;
+    const float bc1 = 1.f - powf(b1, (float)ctx->adam_step), bc2 = 1.f - powf(b2, (float)ctx->adam_step);
+    CK(launch_mlp_adam(ctx->d_master, ctx->d_m1, ctx->d_m2, grads, scale, lr, b1, b2, eps, bc1, bc2, ctx->d_mlp,
+                       ctx->stream), "adam");
+    ctx->stats.kernel_launches += 2;
+    return XPBD_OK;
 }
 
 extern "C" int xpbd_mlp_eval(xpbd_ctx* ctx, const float* features, uint32_t n, float* out) {

@@ -476,10 +476,10 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(const XpbdMlp* __restric
 
 // ---- Adam on the fp32 master parameters, then the bf16 working copy
 __global__ void mlp_adam_kernel(float* __restrict__ master, float* __restrict__ m1, float* __restrict__ m2,
-                                const float* __restrict__ grads, float lr, float beta1, float beta2, float eps,
-                                float bc1, float bc2, XpbdMlp* __restrict__ mlp) {
+                                const float* __restrict__ grads, float gscale, float lr, float beta1, float beta2,
+                                float eps, float bc1, float bc2, XpbdMlp* __restrict__ mlp) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < XPBD_MLP_PARAMS; k += gridDim.x * blockDim.x) {
-        const float gk = grads[k];
+        const float gk = grads[k] * gscale;
         const float a = beta1 * m1[k] + (1.0f - beta1) * gk;
         const float b = beta2 * m2[k] + (1.0f - beta2) * gk * gk;
         m1[k] = a;
@@ -545,9 +545,9 @@ cudaError_t launch_mlp_train(const XpbdMlp* mlp, const float* feat, const float*
     mlp_train_kernel<<<grid, 128, smem, st>>>(mlp, feat, target, idx, nrows, grads, loss);
     return cudaGetLastError();
 }
-cudaError_t launch_mlp_adam(float* master, float* m1, float* m2, const float* grads, float lr, float beta1,
-                            float beta2, float eps, float bc1, float bc2, XpbdMlp* mlp, cudaStream_t st) {
-    mlp_adam_kernel<<<20, 256, 0, st>>>(master, m1, m2, grads, lr, beta1, beta2, eps, bc1, bc2, mlp);
+cudaError_t launch_mlp_adam(float* master, float* m1, float* m2, const float* grads, float gscale, float lr,
+                            float beta1, float beta2, float eps, float bc1, float bc2, XpbdMlp* mlp, cudaStream_t st) {
+    mlp_adam_kernel<<<20, 256, 0, st>>>(master, m1, m2, grads, gscale, lr, beta1, beta2, eps, bc1, bc2, mlp);
     mlp_publish_kernel<<<1, 256, 0, st>>>(master, mlp);
     return cudaGetLastError();
 }

@@ -33,8 +33,8 @@ cudaError_t launch_mlp_collect_targets(const XpbdWorld& W, uint32_t stride, uint
                                        float* target, uint32_t base, uint32_t cap, cudaStream_t st);
 cudaError_t launch_mlp_train(const XpbdMlp* mlp, const float* feat, const float* target, const uint32_t* idx,
                              uint32_t nrows, float* grads, float* loss, cudaStream_t st);
-cudaError_t launch_mlp_adam(float* master, float* m1, float* m2, const float* grads, float lr, float beta1,
-                            float beta2, float eps, float bc1, float bc2, XpbdMlp* mlp, cudaStream_t st);
+cudaError_t launch_mlp_adam(float* master, float* m1, float* m2, const float* grads, float gscale, float lr,
+                            float beta1, float beta2, float eps, float bc1, float bc2, XpbdMlp* mlp, cudaStream_t st);
 cudaError_t launch_mlp_publish(const float* master, XpbdMlp* mlp, cudaStream_t st);
 
 // ---- cluster Gauss–Seidel (cluster_gs.cu)

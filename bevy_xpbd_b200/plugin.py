@@ -347,6 +347,16 @@ class ClothComputePlugin:
         self._check(self._L.xpbd_mlp_train(self._h, steps, batch, C.c_float(lr), seed, _ptr(losses)))
         return losses
 
+    def mlp_minibatch_gradients(self, batch: int, seed: int, grads_ptr: int, loss_ptr: int):
+        """Asynchronous: gradient of a seeded minibatch into the device buffer at grads_ptr (4,865 floats)."""
+        self._check(self._L.xpbd_mlp_minibatch_gradients(self._h, batch, seed, C.c_void_p(grads_ptr),
+                                                         C.c_void_p(loss_ptr)))
+
+    def mlp_apply_gradients(self, grads_ptr: int, scale: float, lr: float):
+        """Asynchronous: one Adam step with the device gradient at grads_ptr times `scale`."""
+        self._check(self._L.xpbd_mlp_apply_gradients(self._h, C.c_void_p(grads_ptr), C.c_float(scale),
+                                                     C.c_float(lr)))
+
     def mlp_eval(self, features) -> np.ndarray:
         f = _f32(features)
         n = f.size // N.MLP_FEATURES

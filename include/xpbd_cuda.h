@@ -273,6 +273,13 @@ int xpbd_mlp_fit_normalization(xpbd_ctx* ctx);
 /* `steps` Adam steps on minibatches of `batch` samples drawn (seeded) from the stored set; losses[steps] (may be NULL)
  * receives each step's mean squared error of the standardised target. */
 int xpbd_mlp_train(xpbd_ctx* ctx, uint32_t steps, uint32_t batch, float lr, uint64_t seed, float* losses);
+/* Data-parallel training, one step in two calls so that the caller can sum the gradients over ranks in between (one
+ * all-reduce of XPBD_MLP_PARAMS floats per step). Both run asynchronously on the context's stream; `grads` and `loss`
+ * are device pointers. minibatch_gradients: gradient of the mean loss over `batch` stored samples drawn with `seed`
+ * (xorshift64, as xpbd_mlp_train), written to grads[XPBD_MLP_PARAMS], the summed squared error to loss[0].
+ * apply_gradients: one Adam step with the gradient grads·scale (scale = 1/ranks after a summing all-reduce). */
+int xpbd_mlp_minibatch_gradients(xpbd_ctx* ctx, uint32_t batch, uint64_t seed, float* grads, float* loss);
+int xpbd_mlp_apply_gradients(xpbd_ctx* ctx, const float* grads, float scale, float lr);
 /* Standardised prediction for n raw feature rows (host arrays). */
 int xpbd_mlp_eval(xpbd_ctx* ctx, const float* features, uint32_t n, float* out);
 /* Gradient of mean((y - (t - f1 - tmean)/tstd)^2) over n rows w.r.t. the XPBD_MLP_PARAMS parameters (host arrays). */

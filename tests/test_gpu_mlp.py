@@ -238,3 +238,25 @@ def test_learned_warm_start_reduces_iterations(record_property):
         runs[name] = st["converge_iterations"] / st["converge_substeps"]
         record_property(f"passes_per_cloth_substep_{name}", runs[name])
     assert runs["learned"] < runs["plain"]
+
+
+def test_data_parallel_training_step_matches_oracle():
+    """The two-call step used for multi-GPU training (minibatch gradient into a caller buffer, then Adam with the
+    scaled buffer), run through bevy_xpbd_b200.mlp_train on one GPU, against the oracle's gradient and Adam."""
+    from bevy_xpbd_b200 import mlp_train
+    sp, prm = _sheet(16)
+    plug = gpu_sim(sp, prm, _cfg())
+    plug.mlp_init(seed=4, capacity=1 << 14)
+    n = plug.mlp_collect(2, stride=1)
+    p0 = plug.mlp_params()[0]
+    lr = 1e-3
+    losses = mlp_train.train_on_gpus(plug, steps=1, batch=512, lr=lr, seed=5)
+    p1, norm = plug.mlp_params()
+    f, t = plug.mlp_dataset()
+    idx = MO.xorshift_indices(mlp_train.minibatch_seed(5, 0, 0), 512, n)
+    g_ref, loss_ref = MO.gradients(p0, norm, f[idx], t[idx])
+    assert abs(losses[0] - loss_ref) <= 1e-3 * max(loss_ref, 1e-6)
+    p1_ref, _, _ = MO.adam(p0, np.zeros_like(p0), np.zeros_like(p0), g_ref, 1, lr)
+    big = np.abs(g_ref) > 1e-2 * np.abs(g_ref).max()
+    assert big.sum() > 100
+    np.testing.assert_allclose(p1[big], p1_ref[big], atol=1e-5 * lr * 100)
