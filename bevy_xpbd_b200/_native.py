@@ -35,7 +35,7 @@ EXPORTED = [
     "xpbd_mlp_get_params", "xpbd_mlp_collect", "xpbd_mlp_dataset_size", "xpbd_mlp_dataset_read",
     "xpbd_mlp_fit_normalization", "xpbd_mlp_train", "xpbd_mlp_eval", "xpbd_mlp_gradients", "xpbd_mlp_predict_lambda",
     "xpbd_converge_history", "xpbd_converge_cloth_iterations", "xpbd_selftest_division",
-    "xpbd_mlp_minibatch_gradients", "xpbd_mlp_apply_gradients",
+    "xpbd_mlp_minibatch_gradients", "xpbd_mlp_apply_gradients", "xpbd_set_triangles", "xpbd_read_normals",
 ]
 MLP_PARAMS = 4865
 MLP_NORM = 20
@@ -146,6 +146,8 @@ def load():
         "xpbd_selftest_division": (I, [I, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]),
         "xpbd_mlp_minibatch_gradients": (I, [P, U, C.c_uint64, P, P]),
         "xpbd_mlp_apply_gradients": (I, [P, P, C.c_float, C.c_float]),
+        "xpbd_set_triangles": (I, [P, U, U, P]),
+        "xpbd_read_normals": (I, [P, U, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -39,6 +39,7 @@ struct ClothHost {
     std::vector<uint32_t> lambda_gs;   // per input constraint: position in the color-major table
     std::vector<uint32_t> lambda_patch;  // per input constraint: patch slot holding its λ, or UINT32_MAX
     std::vector<uint32_t> inc_i, inc_j;  // per input constraint: incidence in the i / j particle's row (or MAX)
+    std::vector<uint32_t> tris;          // render triangles (local vertex indices), for the vertex normals
 };
 
 struct DeviceBuf {
@@ -294,6 +295,17 @@ static void ensure_pinned(xpbd_ctx* ctx, size_t bytes) {
     if (cudaHostAlloc((void**)&ctx->pinned, bytes, cudaHostAllocDefault) == cudaSuccess) ctx->pinned_bytes = bytes;
 }
 
+extern "C" int xpbd_set_triangles(xpbd_ctx* ctx, uint32_t cloth_id, uint32_t num_tris, const uint32_t* tri_indices) {
+    if (!ctx || (num_tris && !tri_indices)) return XPBD_ERR_INVALID_ARGUMENT;
+    if (ctx->committed) return fail(ctx, XPBD_ERR_STATE, "xpbd_set_triangles after xpbd_commit");
+    if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+    ClothHost& c = ctx->cloths[cloth_id];
+    for (size_t k = 0; k < 3 * (size_t)num_tris; ++k)
+        if (tri_indices[k] >= c.n) return fail(ctx, XPBD_ERR_INDEX_RANGE, "triangle vertex index out of range");
+    c.tris.assign(tri_indices, tri_indices + 3 * (size_t)num_tris);
+    return XPBD_OK;
+}
+
 extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
     if (ctx->committed) return fail(ctx, XPBD_ERR_STATE, "already committed");
@@ -487,6 +499,36 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     ALLOC(cloth_iters_d, unsigned, C);
     ALLOC(cstats_d, XpbdConvergeStats, 1);
     ALLOC(ctx->d_resid, unsigned, 4);
+    // render triangles: packed global vertex indices and the vertex → triangle table for the vertex normals
+    std::vector<uint4> tri_all;
+    for (auto& c : ctx->cloths)
+        for (size_t t = 0; t + 2 < c.tris.size(); t += 3)
+            tri_all.push_back(make_uint4(c.tris[t] + c.vtx_off, c.tris[t + 1] + c.vtx_off, c.tris[t + 2] + c.vtx_off, 0u));
+    const uint32_t T = (uint32_t)tri_all.size();
+    std::vector<uint32_t> vt_off(N + 1, 0), vt_tri(3 * (size_t)T);
+    for (const uint4& t : tri_all) {
+        ++vt_off[t.x + 1];
+        ++vt_off[t.y + 1];
+        ++vt_off[t.z + 1];
+    }
+    for (uint32_t v = 0; v < N; ++v) vt_off[v + 1] += vt_off[v];
+    {
+        std::vector<uint32_t> cur(vt_off.begin(), vt_off.end() - 1);
+        for (uint32_t t = 0; t < T; ++t) {
+            vt_tri[cur[tri_all[t].x]++] = t;
+            vt_tri[cur[tri_all[t].y]++] = t;
+            vt_tri[cur[tri_all[t].z]++] = t;
+        }
+    }
+    uint4* tris_d = nullptr;
+    uint32_t *vt_off_d = nullptr, *vt_tri_d = nullptr;
+    float4* normals_d = nullptr;
+    if (T) {
+        ALLOC(tris_d, uint4, T);
+        ALLOC(vt_off_d, uint32_t, N + 1);
+        ALLOC(vt_tri_d, uint32_t, 3 * (size_t)T);
+        ALLOC(normals_d, float4, N);
+    }
     cudaStream_t st = ctx->stream;
 #define H2D(dst, src, bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st), "upload")
     H2D(x, hx.data(), N * sizeof(float4));
@@ -621,6 +663,17 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     W.iter_res = iter_res_d;
     W.cloth_ires = cloth_ires_d;
     W.cloth_iters = cloth_iters_d;
+    W.n_tris = T;
+    W.tris = tris_d;
+    W.vt_off = vt_off_d;
+    W.vt_tri = vt_tri_d;
+    W.normals = normals_d;
+    if (T) {
+        H2D(tris_d, tri_all.data(), T * sizeof(uint4));
+        H2D(vt_off_d, vt_off.data(), (N + 1) * sizeof(uint32_t));
+        H2D(vt_tri_d, vt_tri.data(), 3 * (size_t)T * sizeof(uint32_t));
+        CK(cudaStreamSynchronize(st), "commit sync");
+    }
     W.cstats = cstats_d;
     ensure_pinned(ctx, 16 * (size_t)N);
     ctx->committed = true;
@@ -1101,6 +1154,17 @@ extern "C" int xpbd_reset(xpbd_ctx* ctx) {
     if (ctx->W.patch_lambda)
         CK(cudaMemset(ctx->W.patch_lambda, 0, std::max<size_t>(ctx->W.patch_con_total, 1) * 4), "memset");
     return XPBD_OK;
+}
+
+extern "C" int xpbd_read_normals(xpbd_ctx* ctx, uint32_t cloth_id, float* out_xyz) {
+    if (!ctx || !out_xyz) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+    if (ctx->W.n_tris == 0) return fail(ctx, XPBD_ERR_STATE, "no triangles: xpbd_set_triangles before xpbd_commit");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(launch_vertex_normals(ctx->W, ctx->sms, ctx->stream), "normals");
+    ctx->stats.kernel_launches += 1;
+    return read_vec(ctx, ctx->W.normals, cloth_id, out_xyz);
 }
 
 extern "C" int xpbd_read_lambda(xpbd_ctx* ctx, uint32_t cloth_id, float* out) {

@@ -1237,6 +1237,44 @@ cudaError_t launch_strain_residual(const XpbdWorld& W, uint32_t e0, uint32_t e1,
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------------------------- vertex normals
+// accumulate_normals + finalize_normals (cloth_sim_jacobi.wgsl:492-547): per triangle c = cross(p1 - p0, p2 - p0),
+// converted to fixed point i32(c · 33333) (round toward zero, saturating) and summed into each of its three vertices;
+// then n = f32(sum) / 33333, normalised when |n| > 1e-8, else (0, 1, 0). The reference sums with integer atomics; here
+// each vertex gathers its triangles from a vertex → triangle table (no atomics). Integer sums (wrapping, as i32
+// atomics wrap) do not depend on order, so the result is the same bits either way.
+__device__ __forceinline__ int fixed_normal(float c) { return __float2int_rz(__fmul_rn(c, 33333.0f)); }
+
+__global__ void vertex_normals_kernel(XpbdWorld W) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < W.n; v += gridDim.x * blockDim.x) {
+        uint32_t sx = 0u, sy = 0u, sz = 0u;  // i32 sums with wrap-around
+        for (uint32_t k = W.vt_off[v]; k < W.vt_off[v + 1]; ++k) {
+            const uint4 t = W.tris[W.vt_tri[k]];
+            const F3 p0 = f3(W.x[t.x]), p1 = f3(W.x[t.y]), p2 = f3(W.x[t.z]);
+            const F3 e0 = sub3(p1, p0), e1 = sub3(p2, p0);
+            const float cx = __fsub_rn(__fmul_rn(e0.y, e1.z), __fmul_rn(e0.z, e1.y));
+            const float cy = __fsub_rn(__fmul_rn(e0.z, e1.x), __fmul_rn(e0.x, e1.z));
+            const float cz = __fsub_rn(__fmul_rn(e0.x, e1.y), __fmul_rn(e0.y, e1.x));
+            sx += (uint32_t)fixed_normal(cx);
+            sy += (uint32_t)fixed_normal(cy);
+            sz += (uint32_t)fixed_normal(cz);
+        }
+        F3 n = {__fdiv_rn(__int2float_rn((int)sx), 33333.0f), __fdiv_rn(__int2float_rn((int)sy), 33333.0f),
+                __fdiv_rn(__int2float_rn((int)sz), 33333.0f)};
+        const float ln = len3(n);
+        n = (ln > 1e-8f) ? div3(n, ln) : F3{0.0f, 1.0f, 0.0f};
+        W.normals[v] = make_float4(n.x, n.y, n.z, 0.0f);
+    }
+}
+
+cudaError_t launch_vertex_normals(const XpbdWorld& W, int sms, cudaStream_t st) {
+    uint32_t grid = (W.n + 255) / 256;
+    if (grid > (uint32_t)sms * 8) grid = (uint32_t)sms * 8;
+    if (grid == 0) grid = 1;
+    vertex_normals_kernel<<<grid, 256, 0, st>>>(W);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------------------------- self test
 // The shared-reciprocal division against the ordinary correctly rounded division on `count` operand triples drawn
 // (splitmix64 of the index) over all finite float bit patterns for the numerators and for the divisor.

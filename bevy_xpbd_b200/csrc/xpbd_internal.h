@@ -130,5 +130,11 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     unsigned* iter_res;             // per iteration of a substep: residual of the still-active cloths (float bits)
     unsigned* cloth_ires;           // 3 x n_cloths: per-cloth residual of iterations it % 3 (float bits)
     unsigned* cloth_iters;          // per cloth: update passes of the current substep
+    // render triangles (vertex normals)
+    uint32_t n_tris;
+    const uint4* tris;              // global vertex indices {a, b, c, 0}
+    const uint32_t* vt_off;         // vertex → triangle table (CSR over vertices, triangles ascending)
+    const uint32_t* vt_tri;
+    float4* normals;
     XpbdConvergeStats* cstats;
 };

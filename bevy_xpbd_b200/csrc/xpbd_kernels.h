@@ -21,6 +21,7 @@ cudaError_t launch_converge_predict(const XpbdWorld& W, int sms, cudaStream_t st
 cudaError_t launch_strain_residual(const XpbdWorld& W, uint32_t e0, uint32_t e1, unsigned* out_bits, int sms,
                                    cudaStream_t st);
 
+cudaError_t launch_vertex_normals(const XpbdWorld& W, int sms, cudaStream_t st);
 cudaError_t launch_division_selftest(uint64_t count, uint64_t seed, unsigned long long* mismatches, int sms,
                                      cudaStream_t st);
 

@@ -216,6 +216,17 @@ class ClothComputePlugin:
         return self.add_cloth(spec.positions, spec.inv_mass, spec.constraint_i, spec.constraint_j, spec.rest_len,
                               spec.compliance, spec.velocities, spec.rest_positions, spec.constraint_type, order)
 
+    def set_triangles(self, cloth: int, tri_indices):
+        """Render triangles (local vertex indices, 3 per triangle) of a cloth, for `normals`."""
+        t = _u32(tri_indices).reshape(-1)
+        self._check(self._L.xpbd_set_triangles(self._h, cloth, t.size // 3, _ptr(t)))
+
+    def normals(self, cloth: int = 0) -> np.ndarray:
+        """Vertex normals of the current positions (accumulate_normals + finalize_normals)."""
+        out = np.empty((self._cloths[cloth][0], 3), np.float32)
+        self._check(self._L.xpbd_read_normals(self._h, cloth, _ptr(out)))
+        return out
+
     def commit(self):
         self._check(self._L.xpbd_commit(self._h))
 
@@ -428,3 +439,7 @@ class ClothMaterialPlugin:
 
     def render_positions(self, cloth: int | None = None) -> np.ndarray:
         return self.compute.positions(cloth)
+
+    def render_normals(self, cloth: int = 0) -> np.ndarray:
+        """render_normals of the reference (finalize_normals, cloth_sim_jacobi.wgsl:528-547)."""
+        return self.compute.normals(cloth)

@@ -140,6 +140,14 @@ def config2_sheet(seed: int = 2, side: int = 512) -> ClothSpec:
     return make_sheet(side, 2.0, 1.0, "none", jitter=0.0, seed=seed, velocity=vel)
 
 
+def sheet_triangles(s: int) -> np.ndarray:
+    """Two render triangles per quad of an s×s sheet (vertex r*s + c), counter-clockwise seen from +y."""
+    r, c = np.meshgrid(np.arange(s - 1), np.arange(s - 1), indexing="ij")
+    i = (r * s + c).ravel()
+    t = np.stack([np.stack([i, i + s, i + 1], 1), np.stack([i + 1, i + s, i + s + 1], 1)], 1)
+    return t.reshape(-1, 3).astype(np.uint32)
+
+
 def config3_batch(seed: int = 3, count: int = 256, side_lo: int = 16, side_hi: int = 192) -> list[ClothSpec]:
     """`count` square cloths, side uniform in [side_lo, side_hi] vertices, random pin pattern and log-uniform
     stretch compliance in [1e-8, 1e-3]; shear and bend as config 0."""

@@ -167,6 +167,11 @@ int xpbd_set_stream(xpbd_ctx* ctx, void* stream);
 int xpbd_add_cloth(xpbd_ctx* ctx, const xpbd_cloth_desc* desc, uint32_t* cloth_id);
 /* Builds coloring, neighbour tables and device buffers for every added cloth. */
 int xpbd_commit(xpbd_ctx* ctx);
+/* Render triangles of a cloth (3 local vertex indices each; before xpbd_commit), for xpbd_read_normals. */
+int xpbd_set_triangles(xpbd_ctx* ctx, uint32_t cloth_id, uint32_t num_tris, const uint32_t* tri_indices);
+/* Vertex normals of the current positions, accumulate_normals + finalize_normals (cloth_sim_jacobi.wgsl:492-547):
+ * area-weighted fixed-point sums (×33333, truncation) normalised, (0, 1, 0) where degenerate. xyz per vertex. */
+int xpbd_read_normals(xpbd_ctx* ctx, uint32_t cloth_id, float* out_xyz);
 
 /* ---- per-frame --------------------------------------------------------------------------------------------- */
 /* prepare_cloth_bind_groups_jacobi's per-frame ClothSimParamsGpu::pack upload (cloth_jacobi.rs:583-584). */
