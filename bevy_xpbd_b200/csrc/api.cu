@@ -15,6 +15,8 @@
 #include <map>
 #include <string>
 #include <vector>
+#include <thread>
+#include <atomic>
 
 #include "../../include/xpbd_cuda.h"
 #include "mesh_prep.h"
@@ -313,23 +315,36 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const uint32_t C = (uint32_t)ctx->cloths.size();
     uint32_t N = 0, E = 0, max_colors = 0;
-    // ---- coloring + per-cloth offsets
+    // ---- coloring (cloths are independent: one host thread per cloth at a time) + per-cloth offsets
+    {
+        std::atomic<uint32_t> next{0};
+        auto worker = [&]() {
+            for (uint32_t k = next++; k < C; k = next++) {
+                ClothHost& c = ctx->cloths[k];
+                if (c.order == XPBD_ORDER_PRESORTED) {
+                    c.perm.resize(c.e);
+                    for (uint32_t q = 0; q < c.e; ++q) c.perm[q] = q;
+                    c.batch_off = c.given_offsets;
+                    c.colors.assign(c.e, 0);
+                    for (size_t b = 0; b + 1 < c.batch_off.size(); ++b)
+                        for (uint32_t q = c.batch_off[b]; q < c.batch_off[b + 1]; ++q) c.colors[q] = (uint32_t)b;
+                } else {
+                    color_constraints(c.n, c.e, c.ci.data(), c.cj.data(), c.order == XPBD_ORDER_COLOR_INDEX, c.perm,
+                                      c.colors, c.batch_off);
+                }
+            }
+        };
+        const uint32_t nthreads = std::max(1u, std::min<uint32_t>(C, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (uint32_t t = 1; t < nthreads; ++t) pool.emplace_back(worker);
+        worker();
+        for (auto& th : pool) th.join();
+    }
     for (auto& c : ctx->cloths) {
         c.vtx_off = N;
         c.con_off = E;
         N += c.n;
         E += c.e;
-        if (c.order == XPBD_ORDER_PRESORTED) {
-            c.perm.resize(c.e);
-            for (uint32_t k = 0; k < c.e; ++k) c.perm[k] = k;
-            c.batch_off = c.given_offsets;
-            c.colors.assign(c.e, 0);
-            for (size_t b = 0; b + 1 < c.batch_off.size(); ++b)
-                for (uint32_t k = c.batch_off[b]; k < c.batch_off[b + 1]; ++k) c.colors[k] = (uint32_t)b;
-        } else {
-            color_constraints(c.n, c.e, c.ci.data(), c.cj.data(), c.order == XPBD_ORDER_COLOR_INDEX, c.perm,
-                              c.colors, c.batch_off);
-        }
         max_colors = std::max<uint32_t>(max_colors, (uint32_t)c.batch_off.size() - 1);
     }
     // ---- host tables
@@ -499,6 +514,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     ALLOC(cloth_iters_d, unsigned, C);
     ALLOC(cstats_d, XpbdConvergeStats, 1);
     ALLOC(ctx->d_resid, unsigned, 4);
+    unsigned* div_exact_d;
+    ALLOC(div_exact_d, unsigned, 4);
     // render triangles: packed global vertex indices and the vertex → triangle table for the vertex normals
     std::vector<uint4> tri_all;
     for (auto& c : ctx->cloths)
@@ -663,6 +680,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     W.iter_res = iter_res_d;
     W.cloth_ires = cloth_ires_d;
     W.cloth_iters = cloth_iters_d;
+    W.div_exact = div_exact_d;
+    CK(cudaMemsetAsync(div_exact_d, 0xFF, 4 * sizeof(unsigned), st), "memset");  // exact until the first check
     W.n_tris = T;
     W.tris = tris_d;
     W.vt_off = vt_off_d;

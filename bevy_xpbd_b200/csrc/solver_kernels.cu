@@ -20,6 +20,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "xpbd_fpdiv.h"
 #include "xpbd_internal.h"
 #include "xpbd_kernels.h"
@@ -152,8 +154,10 @@ __device__ __forceinline__ bool status_clear(const XpbdWorld& W) { return *(vola
 // ---------------------------------------------------------------------------------------------- predict phase
 // Grid-stride over particles. Optionally finalizes a pending substep (positions in jac[pend]) first, then predicts
 // into jac[start]. Pinned particles are written to both ping-pong buffers (they never move).
+// `range_flag` (optional): set to 1 when a predicted or pinned position has a coordinate outside the range of the
+// unchecked shared-reciprocal division (coord_outside_fast_range).
 __device__ void predict_phase(const XpbdWorld& W, const XpbdDevParams& P, bool finalize_pending, uint32_t pend,
-                              uint32_t start, bool predict) {
+                              uint32_t start, bool predict, unsigned* range_flag = nullptr) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n; i += stride) {
         float4 xo4 = W.x[i];
@@ -163,6 +167,9 @@ __device__ void predict_phase(const XpbdWorld& W, const XpbdDevParams& P, bool f
             if (predict) {
                 W.jac[0][i] = xo4;
                 W.jac[1][i] = xo4;
+                if (range_flag && (coord_outside_fast_range(xo4.x) | coord_outside_fast_range(xo4.y) |
+                                   coord_outside_fast_range(xo4.z)))
+                    *range_flag = 1u;
             }
             continue;
         }
@@ -177,6 +184,9 @@ __device__ void predict_phase(const XpbdWorld& W, const XpbdDevParams& P, bool f
         if (predict) {
             F3 pos = predict_particle(i, xo, vel, P);
             W.jac[start][i] = make_float4(pos.x, pos.y, pos.z, w);
+            if (range_flag && (coord_outside_fast_range(pos.x) | coord_outside_fast_range(pos.y) |
+                               coord_outside_fast_range(pos.z)))
+                *range_flag = 1u;
         }
     }
 }
@@ -373,15 +383,16 @@ __global__ void __launch_bounds__(BLOCK) jacobi_persistent_kernel(XpbdWorld W, u
 // correction (n̂·w_i)·Δλ, or zero where the reference skips the constraint (|d| < 1e-8) or has Δλ = 0 (w sum < 1e-8).
 // Branch-free: a skipped term is selected as +0, which leaves the running sum unchanged (the sum starts at +0 and
 // adding terms never yields -0).
-template <bool EXACT_FALLBACK>
-__device__ __forceinline__ F3 row_term(const F3 self, float wi, const float4 po, float rest, float alpha_t, bool& ok) {
+// UNCHECKED: n̂ by fpdiv3_unchecked — only when the pass's coordinate check found every position in range.
+template <bool UNCHECKED>
+__device__ __forceinline__ F3 row_term(const F3 self, float wi, const float4 po, float rest, float alpha_t) {
     const F3 gv = sub3(self, f3(po));
     const float len = len3(gv);
     F3 nrm;
-    if (EXACT_FALLBACK) {
-        nrm = div3(gv, len);
+    if (UNCHECKED) {
+        fpdiv3_unchecked(gv.x, gv.y, gv.z, len, nrm.x, nrm.y, nrm.z);  // a skipped term (len < 1e-8) is discarded
     } else {
-        ok = fpdiv3_by_length_fast(gv.x, gv.y, gv.z, len, nrm.x, nrm.y, nrm.z) | (len < 1e-8f);  // skipped: fine
+        nrm = div3(gv, len);
     }
     const float C = __fsub_rn(len, rest);
     const float wsum = __fadd_rn(__fadd_rn(wi, po.w), alpha_t);
@@ -391,11 +402,17 @@ __device__ __forceinline__ F3 row_term(const F3 self, float wi, const float4 po,
             use ? __fmul_rn(__fmul_rn(nrm.z, wi), dlam) : 0.0f};
 }
 
+// unchecked: every position of this pass's input is in the fast-division range; range_next: the flag of the next
+// pass, set when a position this call writes is not.
 __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevParams& P, uint32_t i,
                                            const float4* __restrict__ jin, float4* __restrict__ jout,
-                                           TailMode tail) {
+                                           TailMode tail, bool unchecked, unsigned* range_next) {
     const float4 ps = jin[i];
-    if (ps.w <= 0.0f) return;
+    if (ps.w <= 0.0f) {  // pinned: not moved, but its position is read by its neighbours in the next pass too
+        if (coord_outside_fast_range(ps.x) | coord_outside_fast_range(ps.y) | coord_outside_fast_range(ps.z))
+            *range_next = 1u;
+        return;
+    }
     const uint32_t rs = W.row_off[i], re = W.row_off[i + 1];
     const bool persist = P.lambda_mode != 0u;
     const float* __restrict__ pal = W.palette_comp + (uint32_t)W.row_cloth[i] * XPBD_PALETTE;
@@ -405,43 +422,37 @@ __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevPara
     if (!persist) {
         // λ = 0 at every pass (reference mode): groups of four independent terms, then the remainder, summed in
         // incidence order
-        uint32_t k = rs;
-        for (; k + 4 <= re; k += 4) {
-            F3 c[4];
-            bool ok = true;
+        auto sum_terms = [&](auto unchecked_tag) {
+            constexpr bool U = decltype(unchecked_tag)::value;
+            uint32_t k = rs;
+            for (; k + 4 <= re; k += 4) {
+                F3 c[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const uint2 rec = recs[k + u];
-                bool oku = true;
-                c[u] = row_term<false>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
-                                       __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq), oku);
-                ok &= oku;
-            }
-            if (!ok) {  // an operand outside the shared-reciprocal range (tiny nonzero component): exact division
-#pragma unroll 1
                 for (int u = 0; u < 4; ++u) {
                     const uint2 rec = recs[k + u];
-                    bool unused = true;
-                    c[u] = row_term<true>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
-                                          __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq), unused);
+                    c[u] = row_term<U>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
+                                       __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq));
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    ax = __fadd_rn(ax, c[u].x);
+                    ay = __fadd_rn(ay, c[u].y);
+                    az = __fadd_rn(az, c[u].z);
                 }
             }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                ax = __fadd_rn(ax, c[u].x);
-                ay = __fadd_rn(ay, c[u].y);
-                az = __fadd_rn(az, c[u].z);
+            for (; k < re; ++k) {
+                const uint2 rec = recs[k];
+                const F3 c = row_term<U>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
+                                         __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq));
+                ax = __fadd_rn(ax, c.x);
+                ay = __fadd_rn(ay, c.y);
+                az = __fadd_rn(az, c.z);
             }
-        }
-        for (; k < re; ++k) {
-            const uint2 rec = recs[k];
-            bool unused = true;
-            const F3 c = row_term<true>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
-                                        __fmul_rn(pal[rec.x >> 28], P.inv_dt_sq), unused);
-            ax = __fadd_rn(ax, c.x);
-            ay = __fadd_rn(ay, c.y);
-            az = __fadd_rn(az, c.z);
-        }
+        };
+        if (unchecked)
+            sum_terms(std::true_type{});
+        else
+            sum_terms(std::false_type{});
     } else {
         for (uint32_t k = rs; k < re; k += 4) {
             float cx[4], cy[4], cz[4];
@@ -487,8 +498,13 @@ __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevPara
     if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
     delta = clamp_correction(delta);
     F3 xn = add3(self, delta);
+    auto note_range = [&](const F3& q) {
+        if (coord_outside_fast_range(q.x) | coord_outside_fast_range(q.y) | coord_outside_fast_range(q.z))
+            *range_next = 1u;
+    };
     if (tail == kTailNone) {
         jout[i] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        note_range(xn);
         return;
     }
     const F3 xo = f3(W.x[i]);
@@ -499,8 +515,10 @@ __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevPara
     if (tail == kTailFinalizePredict) {
         const F3 pos = predict_particle(i, xn, vel, P);
         jout[i] = make_float4(pos.x, pos.y, pos.z, ps.w);
+        note_range(pos);
     } else {
         jout[i] = make_float4(xn.x, xn.y, xn.z, ps.w);
+        note_range(xn);
     }
 }
 
@@ -511,11 +529,14 @@ __device__ __forceinline__ void jacobi_rows_body(const XpbdWorld& W, uint32_t fl
     const XpbdDevParams P = *W.params;
     const bool persist = P.lambda_mode != 0u;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
-    predict_phase(W, P, (flags & kBeginFinalize) != 0u, pend, start, true);
+    // Pass p of this launch reads range slot p % 3 (written while its input positions were written: by the predict
+    // phase for p = 0, by pass p - 1 otherwise) and clears slot (p + 2) % 3, last read by pass p - 1. Slots only ever
+    // get set between clears, so a stale value can only force the exact division, never skip it.
+    predict_phase(W, P, (flags & kBeginFinalize) != 0u, pend, start, true, W.div_exact);
     if (persist)
         for (uint32_t k = gtid; k < W.n_inc; k += gstride) W.inc_lambda[k] = 0.0f;
     if (!grid_barrier(W, P)) return;
-    uint32_t b = start;
+    uint32_t b = start, pass = 0;
     const uint32_t I = P.iterations;
     for (uint32_t s = 0; s < substeps; ++s) {
         const bool last_sub = (s + 1 == substeps);
@@ -545,7 +566,12 @@ __device__ __forceinline__ void jacobi_rows_body(const XpbdWorld& W, uint32_t fl
                 if (!last_sub) tail = kTailFinalizePredict;
                 else if (flags & kEndFinalize) tail = kTailFinalize;
             }
-            for (uint32_t i = gtid; i < W.n; i += gstride) jacobi_row(W, P, i, jin, jout, tail);
+            const bool unchecked = *(volatile unsigned*)&W.div_exact[pass % 3u] == 0u;
+            if (gtid == 0) W.div_exact[(pass + 2u) % 3u] = 0u;
+            unsigned* range_next = W.div_exact + (pass + 1u) % 3u;
+            for (uint32_t i = gtid; i < W.n; i += gstride)
+                jacobi_row(W, P, i, jin, jout, tail, unchecked, range_next);
+            ++pass;
             const bool very_last = last_sub && (k + 1 == I);
             if (!very_last && !grid_barrier(W, P)) return;
         }

@@ -55,6 +55,26 @@ __device__ __forceinline__ bool fpdiv3_by_length_fast(float ax, float ay, float 
     return b_ok & (mn >= (67u << 24) - 1u);
 }
 
+// The bare shared-reciprocal quotients, for callers that have established the theorem's conditions beforehand. The
+// Jacobi row kernel does so once per pass for the whole grid: when every coordinate of every particle is 0 or has a
+// magnitude in [2^-37, 2^58] (see coord_outside_fast_range), every nonzero difference of two coordinates is a
+// multiple of 2^-60 (so |a_k| >= 2^-60), every length of a used term is in [1e-8, 2^60), and the quotients are in
+// [2^-120, 1 + 2^-23] — all normal, so the result is RN(a_k / b).
+__device__ __forceinline__ void fpdiv3_unchecked(float ax, float ay, float az, float b, float& qx, float& qy,
+                                                 float& qz) {
+    const float y = __frcp_rn(b);
+    qx = fpdiv_step(ax, b, y);
+    qy = fpdiv_step(ay, b, y);
+    qz = fpdiv_step(az, b, y);
+}
+
+// True when a coordinate breaks the fpdiv3_unchecked invariant: nonzero and below 2^-37 in magnitude, above 2^58,
+// or not a number.
+__device__ __forceinline__ bool coord_outside_fast_range(float c) {
+    const float m = fabsf(c);
+    return ((m < 0x1p-37f) & (m != 0.0f)) | !(m <= 0x1p58f);
+}
+
 // {ax, ay, az} / b, each correctly rounded.
 __device__ __forceinline__ void fpdiv3(float ax, float ay, float az, float b, float& qx, float& qy, float& qz) {
     const float mb = fabsf(b);

@@ -130,6 +130,7 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     unsigned* iter_res;             // per iteration of a substep: residual of the still-active cloths (float bits)
     unsigned* cloth_ires;           // 3 x n_cloths: per-cloth residual of iterations it % 3 (float bits)
     unsigned* cloth_iters;          // per cloth: update passes of the current substep
+    unsigned* div_exact;            // 3 slots: pass p of the row kernel takes the exact division when slot p % 3 != 0
     // render triangles (vertex normals)
     uint32_t n_tris;
     const uint4* tris;              // global vertex indices {a, b, c, 0}

@@ -353,3 +353,24 @@ def test_jacobi_execution_paths_bit_exact(kernel, lam):
             lam_o[perm] = o.lambdas()
             both = (sp.inv_mass[sp.constraint_i] == 0) & (sp.inv_mass[sp.constraint_j] == 0)
             assert np.array_equal(plug.lambdas(k)[~both].astype(np.float64), lam_o[~both]), k
+
+
+@pytest.mark.parametrize("where", ["pinned", "free"])
+def test_row_kernel_coordinates_outside_fast_division_range_bit_exact(where):
+    """The row kernel divides by a constraint's length through one shared reciprocal when every position of a pass has
+    all coordinates 0 or in [2^-37, 2^58], and by the ordinary division otherwise (decided per pass on the GPU).
+    Coordinates of 1e-13 on a pinned particle (every pass takes the exact path) or on free particles (the first
+    passes do) give the reference result as well."""
+    sp = wl.make_sheet(24, 1.0, 1.0, "corners", seed=21)
+    x = sp.positions.copy()
+    idx = np.flatnonzero(sp.inv_mass == 0)[:1] if where == "pinned" else np.array([30, 31, 57, 300])
+    x[idx, 0] = np.float32(1e-13)
+    x[idx[-1], 2] = np.float32(-3e-20)
+    sp.positions = x
+    prm = params_for(10, 10, 1.0)
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10, jacobi_kernel=3)
+    plug = gpu_sim(sp, prm, cfg)
+    plug.step(frames=3)
+    o = oracle_sim(sp, prm, cfg)
+    o.substeps(30)
+    assert max_abs(plug.positions(), o.state()[0]) == 0.0
