@@ -374,3 +374,23 @@ def test_row_kernel_coordinates_outside_fast_division_range_bit_exact(where):
     o = oracle_sim(sp, prm, cfg)
     o.substeps(30)
     assert max_abs(plug.positions(), o.state()[0]) == 0.0
+
+
+@pytest.mark.parametrize("where", ["pinned", "free"])
+def test_cluster_gs_coordinates_outside_fast_division_range_bit_exact(where):
+    """The cluster Gauss–Seidel kernel takes the shared-reciprocal division per constraint when its operands pass
+    the range test and the ordinary division otherwise: coordinates of 1e-13 and -3e-20 give the reference result."""
+    sp = wl.make_sheet(64, 2.0, 1.0, "top_edge", seed=22)
+    x = sp.positions.copy()
+    idx = np.flatnonzero(sp.inv_mass == 0)[:1] if where == "pinned" else np.array([700, 701, 1500, 3000])
+    x[idx, 0] = np.float32(1e-13)
+    x[idx[-1], 2] = np.float32(-3e-20)
+    sp.positions = x
+    prm = params_for(10, 10, 1.0, drag=0.01)
+    cfg = _cfg(solver=P.SOLVER_GAUSS_SEIDEL, solve_substeps=10, cluster_ctas=16)
+    plug = gpu_sim(sp, prm, cfg)
+    assert plug.stats()["cluster_ctas"] == 16
+    plug.step(frames=2)
+    o = oracle_sim(sp, prm, cfg)
+    o.substeps(20)
+    assert max_abs(plug.positions(), o.state()[0]) == 0.0
