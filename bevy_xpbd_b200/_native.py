@@ -36,6 +36,8 @@ EXPORTED = [
     "xpbd_mlp_fit_normalization", "xpbd_mlp_train", "xpbd_mlp_eval", "xpbd_mlp_gradients", "xpbd_mlp_predict_lambda",
     "xpbd_converge_history", "xpbd_converge_cloth_iterations", "xpbd_selftest_division",
     "xpbd_mlp_minibatch_gradients", "xpbd_mlp_apply_gradients", "xpbd_set_triangles", "xpbd_read_normals",
+    "xpbd_mesh_grid_hanging", "xpbd_mesh_from_obj", "xpbd_mesh_from_triangles", "xpbd_mesh_sizes", "xpbd_mesh_get",
+    "xpbd_mesh_free",
 ]
 MLP_PARAMS = 4865
 MLP_NORM = 20
@@ -148,6 +150,12 @@ def load():
         "xpbd_mlp_apply_gradients": (I, [P, P, C.c_float, C.c_float]),
         "xpbd_set_triangles": (I, [P, U, U, P]),
         "xpbd_read_normals": (I, [P, U, P]),
+        "xpbd_mesh_grid_hanging": (I, [U, U, C.c_float, C.POINTER(C.c_void_p)]),
+        "xpbd_mesh_from_obj": (I, [C.c_char_p, C.POINTER(C.c_void_p)]),
+        "xpbd_mesh_from_triangles": (I, [U, P, U, P, U, P, P, P, P, C.POINTER(C.c_void_p)]),
+        "xpbd_mesh_sizes": (I, [P, C.POINTER(U), C.POINTER(U), C.POINTER(U), C.POINTER(U)]),
+        "xpbd_mesh_get": (I, [P, P, P, P, P, P, P, P, P]),
+        "xpbd_mesh_free": (None, [P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

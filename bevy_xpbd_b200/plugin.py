@@ -216,6 +216,13 @@ class ClothComputePlugin:
         return self.add_cloth(spec.positions, spec.inv_mass, spec.constraint_i, spec.constraint_j, spec.rest_len,
                               spec.compliance, spec.velocities, spec.rest_positions, spec.constraint_type, order)
 
+    def add_mesh(self, mesh) -> int:
+        """A ClothMeshData (bevy_xpbd_b200.mesh) with its batch order and render triangles."""
+        cid = self.add_cloth(**mesh.to_spec_arrays())
+        if len(mesh.indices):
+            self.set_triangles(cid, mesh.indices)
+        return cid
+
     def set_triangles(self, cloth: int, tri_indices):
         """Render triangles (local vertex indices, 3 per triangle) of a cloth, for `normals`."""
         t = _u32(tri_indices).reshape(-1)

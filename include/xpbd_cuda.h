@@ -291,6 +291,30 @@ int xpbd_mlp_eval(xpbd_ctx* ctx, const float* features, uint32_t n, float* out);
 int xpbd_mlp_gradients(xpbd_ctx* ctx, const float* features, const float* targets, uint32_t n, float* grads,
                        float* loss);
 
+/* ---- cloth meshes: the crate's host-side mesh preparation (src/mesh_prep.rs) -------------------------------------
+ * A built mesh holds positions, inverse masses (a third of 1/area of each incident triangle; top row pinned), render
+ * triangles and its constraints — structural edges (α 2e-8), hinge bends (α 3.8), then the extras — already in the
+ * greedy-colored batch order with batch offsets: pass them to xpbd_add_cloth with XPBD_ORDER_PRESORTED. */
+typedef struct xpbd_mesh xpbd_mesh;
+/* grid_cloth_hanging (mesh_prep.rs:363-406): quad grid in the XY plane, skip-2 braces and cross diagonals. */
+int xpbd_mesh_grid_hanging(uint32_t quad_cols, uint32_t quad_rows, float cell_size, xpbd_mesh** out);
+/* parse_welded_obj (mesh_prep.rs:223-357): vertices welded by corner string, quads split v0-v2 with a v1-v3 brace,
+ * n-gons fanned, skip-2 braces when the vertices form an axis-aligned grid. */
+int xpbd_mesh_from_obj(const char* obj_text, xpbd_mesh** out);
+/* finalize_cloth_mesh (mesh_prep.rs:532-659) of a triangle mesh with extra constraints (i, j, rest, compliance). */
+int xpbd_mesh_from_triangles(uint32_t num_vertices, const float* positions_xyz, uint32_t num_tris,
+                             const uint32_t* tri_indices, uint32_t num_extra, const uint32_t* extra_i,
+                             const uint32_t* extra_j, const float* extra_rest, const float* extra_comp,
+                             xpbd_mesh** out);
+int xpbd_mesh_sizes(const xpbd_mesh* mesh, uint32_t* num_vertices, uint32_t* num_tris, uint32_t* num_constraints,
+                    uint32_t* num_batches);
+/* Copies out any of: positions (xyz), inverse masses, triangles (3 per), constraint i/j/rest/compliance (batch
+ * order), batch offsets (num_batches + 1). NULL skips an array. */
+int xpbd_mesh_get(const xpbd_mesh* mesh, float* positions_xyz, float* inv_mass, uint32_t* tri_indices,
+                  uint32_t* constraint_i, uint32_t* constraint_j, float* rest_len, float* compliance,
+                  uint32_t* batch_offsets);
+void xpbd_mesh_free(xpbd_mesh* mesh);
+
 /* ---- diagnostics ------------------------------------------------------------------------------------------- */
 const char* xpbd_last_error(xpbd_ctx* ctx);
 const char* xpbd_status_string(int status);

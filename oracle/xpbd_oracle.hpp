@@ -393,12 +393,17 @@ inline bool axis_aligned_grid_skip_two(const std::vector<V3f>& pos, std::vector<
 }
 
 // parse_welded_obj, mesh_prep.rs:223-357 (normals/uvs are render-only and not kept).
+// Rust's str::parse::<usize>: an optional '+', then at least one decimal digit; overflow is an error.
 inline bool parse_usize(const std::string& s, size_t& out) {
-    if (s.empty()) return false;
+    size_t k = (!s.empty() && s[0] == '+') ? 1 : 0;
+    if (k == s.size()) return false;
     size_t v = 0;
-    for (char ch : s) {
+    for (; k < s.size(); ++k) {
+        const char ch = s[k];
         if (ch < '0' || ch > '9') return false;
-        v = v * 10 + (size_t)(ch - '0');
+        const size_t d = (size_t)(ch - '0');
+        if (v > (SIZE_MAX - d) / 10) return false;
+        v = v * 10 + d;
     }
     out = v;
     return true;

@@ -48,3 +48,28 @@ def test_normals_need_triangles():
     plug.commit()
     with pytest.raises(P.XpbdError):
         plug.normals(0)
+
+
+def test_mesh_builder_to_solver_and_normals():
+    """A mesh from the product's builder (grid_cloth_hanging) through add_mesh — batch order and triangles included —
+    steps exactly like the oracle fed the oracle's own mesh, and its normals match the oracle's."""
+    from bevy_xpbd_b200 import mesh as M
+    m = M.grid_cloth_hanging(16, 16, 0.045)
+    ref = orc.grid_cloth_hanging(16, 16, 0.045)
+    plug = P.ClothComputePlugin(0)
+    plug.add_mesh(m)
+    plug.commit()
+    u = P.ClothSimUniforms(solver=P.SOLVER_JACOBI)
+    prm = u.substep_params()
+    prm.grab_active = False
+    plug.set_params(prm, P.ClothSimConfig(solver=P.SOLVER_JACOBI, solve_substeps=P.SUBSTEPS))
+    plug.step(frames=2)
+    s = orc.OracleSim(ref.positions, ref.inv_mass, ref.constraint_i, ref.constraint_j, ref.constraint_rest_len,
+                      ref.constraint_compliance, rest_pos=ref.rest_positions)
+    d = prm.as_dict()
+    d.update(grab_active=0, solver=P.SOLVER_JACOBI)
+    s.set_params(d)
+    s.substeps(2 * P.SUBSTEPS)
+    x = plug.positions(0)
+    assert np.array_equal(x.astype(np.float64), s.state()[0])
+    assert np.array_equal(plug.normals(0).view(np.uint32), NO.vertex_normals(x, ref.indices).view(np.uint32))
