@@ -129,6 +129,16 @@ static T* dev_alloc(xpbd_ctx* ctx, size_t count, cudaError_t* err) {
     return (T*)p;
 }
 
+// Frees one buffer obtained from dev_alloc (growing scratch buffers replace theirs).
+static void dev_release(xpbd_ctx* ctx, void* p) {
+    if (!p) return;
+    auto it = std::find(ctx->allocs.begin(), ctx->allocs.end(), p);
+    if (it != ctx->allocs.end()) {
+        ctx->allocs.erase(it);
+        cudaFree(p);
+    }
+}
+
 static void free_device(xpbd_ctx* ctx) {
     if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
     ctx->exec = nullptr;
@@ -1488,6 +1498,12 @@ extern "C" int xpbd_mlp_init(xpbd_ctx* ctx, uint64_t seed, uint32_t capacity) {
         if (err != cudaSuccess) return cuda_fail(ctx, err, "mlp buffers");
     }
     if (capacity > ctx->ds_cap) {
+        CK(cudaStreamSynchronize(ctx->stream), "sync");  // no launch may still use the old buffers
+        dev_release(ctx, ctx->d_feat);
+        dev_release(ctx, ctx->d_scale);
+        dev_release(ctx, ctx->d_target);
+        ctx->d_feat = ctx->d_scale = ctx->d_target = nullptr;
+        ctx->ds_cap = 0;
         ctx->d_feat = dev_alloc<float>(ctx, (size_t)capacity * 9, &err);
         if (err == cudaSuccess) ctx->d_scale = dev_alloc<float>(ctx, capacity, &err);
         if (err == cudaSuccess) ctx->d_target = dev_alloc<float>(ctx, capacity, &err);
@@ -1691,6 +1707,10 @@ extern "C" int xpbd_mlp_train(xpbd_ctx* ctx, uint32_t steps, uint32_t batch, flo
     const size_t need = (size_t)steps * batch;
     if (need > ctx->idx_cap) {
         cudaError_t err = cudaSuccess;
+        CK(cudaStreamSynchronize(ctx->stream), "sync");
+        dev_release(ctx, ctx->d_idx);
+        ctx->d_idx = nullptr;
+        ctx->idx_cap = 0;
         ctx->d_idx = dev_alloc<uint32_t>(ctx, need, &err);
         if (err != cudaSuccess) return cuda_fail(ctx, err, "batch indices");
         ctx->idx_cap = (uint32_t)need;
@@ -1726,6 +1746,10 @@ extern "C" int xpbd_mlp_minibatch_gradients(xpbd_ctx* ctx, uint32_t batch, uint6
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     if (batch > ctx->idx_cap) {
         cudaError_t err = cudaSuccess;
+        CK(cudaStreamSynchronize(ctx->stream), "sync");
+        dev_release(ctx, ctx->d_idx);
+        ctx->d_idx = nullptr;
+        ctx->idx_cap = 0;
         ctx->d_idx = dev_alloc<uint32_t>(ctx, batch, &err);
         if (err != cudaSuccess) return cuda_fail(ctx, err, "batch indices");
         ctx->idx_cap = batch;
