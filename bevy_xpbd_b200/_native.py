@@ -37,7 +37,7 @@ EXPORTED = [
     "xpbd_converge_history", "xpbd_converge_cloth_iterations", "xpbd_selftest_division",
     "xpbd_mlp_minibatch_gradients", "xpbd_mlp_apply_gradients", "xpbd_set_triangles", "xpbd_read_normals",
     "xpbd_mesh_grid_hanging", "xpbd_mesh_from_obj", "xpbd_mesh_from_triangles", "xpbd_mesh_sizes", "xpbd_mesh_get",
-    "xpbd_mesh_free",
+    "xpbd_mesh_free", "xpbd_set_cloth_grab",
 ]
 MLP_PARAMS = 4865
 MLP_NORM = 20
@@ -156,6 +156,7 @@ def load():
         "xpbd_mesh_sizes": (I, [P, C.POINTER(U), C.POINTER(U), C.POINTER(U), C.POINTER(U)]),
         "xpbd_mesh_get": (I, [P, P, P, P, P, P, P, P, P]),
         "xpbd_mesh_free": (None, [P]),
+        "xpbd_set_cloth_grab": (I, [P, U, C.c_int32, P, C.c_float]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -102,6 +102,7 @@ struct xpbd_ctx {
     uint32_t idx_cap = 0, ds_count = 0, ds_cap = 0, collect_offset = 0;
     uint64_t adam_step = 0;
     float norm[XPBD_MLP_NORM] = {0};
+    std::vector<XpbdGrab> grabs;  // per cloth (host copy)
     float forced_timeout_ms = 0.f;
 };
 
@@ -526,6 +527,11 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     ALLOC(ctx->d_resid, unsigned, 4);
     unsigned* div_exact_d;
     ALLOC(div_exact_d, unsigned, 4);
+    XpbdGrab* grabs_d;
+    uint32_t* grab_count_d;
+    ALLOC(grabs_d, XpbdGrab, C);
+    ALLOC(grab_count_d, uint32_t, 1);
+    ctx->grabs.assign(C, XpbdGrab{-1, {0.f, 0.f, 0.f}, 0.f, {0u, 0u, 0u}});
     // render triangles: packed global vertex indices and the vertex → triangle table for the vertex normals
     std::vector<uint4> tri_all;
     for (auto& c : ctx->cloths)
@@ -691,6 +697,10 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     W.cloth_ires = cloth_ires_d;
     W.cloth_iters = cloth_iters_d;
     W.div_exact = div_exact_d;
+    W.grabs = grabs_d;
+    W.grab_count = grab_count_d;
+    H2D(grabs_d, ctx->grabs.data(), C * sizeof(XpbdGrab));
+    CK(cudaMemsetAsync(grab_count_d, 0, sizeof(uint32_t), st), "memset");
     CK(cudaMemsetAsync(div_exact_d, 0xFF, 4 * sizeof(unsigned), st), "memset");  // exact until the first check
     W.n_tris = T;
     W.tris = tris_d;
@@ -1182,6 +1192,34 @@ extern "C" int xpbd_reset(xpbd_ctx* ctx) {
     CK(cudaMemset(ctx->W.con_lambda, 0, std::max<size_t>(ctx->W.e, 1) * 4), "memset");
     if (ctx->W.patch_lambda)
         CK(cudaMemset(ctx->W.patch_lambda, 0, std::max<size_t>(ctx->W.patch_con_total, 1) * 4), "memset");
+    return XPBD_OK;
+}
+
+extern "C" int xpbd_set_cloth_grab(xpbd_ctx* ctx, uint32_t cloth_id, int32_t vertex, const float* target,
+                                   float stiffness) {
+    if (!ctx || (vertex >= 0 && !target)) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+    const ClothHost& c = ctx->cloths[cloth_id];
+    if (vertex >= (int32_t)c.n) return fail(ctx, XPBD_ERR_INDEX_RANGE, "grab vertex out of range");
+    XpbdGrab g{-1, {0.f, 0.f, 0.f}, 0.f, {0u, 0u, 0u}};
+    if (vertex >= 0) {
+        g.idx = (int32_t)(c.vtx_off + (uint32_t)vertex);
+        g.target[0] = target[0];
+        g.target[1] = target[1];
+        g.target[2] = target[2];
+        g.stiffness = stiffness;
+    }
+    ctx->grabs[cloth_id] = g;
+    uint32_t active = 0;
+    for (const XpbdGrab& h : ctx->grabs) active += h.idx >= 0 ? 1u : 0u;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    // ordered with the frames on the context's stream; the host copies are staged before the calls return
+    CK(cudaMemcpyAsync(const_cast<XpbdGrab*>(ctx->W.grabs) + cloth_id, &ctx->grabs[cloth_id], sizeof(XpbdGrab), cudaMemcpyHostToDevice,
+                       ctx->stream), "grab");
+    CK(cudaMemcpyAsync(const_cast<uint32_t*>(ctx->W.grab_count), &active, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                       ctx->stream), "grab");
+    CK(cudaStreamSynchronize(ctx->stream), "grab");
     return XPBD_OK;
 }
 

@@ -193,7 +193,16 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
                 W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
                 xo = xn;
             }
-            const V3 p = predict(i, xo, vel, P);
+            V3 p = predict(i, xo, vel, P);
+            if (*W.grab_count != 0u) {  // per-cloth grab (extension), the reference's pull on the grabbed vertex
+                const XpbdGrab g = W.grabs[W.row_cloth[i]];
+                if (g.idx == (int32_t)i) {
+                    V3 pull = vmul(vsub(V3{g.target[0], g.target[1], g.target[2]}, p), g.stiffness);
+                    const float pl = vlen(pull);
+                    if (pl > kGrab && pl > 0.0f) pull = vmul(pull, __fdiv_rn(kGrab, pl));
+                    p = vadd(p, pull);
+                }
+            }
             xs[k] = make_float4(p.x, p.y, p.z, x4.w);
         }
         pending = true;

@@ -88,6 +88,21 @@ __device__ __forceinline__ F3 predict_particle(uint32_t i, F3 sim, F3& vel, cons
     return pos;
 }
 
+// Per-cloth grab (extension of the reference's single grab, xpbd_cpu.rs:56-63): the same pull, applied after
+// predict_particle to the cloth's grabbed vertex.
+__device__ __forceinline__ F3 apply_cloth_grab(const XpbdWorld& W, uint32_t i, F3 pos) {
+    if (*W.grab_count == 0u) return pos;
+    const XpbdGrab g = W.grabs[W.row_cloth[i]];
+    if (g.idx != (int32_t)i) return pos;
+    F3 pull = mul3(sub3(F3{g.target[0], g.target[1], g.target[2]}, pos), g.stiffness);
+    const float pl = len3(pull);
+    if (pl > kGrabMaxPull && pl > 0.0f) pull = mul3(pull, __fdiv_rn(kGrabMaxPull, pl));
+    return add3(pos, pull);
+}
+__device__ __forceinline__ F3 predict_w(const XpbdWorld& W, uint32_t i, F3 sim, F3& vel, const XpbdDevParams& P) {
+    return apply_cloth_grab(W, i, predict_particle(i, sim, vel, P));
+}
+
 // xpbd_substep_post_velocity, xpbd_cpu.rs:393-409, for an unpinned particle: ground plane (extension), then
 // v = ((x - prev) * inv_dt) * exp(-k dt). Returns the (possibly clamped) new position.
 __device__ __forceinline__ F3 finalize_particle(F3 xn, F3 xo, F3& vel, const XpbdDevParams& P, int* status) {
@@ -182,7 +197,7 @@ __device__ void predict_phase(const XpbdWorld& W, const XpbdDevParams& P, bool f
             xo = xn;
         }
         if (predict) {
-            F3 pos = predict_particle(i, xo, vel, P);
+            F3 pos = predict_w(W, i, xo, vel, P);
             W.jac[start][i] = make_float4(pos.x, pos.y, pos.z, w);
             if (range_flag && (coord_outside_fast_range(pos.x) | coord_outside_fast_range(pos.y) |
                                coord_outside_fast_range(pos.z)))
@@ -304,7 +319,7 @@ __device__ __forceinline__ void jacobi_tile(const XpbdWorld& W, const XpbdDevPar
     W.x[r] = make_float4(xn.x, xn.y, xn.z, ps.w);
     W.v[r] = make_float4(vel.x, vel.y, vel.z, 0.0f);
     if (tail == kTailFinalizePredict) {
-        F3 pos = predict_particle(r, xn, vel, P);
+        F3 pos = predict_w(W, r, xn, vel, P);
         jout[r] = make_float4(pos.x, pos.y, pos.z, ps.w);
     } else {
         jout[r] = make_float4(xn.x, xn.y, xn.z, ps.w);
@@ -351,7 +366,7 @@ __global__ void __launch_bounds__(BLOCK) jacobi_persistent_kernel(XpbdWorld W, u
                 W.x[i] = make_float4(xn.x, xn.y, xn.z, p4.w);
                 W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
                 if (!last_sub) {
-                    F3 pos = predict_particle(i, xn, vel, P);
+                    F3 pos = predict_w(W, i, xn, vel, P);
                     W.jac[b][i] = make_float4(pos.x, pos.y, pos.z, p4.w);
                 }
             }
@@ -513,7 +528,7 @@ __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevPara
     W.x[i] = make_float4(xn.x, xn.y, xn.z, ps.w);
     W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
     if (tail == kTailFinalizePredict) {
-        const F3 pos = predict_particle(i, xn, vel, P);
+        const F3 pos = predict_w(W, i, xn, vel, P);
         jout[i] = make_float4(pos.x, pos.y, pos.z, ps.w);
         note_range(pos);
     } else {
@@ -551,7 +566,7 @@ __device__ __forceinline__ void jacobi_rows_body(const XpbdWorld& W, uint32_t fl
                 W.x[i] = make_float4(xn.x, xn.y, xn.z, p4.w);
                 W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
                 if (!last_sub) {
-                    F3 pos = predict_particle(i, xn, vel, P);
+                    F3 pos = predict_w(W, i, xn, vel, P);
                     W.jac[b][i] = make_float4(pos.x, pos.y, pos.z, p4.w);
                 }
             }
@@ -626,7 +641,7 @@ __global__ void converge_predict_kernel(XpbdWorld W) {
             continue;
         }
         F3 vel = f3(W.v[i]);
-        const F3 pos = predict_particle(i, f3(x4), vel, P);
+        const F3 pos = predict_w(W, i, f3(x4), vel, P);
         W.jac[0][i] = make_float4(pos.x, pos.y, pos.z, x4.w);
     }
 }
@@ -920,7 +935,7 @@ __device__ __forceinline__ void patch_gather(const XpbdWorld& W, const XpbdDevPa
         W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
         W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
         if (tail == kTailFinalizePredict) {
-            const F3 pos = predict_particle(g, xn, vel, P);
+            const F3 pos = predict_w(W, g, xn, vel, P);
             jout[g] = make_float4(pos.x, pos.y, pos.z, ps.w);
         } else {
             jout[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
@@ -991,7 +1006,7 @@ __global__ void __launch_bounds__(BLOCK) jacobi_patch_kernel(XpbdWorld W, uint32
                 W.x[i] = make_float4(xn.x, xn.y, xn.z, p4.w);
                 W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
                 if (!last_sub) {
-                    F3 pos = predict_particle(i, xn, vel, P);
+                    F3 pos = predict_w(W, i, xn, vel, P);
                     W.jac[b][i] = make_float4(pos.x, pos.y, pos.z, p4.w);
                 }
             }

@@ -65,6 +65,15 @@ struct XpbdConvergeStats {  // device counters of the convergence solve
     unsigned int last_iterations;   // passes of the most recent substep, slowest cloth (its residuals stay in iter_res)
 };
 
+// Kinematic grab of one vertex of a cloth (the reference's mouse grab, one per cloth): after the prediction, the
+// vertex is pulled toward the target by stiffness·(target − x), at most 0.065 per substep.
+struct XpbdGrab {
+    int32_t idx;  // global particle index, -1 = none
+    float target[3];
+    float stiffness;
+    uint32_t pad[3];
+};
+
 struct XpbdGridSync {
     unsigned int count;
     unsigned int gen;
@@ -130,6 +139,8 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     unsigned* iter_res;             // per iteration of a substep: residual of the still-active cloths (float bits)
     unsigned* cloth_ires;           // 3 x n_cloths: per-cloth residual of iterations it % 3 (float bits)
     unsigned* cloth_iters;          // per cloth: update passes of the current substep
+    const XpbdGrab* grabs;          // per cloth
+    const uint32_t* grab_count;     // number of cloths with an active grab (device word)
     unsigned* div_exact;            // 3 slots: pass p of the row kernel takes the exact division when slot p % 3 != 0
     // render triangles (vertex normals)
     uint32_t n_tris;

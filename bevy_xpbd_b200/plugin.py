@@ -223,6 +223,12 @@ class ClothComputePlugin:
             self.set_triangles(cid, mesh.indices)
         return cid
 
+    def set_cloth_grab(self, cloth: int, vertex: int | None, target=(0.0, 0.0, 0.0), stiffness: float = 0.0):
+        """Grab one vertex of a cloth (None releases it): pulled toward `target` after each prediction."""
+        t = np.ascontiguousarray(target, np.float32)
+        self._check(self._L.xpbd_set_cloth_grab(self._h, cloth, -1 if vertex is None else int(vertex), _ptr(t),
+                                                C.c_float(stiffness)))
+
     def set_triangles(self, cloth: int, tri_indices):
         """Render triangles (local vertex indices, 3 per triangle) of a cloth, for `normals`."""
         t = _u32(tri_indices).reshape(-1)

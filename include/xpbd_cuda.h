@@ -167,6 +167,10 @@ int xpbd_set_stream(xpbd_ctx* ctx, void* stream);
 int xpbd_add_cloth(xpbd_ctx* ctx, const xpbd_cloth_desc* desc, uint32_t* cloth_id);
 /* Builds coloring, neighbour tables and device buffers for every added cloth. */
 int xpbd_commit(xpbd_ctx* ctx);
+/* Kinematic grab of one vertex per cloth (extension of the single grab of xpbd_time_step_params, which stays): after
+ * each prediction the cloth's local vertex `vertex` moves by stiffness·(target − x), at most 0.065 per substep
+ * (xpbd_cpu.rs:56-63). vertex < 0 releases it. Takes effect from the next frame; no graph recapture. */
+int xpbd_set_cloth_grab(xpbd_ctx* ctx, uint32_t cloth_id, int32_t vertex, const float* target_xyz, float stiffness);
 /* Render triangles of a cloth (3 local vertex indices each; before xpbd_commit), for xpbd_read_normals. */
 int xpbd_set_triangles(xpbd_ctx* ctx, uint32_t cloth_id, uint32_t num_tris, const uint32_t* tri_indices);
 /* Vertex normals of the current positions, accumulate_normals + finalize_normals (cloth_sim_jacobi.wgsl:492-547):
