@@ -15,6 +15,9 @@ the public API with host buffers: per step the parameter block goes host->device
 positions come back device->host, timed on the host clock. Multi-GPU: one process per GPU (torchrun); c1 runs one
 independent replica per rank, c3 shards the cloths across ranks — no collective in the step (weak scaling).
 
+The same line also carries `warm_start`: the convergence solve (Jacobi to a 1e-4 residual, capped) with a plain,
+previous-λ and learned (on-GPU trained MLP) start — passes per cloth-substep and cloth-steps/s for each.
+
 --impl reference times the CPU restatement of the reference solver (src/xpbd_cpu.rs, OpenMP over the independent
 loops) on the same workload and prints the same line with "impl": "reference".
 """
@@ -521,10 +524,10 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    rank, world, local = dist_setup()
-    if args.impl == "reference":
-        run_reference(args, rank, world)
+    if args.impl == "reference":  # CPU only, rank 0 alone: no process group needed
+        run_reference(args, int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")))
         return
+    rank, world, local = dist_setup()
     import torch
     torch.cuda.set_device(local)
     peaks = load_peaks()
