@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <map>
 #include <string>
@@ -319,38 +320,59 @@ extern "C" int xpbd_set_triangles(xpbd_ctx* ctx, uint32_t cloth_id, uint32_t num
     return XPBD_OK;
 }
 
+// Runs fn(k) for k in [0, count) on up to hardware_concurrency host threads (each k exactly once).
+template <typename Fn>
+static void parallel_for(uint32_t count, Fn&& fn) {
+    std::atomic<uint32_t> next{0};
+    auto worker = [&]() {
+        for (uint32_t k = next++; k < count; k = next++) fn(k);
+    };
+    const uint32_t nthreads = std::max(1u, std::min<uint32_t>(count, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < nthreads; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+}
+
+// XPBD_TRACE=1 in the environment: commit prints the host time of its phases to stderr.
+static bool trace_enabled() {
+    static const bool on = [] {
+        const char* v = getenv("XPBD_TRACE");
+        return v && *v && *v != '0';
+    }();
+    return on;
+}
+
 extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     if (!ctx) return XPBD_ERR_INVALID_ARGUMENT;
+    auto t_last = std::chrono::steady_clock::now();
+    auto mark = [&](const char* phase) {
+        if (!trace_enabled()) return;
+        const auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "[xpbd] commit %-28s %9.1f ms\n", phase,
+                std::chrono::duration<double, std::milli>(now - t_last).count());
+        t_last = now;
+    };
     if (ctx->committed) return fail(ctx, XPBD_ERR_STATE, "already committed");
     if (ctx->cloths.empty()) return fail(ctx, XPBD_ERR_STATE, "no cloth added");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const uint32_t C = (uint32_t)ctx->cloths.size();
     uint32_t N = 0, E = 0, max_colors = 0;
     // ---- coloring (cloths are independent: one host thread per cloth at a time) + per-cloth offsets
-    {
-        std::atomic<uint32_t> next{0};
-        auto worker = [&]() {
-            for (uint32_t k = next++; k < C; k = next++) {
-                ClothHost& c = ctx->cloths[k];
-                if (c.order == XPBD_ORDER_PRESORTED) {
-                    c.perm.resize(c.e);
-                    for (uint32_t q = 0; q < c.e; ++q) c.perm[q] = q;
-                    c.batch_off = c.given_offsets;
-                    c.colors.assign(c.e, 0);
-                    for (size_t b = 0; b + 1 < c.batch_off.size(); ++b)
-                        for (uint32_t q = c.batch_off[b]; q < c.batch_off[b + 1]; ++q) c.colors[q] = (uint32_t)b;
-                } else {
-                    color_constraints(c.n, c.e, c.ci.data(), c.cj.data(), c.order == XPBD_ORDER_COLOR_INDEX, c.perm,
-                                      c.colors, c.batch_off);
-                }
-            }
-        };
-        const uint32_t nthreads = std::max(1u, std::min<uint32_t>(C, std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        for (uint32_t t = 1; t < nthreads; ++t) pool.emplace_back(worker);
-        worker();
-        for (auto& th : pool) th.join();
-    }
+    parallel_for(C, [&](uint32_t k) {
+        ClothHost& c = ctx->cloths[k];
+        if (c.order == XPBD_ORDER_PRESORTED) {
+            c.perm.resize(c.e);
+            for (uint32_t q = 0; q < c.e; ++q) c.perm[q] = q;
+            c.batch_off = c.given_offsets;
+            c.colors.assign(c.e, 0);
+            for (size_t b = 0; b + 1 < c.batch_off.size(); ++b)
+                for (uint32_t q = c.batch_off[b]; q < c.batch_off[b + 1]; ++q) c.colors[q] = (uint32_t)b;
+        } else {
+            color_constraints(c.n, c.e, c.ci.data(), c.cj.data(), c.order == XPBD_ORDER_COLOR_INDEX, c.perm, c.colors,
+                              c.batch_off);
+        }
+    });
     for (auto& c : ctx->cloths) {
         c.vtx_off = N;
         c.con_off = E;
@@ -358,18 +380,27 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
         E += c.e;
         max_colors = std::max<uint32_t>(max_colors, (uint32_t)c.batch_off.size() - 1);
     }
-    // ---- host tables
+    mark("coloring");
+    // ---- host tables: per cloth on parallel host threads (each writes only its own slices and its own local
+    // tables), then concatenated in cloth order
     std::vector<float4> hx(N), hv(N), hrest(N);
     std::vector<uint32_t> row_off(N + 1, 0);
     std::vector<uint2> inc;
     std::vector<XpbdTile> tiles;
     std::vector<float> palette((size_t)C * XPBD_PALETTE, 0.f);
     std::vector<uint4> con_in(E);
-    inc.reserve(2 * (size_t)E);
-    PatchArrays patch_arrays;
-    bool patches_ok = true;
-    for (uint32_t ci_ = 0; ci_ < C; ++ci_) {
+    struct ClothTables {
+        std::vector<uint2> inc;         // this cloth's incidences (rows in particle order)
+        std::vector<uint32_t> row_off;  // local row starts (n)
+        PatchArrays patches;
+        std::vector<uint32_t> slot;     // sorted constraint → local patch slot
+        bool patches_ok = false;
+        bool palette_ok = true;
+    };
+    std::vector<ClothTables> ct(C);
+    parallel_for(C, [&](uint32_t ci_) {
         ClothHost& c = ctx->cloths[ci_];
+        ClothTables& t = ct[ci_];
         for (uint32_t i = 0; i < c.n; ++i) {
             hx[c.vtx_off + i] = make_float4(c.pos[3 * i], c.pos[3 * i + 1], c.pos[3 * i + 2], c.w[i]);
             hv[c.vtx_off + i] = make_float4(c.vel[3 * i], c.vel[3 * i + 1], c.vel[3 * i + 2], 0.f);
@@ -389,8 +420,10 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
                 if (pb == bits) break;
             }
             if (k == pal.size()) {
-                if (pal.size() == XPBD_PALETTE)
-                    return fail(ctx, XPBD_ERR_UNSUPPORTED, "more than 16 distinct compliance values in one cloth");
+                if (pal.size() == XPBD_PALETTE) {
+                    t.palette_ok = false;
+                    return;
+                }
                 pal.push_back(c.comp[e]);
             }
             pidx[e] = (uint32_t)k;
@@ -404,42 +437,33 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
         }
         std::vector<uint32_t> roff, other, eid;
         neighbor_csr(c.n, c.e, si.data(), sj.data(), roff, other, eid);
-        if (patches_ok) {  // spatial patches for the shared-memory Jacobi kernel
+        {  // spatial patches for the shared-memory Jacobi kernel
             std::vector<float> srest(c.e);
-            std::vector<uint32_t> spal(c.e), slot;
+            std::vector<uint32_t> spal(c.e);
             for (uint32_t k = 0; k < c.e; ++k) {
                 srest[k] = c.rest[c.perm[k]];
                 spal[k] = pidx[c.perm[k]];
             }
-            patches_ok = build_cloth_patches(c.n, c.rest_pos.data(), c.w.data(), c.e, si.data(), sj.data(),
-                                             srest.data(), spal.data(), roff, other, eid, c.vtx_off, ci_, 256,
-                                             4096, patch_arrays, slot);
-            c.lambda_patch.assign(c.e, 0xFFFFFFFFu);
-            if (patches_ok)
-                for (uint32_t k = 0; k < c.e; ++k) c.lambda_patch[c.perm[k]] = slot[k];
+            t.patches_ok = build_cloth_patches(c.n, c.rest_pos.data(), c.w.data(), c.e, si.data(), sj.data(),
+                                               srest.data(), spal.data(), roff, other, eid, c.vtx_off, ci_, 256,
+                                               4096, t.patches, t.slot);
         }
         c.lambda_inc.assign(c.e, 0xFFFFFFFFu);
         c.inc_i.assign(c.e, 0xFFFFFFFFu);
         c.inc_j.assign(c.e, 0xFFFFFFFFu);
+        t.row_off.resize(c.n);
+        t.inc.reserve(roff[c.n]);
         for (uint32_t i = 0; i < c.n; ++i) {
-            const uint32_t g = c.vtx_off + i;
-            row_off[g] = (uint32_t)inc.size();
+            t.row_off[i] = (uint32_t)t.inc.size();
             if (c.w[i] <= 0.f) continue;  // pinned rows stay empty: jacobi_gather returns jac_in for them
             for (uint32_t k = roff[i]; k < roff[i + 1]; ++k) {
                 const uint32_t e_in = c.perm[eid[k]];
                 uint32_t rb;
                 memcpy(&rb, &c.rest[e_in], 4);
-                if (c.lambda_inc[e_in] == 0xFFFFFFFFu) c.lambda_inc[e_in] = (uint32_t)inc.size();
-                (c.ci[e_in] == i ? c.inc_i : c.inc_j)[e_in] = (uint32_t)inc.size();
-                inc.push_back(make_uint2((other[k] + c.vtx_off) | (pidx[e_in] << 28), rb));
+                if (c.lambda_inc[e_in] == 0xFFFFFFFFu) c.lambda_inc[e_in] = (uint32_t)t.inc.size();
+                (c.ci[e_in] == i ? c.inc_i : c.inc_j)[e_in] = (uint32_t)t.inc.size();
+                t.inc.push_back(make_uint2((other[k] + c.vtx_off) | (pidx[e_in] << 28), rb));
             }
-        }
-        for (uint32_t first = 0; first < c.n; first += 32) {
-            XpbdTile t;
-            t.first = c.vtx_off + first;
-            t.count = (uint16_t)std::min<uint32_t>(32, c.n - first);
-            t.cloth = (uint16_t)ci_;
-            tiles.push_back(t);
         }
         for (uint32_t e = 0; e < c.e; ++e) {
             uint32_t rb, cb;
@@ -447,8 +471,58 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
             memcpy(&cb, &c.comp[e], 4);
             con_in[c.con_off + e] = make_uint4(c.ci[e] + c.vtx_off, c.cj[e] + c.vtx_off, rb, cb);
         }
+    });
+    bool patches_ok = true;
+    for (uint32_t ci_ = 0; ci_ < C; ++ci_) {
+        if (!ct[ci_].palette_ok)
+            return fail(ctx, XPBD_ERR_UNSUPPORTED, "more than 16 distinct compliance values in one cloth");
+        patches_ok = patches_ok && ct[ci_].patches_ok;
+    }
+    inc.reserve(2 * (size_t)E);
+    PatchArrays patch_arrays;
+    for (uint32_t ci_ = 0; ci_ < C; ++ci_) {
+        ClothHost& c = ctx->cloths[ci_];
+        ClothTables& t = ct[ci_];
+        const uint32_t base = (uint32_t)inc.size();
+        for (uint32_t i = 0; i < c.n; ++i) row_off[c.vtx_off + i] = base + t.row_off[i];
+        for (uint32_t e = 0; e < c.e; ++e) {
+            if (c.lambda_inc[e] != 0xFFFFFFFFu) c.lambda_inc[e] += base;
+            if (c.inc_i[e] != 0xFFFFFFFFu) c.inc_i[e] += base;
+            if (c.inc_j[e] != 0xFFFFFFFFu) c.inc_j[e] += base;
+        }
+        inc.insert(inc.end(), t.inc.begin(), t.inc.end());
+        std::vector<uint2>().swap(t.inc);
+        for (uint32_t first = 0; first < c.n; first += 32) {
+            XpbdTile tile;
+            tile.first = c.vtx_off + first;
+            tile.count = (uint16_t)std::min<uint32_t>(32, c.n - first);
+            tile.cloth = (uint16_t)ci_;
+            tiles.push_back(tile);
+        }
+        c.lambda_patch.assign(c.e, 0xFFFFFFFFu);
+        if (patches_ok) {  // append this cloth's patches, rebasing their offsets into the batch arrays
+            PatchArrays& a = patch_arrays;
+            const PatchArrays& b = t.patches;
+            const uint32_t parts0 = (uint32_t)a.parts.size(), con0 = (uint32_t)(a.con.size() / 2),
+                           gofs0 = (uint32_t)a.gofs.size(), slots0 = (uint32_t)a.slots.size();
+            for (size_t h = 0; h < b.header.size(); h += 6) {
+                const uint32_t hd[6] = {b.header[h] + parts0, b.header[h + 1] + con0, b.header[h + 2] + gofs0,
+                                        b.header[h + 3], b.header[h + 4], b.header[h + 5]};
+                a.header.insert(a.header.end(), hd, hd + 6);
+            }
+            a.parts.insert(a.parts.end(), b.parts.begin(), b.parts.end());
+            a.con.insert(a.con.end(), b.con.begin(), b.con.end());
+            for (uint32_t g : b.gofs) a.gofs.push_back(g + slots0);
+            a.slots.insert(a.slots.end(), b.slots.begin(), b.slots.end());
+            a.max_local = std::max(a.max_local, b.max_local);
+            a.max_con = std::max(a.max_con, b.max_con);
+            for (uint32_t k = 0; k < c.e; ++k)
+                if (t.slot[k] != 0xFFFFFFFFu) c.lambda_patch[c.perm[k]] = t.slot[k] + con0;
+        }
+        t.patches = PatchArrays();
     }
     row_off[N] = (uint32_t)inc.size();
+    mark("neighbour tables, patches");
     // ---- Gauss–Seidel table, color-major across cloths
     std::vector<uint4> con(E);
     std::vector<uint32_t> color_off(max_colors + 1, 0);
@@ -469,6 +543,7 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
         }
         color_off[max_colors] = pos;
     }
+    mark("Gauss-Seidel table");
     // ---- device buffers
     cudaError_t err = cudaSuccess;
     XpbdWorld& W = ctx->W;
@@ -715,6 +790,7 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     }
     W.cstats = cstats_d;
     ensure_pinned(ctx, 16 * (size_t)N);
+    mark("device buffers, uploads");
     ctx->committed = true;
     ctx->stats.num_particles = N;
     ctx->stats.num_constraints = E;
