@@ -820,21 +820,40 @@ static bool build_cluster_table(xpbd_ctx* ctx, uint32_t cl) {
     for (size_t k = 1; k < cnt.size(); ++k) max_chunk = std::max(max_chunk, cnt[k]);
     for (size_t k = 1; k < cnt.size(); ++k) cnt[k] += cnt[k - 1];
     if (cluster_gs_smem_bytes(shift, max_chunk) > 220 * 1024) return false;
+    // boundary particles: endpoints of a constraint between two CTAs' particles (any color). Within each
+    // (color, rank) group the records touching a boundary particle come first; the kernel solves them, signals the
+    // cluster barrier, then solves the rest (only this CTA's interior particles) while the barrier completes.
+    std::vector<uint8_t> bnd(N, 0);
+    for (uint32_t e = 0; e < ctx->W.e; ++e) {
+        const uint4 r = ctx->con_host[e];
+        if ((r.x >> shift) != (r.y >> shift)) bnd[r.x] = bnd[r.y] = 1;
+    }
     std::vector<uint4> rec(ctx->W.e);
+    std::vector<uint32_t> nbd((size_t)ncol * cl, 0);
     std::vector<uint32_t> cur(cnt.begin(), cnt.end() - 1);
-    for (uint32_t c = 0; c < ncol; ++c)
-        for (uint32_t e = ctx->color_off_host[c]; e < ctx->color_off_host[c + 1]; ++e)
-            rec[cur[(size_t)c * cl + (ctx->con_host[e].x >> shift)]++] = ctx->con_host[e];
+    for (int pass = 0; pass < 2; ++pass)  // boundary records, then interior records, each in table order
+        for (uint32_t c = 0; c < ncol; ++c)
+            for (uint32_t e = ctx->color_off_host[c]; e < ctx->color_off_host[c + 1]; ++e) {
+                const uint4 r = ctx->con_host[e];
+                const bool b = bnd[r.x] || bnd[r.y];
+                if (b != (pass == 0)) continue;
+                const size_t g = (size_t)c * cl + (r.x >> shift);
+                rec[cur[g]++] = r;
+                if (b) ++nbd[g];
+            }
     cudaError_t err = cudaSuccess;
     uint4* drec = dev_alloc<uint4>(ctx, rec.size(), &err);
-    uint32_t* doff = nullptr;
+    uint32_t *doff = nullptr, *dnbd = nullptr;
     if (err == cudaSuccess) doff = dev_alloc<uint32_t>(ctx, cnt.size(), &err);
+    if (err == cudaSuccess) dnbd = dev_alloc<uint32_t>(ctx, nbd.size(), &err);
     if (err != cudaSuccess) return false;
     if (!rec.empty() && cudaMemcpy(drec, rec.data(), rec.size() * 16, cudaMemcpyHostToDevice) != cudaSuccess)
         return false;
     if (cudaMemcpy(doff, cnt.data(), cnt.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) return false;
+    if (cudaMemcpy(dnbd, nbd.data(), nbd.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) return false;
     ctx->ct.rec = drec;
     ctx->ct.off = doff;
+    ctx->ct.nbd = dnbd;
     ctx->ct.shift = shift;
     ctx->ct.max_chunk = std::max<uint32_t>(max_chunk, 1);
     ctx->ct_cl = cl;

@@ -100,6 +100,12 @@ __device__ __forceinline__ void st_dsmem(uint32_t addr, float4 v) {
                  "f"(v.w)
                  : "memory");
 }
+__device__ __forceinline__ void cluster_arrive() {
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
 __device__ __forceinline__ void cluster_sync() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
@@ -133,6 +139,44 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     return false;
 }
 
+// One constraint of the reference's colored sweep (xpbd_cpu.rs:312-391): both endpoints move by their clamped
+// corrections, pinned endpoints stay.
+__device__ __forceinline__ void gs_solve(const uint4 cr, const uint32_t* s_rank_base, uint32_t shift, uint32_t mask,
+                                         const XpbdDevParams& P) {
+    const uint32_t ai = s_rank_base[cr.x >> shift] + ((cr.x & mask) << 4);
+    const uint32_t aj = s_rank_base[cr.y >> shift] + ((cr.y & mask) << 4);
+    const float4 pi4 = ld_dsmem(ai);
+    const float4 pj4 = ld_dsmem(aj);
+    const float w_i = pi4.w, w_j = pj4.w;
+    if (w_j <= 0.0f && w_i <= 0.0f) return;
+    const V3 p_i = v3(pi4), p_j = v3(pj4);
+    V3 gv = vsub(p_i, p_j);
+    const float len = vlen(gv);
+    if (len < 1e-8f) return;
+    {
+        V3 q;
+        if (!fpdiv3_by_length_fast(gv.x, gv.y, gv.z, len, q.x, q.y, q.z)) q = vdiv(gv, len);
+        gv = q;
+    }
+    const float C = __fsub_rn(len, __uint_as_float(cr.z));
+    const float alpha_t = __fmul_rn(__uint_as_float(cr.w), P.inv_dt_sq);
+    const float wsum = __fadd_rn(__fadd_rn(w_i, w_j), alpha_t);
+    if (wsum < 1e-8f) return;
+    const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
+    const V3 og = {__fmul_rn(P.omega, gv.x), __fmul_rn(P.omega, gv.y), __fmul_rn(P.omega, gv.z)};
+    const V3 dx_i = vclamp(vmul(vmul(og, w_i), dlam));
+    V3 dxj = vmul(vmul(og, w_j), dlam);
+    const V3 dx_j = vclamp(V3{-dxj.x, -dxj.y, -dxj.z});
+    if (w_i > 0.0f) {
+        const V3 n = vadd(p_i, dx_i);
+        st_dsmem(ai, make_float4(n.x, n.y, n.z, w_i));
+    }
+    if (w_j > 0.0f) {
+        const V3 n = vadd(p_j, dx_j);
+        st_dsmem(aj, make_float4(n.x, n.y, n.z, w_j));
+    }
+}
+
 }  // namespace
 
 // T.off[(c * CL + r)] .. T.off[c * CL + r + 1]: records of color c owned by rank r (uint4 {i, j, rest, comp}).
@@ -163,9 +207,18 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
     const uint32_t I = P.iterations;
     // chunk schedule: q = 0, 1, 2, ... over (substep, iteration, color); chunk q uses buffer q&1
     uint32_t phase[2] = {0u, 0u};
+    // the group offsets are read every sweep: keep them in shared memory when they fit
+    constexpr uint32_t kMaxCachedGroups = 512;
+    __shared__ uint32_t s_off[kMaxCachedGroups + 1], s_nbd[kMaxCachedGroups];
+    const bool cached = ncol * CL <= kMaxCachedGroups;
+    if (cached) {
+        for (uint32_t k = tid; k <= ncol * CL; k += nthr) s_off[k] = T.off[k];
+        for (uint32_t k = tid; k < ncol * CL; k += nthr) s_nbd[k] = T.nbd[k];
+    }
+    __syncthreads();
     auto chunk_range = [&](uint32_t c, uint32_t& e0, uint32_t& e1) {
-        e0 = T.off[c * CL + rank];
-        e1 = T.off[c * CL + rank + 1];
+        e0 = cached ? s_off[c * CL + rank] : T.off[c * CL + rank];
+        e1 = cached ? s_off[c * CL + rank + 1] : T.off[c * CL + rank + 1];
     };
     auto issue = [&](uint32_t c, uint32_t b) {
         uint32_t e0, e1;
@@ -213,50 +266,23 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
                 if (q + 1 < total_chunks) issue((c + 1) % ncol, b ^ 1u);  // prefetch the next color's chunk
                 uint32_t e0, e1;
                 chunk_range(c, e0, e1);
+                const uint32_t nb = cached ? s_nbd[c * CL + rank] : T.nbd[c * CL + rank];
+                const uint4* rec = b ? buf1 : buf0;
                 if (e1 > e0) {
                     if (!mbar_wait(&bars[b], phase[b])) {
                         failed = true;
                         if (tid == 0) atomicOr(W.status, XPBD_DEV_BARRIER_TIMEOUT);
                     }
                     phase[b] ^= 1u;
-                    const uint4* rec = b ? buf1 : buf0;
-                    for (uint32_t e = tid; e < e1 - e0 && !failed; e += nthr) {
-                        const uint4 cr = rec[e];
-                        const uint32_t ai = s_rank_base[cr.x >> shift] + ((cr.x & mask) << 4);
-                        const uint32_t aj = s_rank_base[cr.y >> shift] + ((cr.y & mask) << 4);
-                        const float4 pi4 = ld_dsmem(ai);
-                        const float4 pj4 = ld_dsmem(aj);
-                        const float w_i = pi4.w, w_j = pj4.w;
-                        if (w_j <= 0.0f && w_i <= 0.0f) continue;
-                        const V3 p_i = v3(pi4), p_j = v3(pj4);
-                        V3 gv = vsub(p_i, p_j);
-                        const float len = vlen(gv);
-                        if (len < 1e-8f) continue;
-                        {
-                            V3 q;
-                            if (!fpdiv3_by_length_fast(gv.x, gv.y, gv.z, len, q.x, q.y, q.z)) q = vdiv(gv, len);
-                            gv = q;
-                        }
-                        const float C = __fsub_rn(len, __uint_as_float(cr.z));
-                        const float alpha_t = __fmul_rn(__uint_as_float(cr.w), P.inv_dt_sq);
-                        const float wsum = __fadd_rn(__fadd_rn(w_i, w_j), alpha_t);
-                        if (wsum < 1e-8f) continue;
-                        const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
-                        const V3 og = {__fmul_rn(P.omega, gv.x), __fmul_rn(P.omega, gv.y), __fmul_rn(P.omega, gv.z)};
-                        const V3 dx_i = vclamp(vmul(vmul(og, w_i), dlam));
-                        V3 dxj = vmul(vmul(og, w_j), dlam);
-                        const V3 dx_j = vclamp(V3{-dxj.x, -dxj.y, -dxj.z});
-                        if (w_i > 0.0f) {
-                            const V3 n = vadd(p_i, dx_i);
-                            st_dsmem(ai, make_float4(n.x, n.y, n.z, w_i));
-                        }
-                        if (w_j > 0.0f) {
-                            const V3 n = vadd(p_j, dx_j);
-                            st_dsmem(aj, make_float4(n.x, n.y, n.z, w_j));
-                        }
-                    }
                 }
-                cluster_sync();
+                // records touching boundary particles, then the cluster barrier's arrive, then the records of this
+                // CTA's interior particles (no other CTA reads or writes those) while the barrier completes
+                for (uint32_t e = tid; e < nb && !failed; e += nthr) gs_solve(rec[e], s_rank_base, shift, mask, P);
+                cluster_arrive();
+                for (uint32_t e = nb + tid; e < e1 - e0 && !failed; e += nthr)
+                    gs_solve(rec[e], s_rank_base, shift, mask, P);
+                __syncthreads();  // this CTA's interior updates before anyone's next color
+                cluster_wait();
             }
         }
         // finalize own particles (the predict of the next substep re-reads x, v)

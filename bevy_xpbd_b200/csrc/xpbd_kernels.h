@@ -42,6 +42,7 @@ cudaError_t launch_mlp_publish(const float* master, XpbdMlp* mlp, cudaStream_t s
 struct ClusterTable {
     const uint4* rec;    // constraint records grouped by (color, owning rank)
     const uint32_t* off; // ncolors * CL + 1 offsets into rec
+    const uint32_t* nbd; // per (color, rank) group: leading records that touch a boundary particle
     uint32_t shift;      // particles per CTA = 1 << shift
     uint32_t max_chunk;  // largest (color, rank) group, in records
 };
