@@ -901,7 +901,7 @@ static void choose_schedule(xpbd_ctx* ctx) {
     else if (ctx->opts.jacobi_kernel == 3)
         ctx->kernel = 5;
     else
-        ctx->kernel = ctx->patches_ok ? 2 : 5;
+        ctx->kernel = 5;  // thread per particle: measured fastest on the sheets and batches benchmarked
     int maxb = max_blocks_per_sm(ctx->kernel, block, ctx->W);
     if (maxb < 1) maxb = 1;
     int bps = ctx->opts.blocks_per_sm ? (int)ctx->opts.blocks_per_sm : maxb;
