@@ -26,22 +26,11 @@ __device__ __forceinline__ float fpdiv_step(float a, float b, float y) {
     return a == 0.0f ? q : __fmaf_rn(r, y, q);
 }
 
-// The shared-reciprocal quotients without the fallback branch: returns whether every operand is in the range where
-// they are the correctly rounded ones. Hot loops evaluate this for a group of terms and recompute the rare group with
-// a failing operand through fpdiv3, so the common path carries no branch.
-__device__ __forceinline__ bool fpdiv3_fast(float ax, float ay, float az, float b, float& qx, float& qy, float& qz) {
-    const float y = __frcp_rn(b);
-    qx = fpdiv_step(ax, b, y);
-    qy = fpdiv_step(ay, b, y);
-    qz = fpdiv_step(az, b, y);
-    const float mb = fabsf(b);
-    return (mb >= 0x1p-60f) & (mb <= 0x1p60f) & fpdiv_num_ok(ax) & fpdiv_num_ok(ay) & fpdiv_num_ok(az);
-}
-
-// fpdiv3_fast for the components of a vector divided by its own computed length b = |a| (so |a_k| <= b·(1 + 2^-23)
-// and no quotient can overflow): the range test reduces to 2^-60 <= b <= 2^60 and every a_k zero or >= 2^-60 in
-// magnitude, evaluated on the bit patterns — (bits << 1) - 1 wraps zero to the top, so one unsigned minimum over the
-// three components tests "zero or exponent >= 67" at once.
+// The shared-reciprocal quotients for the components of a vector divided by its own computed length b = |a| (so
+// |a_k| <= b·(1 + 2^-23) and no quotient can overflow), without a fallback branch: returns whether they are the
+// correctly rounded ones, so the caller recomputes the rare failing case with fpdiv3. The range test reduces to
+// 2^-60 <= b <= 2^60 and every a_k zero or >= 2^-60 in magnitude, evaluated on the bit patterns — (bits << 1) - 1
+// wraps zero to the top, so one unsigned minimum over the three components tests "zero or exponent >= 67" at once.
 __device__ __forceinline__ bool fpdiv3_by_length_fast(float ax, float ay, float az, float b, float& qx, float& qy,
                                                       float& qz) {
     const float y = __frcp_rn(b);
