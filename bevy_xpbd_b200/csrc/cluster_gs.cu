@@ -100,6 +100,18 @@ __device__ __forceinline__ void st_dsmem(uint32_t addr, float4 v) {
                  "f"(v.w)
                  : "memory");
 }
+__device__ __forceinline__ float4 ld_local(uint32_t addr) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"(addr)
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_local(uint32_t addr, float4 v) {
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+}
 __device__ __forceinline__ void cluster_arrive() {
     asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
 }
@@ -141,12 +153,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 
 // One constraint of the reference's colored sweep (xpbd_cpu.rs:312-391): both endpoints move by their clamped
 // corrections, pinned endpoints stay.
-__device__ __forceinline__ void gs_solve(const uint4 cr, const uint32_t* s_rank_base, uint32_t shift, uint32_t mask,
-                                         const XpbdDevParams& P) {
-    const uint32_t ai = s_rank_base[cr.x >> shift] + ((cr.x & mask) << 4);
-    const uint32_t aj = s_rank_base[cr.y >> shift] + ((cr.y & mask) << 4);
-    const float4 pi4 = ld_dsmem(ai);
-    const float4 pj4 = ld_dsmem(aj);
+// Endpoint i is always this CTA's particle (records are grouped by the rank owning i) and goes through the CTA's own
+// shared window (xs_base); endpoint j too for interior records (LOCAL), otherwise through the cluster window of the
+// CTA owning it.
+template <bool LOCAL>
+__device__ __forceinline__ void gs_solve(const uint4 cr, const uint32_t* s_rank_base, uint32_t xs_base, uint32_t shift,
+                                         uint32_t mask, const XpbdDevParams& P) {
+    const uint32_t ai = xs_base + ((cr.x & mask) << 4);
+    const uint32_t aj = (LOCAL ? xs_base : s_rank_base[cr.y >> shift]) + ((cr.y & mask) << 4);
+    const float4 pi4 = ld_local(ai);
+    const float4 pj4 = LOCAL ? ld_local(aj) : ld_dsmem(aj);
     const float w_i = pi4.w, w_j = pj4.w;
     if (w_j <= 0.0f && w_i <= 0.0f) return;
     const V3 p_i = v3(pi4), p_j = v3(pj4);
@@ -169,11 +185,14 @@ __device__ __forceinline__ void gs_solve(const uint4 cr, const uint32_t* s_rank_
     const V3 dx_j = vclamp(V3{-dxj.x, -dxj.y, -dxj.z});
     if (w_i > 0.0f) {
         const V3 n = vadd(p_i, dx_i);
-        st_dsmem(ai, make_float4(n.x, n.y, n.z, w_i));
+        st_local(ai, make_float4(n.x, n.y, n.z, w_i));
     }
     if (w_j > 0.0f) {
         const V3 n = vadd(p_j, dx_j);
-        st_dsmem(aj, make_float4(n.x, n.y, n.z, w_j));
+        if (LOCAL)
+            st_local(aj, make_float4(n.x, n.y, n.z, w_j));
+        else
+            st_dsmem(aj, make_float4(n.x, n.y, n.z, w_j));
     }
 }
 
@@ -195,6 +214,7 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
     uint4* buf1 = buf0 + T.max_chunk;
     uint64_t* bars = reinterpret_cast<uint64_t*>(buf1 + T.max_chunk);
     __shared__ uint32_t s_rank_base[16];
+    const uint32_t xs_base = smem_u32(xs);
     if (tid < CL) s_rank_base[tid] = map_rank(smem_u32(xs), tid);
     if (tid == 0) {
         mbar_init(&bars[0], 1);
@@ -277,10 +297,11 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
                 }
                 // records touching boundary particles, then the cluster barrier's arrive, then the records of this
                 // CTA's interior particles (no other CTA reads or writes those) while the barrier completes
-                for (uint32_t e = tid; e < nb && !failed; e += nthr) gs_solve(rec[e], s_rank_base, shift, mask, P);
+                for (uint32_t e = tid; e < nb && !failed; e += nthr)
+                    gs_solve<false>(rec[e], s_rank_base, xs_base, shift, mask, P);
                 cluster_arrive();
                 for (uint32_t e = nb + tid; e < e1 - e0 && !failed; e += nthr)
-                    gs_solve(rec[e], s_rank_base, shift, mask, P);
+                    gs_solve<true>(rec[e], s_rank_base, xs_base, shift, mask, P);
                 __syncthreads();  // this CTA's interior updates before anyone's next color
                 cluster_wait();
             }
