@@ -393,7 +393,9 @@ __device__ __forceinline__ bool collect_partners(const float4* __restrict__ src,
 }
 
 // collide: dst[i] = src[i] + clamp(Σ_j corr_ij) with partners in increasing index (xpbd_cpu.rs:82-136).
-__global__ void __launch_bounds__(128) collision_resolve_kernel(XpbdWorld W, const float4* __restrict__ src,
+// 16 blocks of 128 per SM (32 registers): one thread per particle then fits in a single wave for a 262k-particle
+// sheet; the latency-bound walk gains more from the extra resident warps than it loses to the few spills.
+__global__ void __launch_bounds__(128, 16) collision_resolve_kernel(XpbdWorld W, const float4* __restrict__ src,
                                                                 float4* __restrict__ dst, CollisionBuffers B,
                                                                 float inv_cell, uint32_t filter) {
     const XpbdDevParams& P = *W.params;
