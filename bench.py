@@ -67,7 +67,7 @@ def make_workload(name: str, rank: int = 0, world: int = 1, c3_cloths: int = 0) 
                                collision=P.COLLISION_RING_FILTER, thickness=0.002, hash_cell=0.004,
                                hash_table_bits=20, ring_depth=2, ground_enabled=True, ground_y=0.0)
         desc = ("c2: 512x512 sheet, 2 m, unpinned, falling and folding; self collision every substep (hash cell 4 mm, "
-                "2^20 table, stable 4x8-bit radix sort, 27-cell query, 2-ring filter, thickness 2 mm); Jacobi 10x10")
+                "2^20 table, stable 3x8-bit radix sort, 27-cell query, 2-ring filter, thickness 2 mm); Jacobi 10x10")
         total_cloths = world
     elif name == "c3":
         allspecs = wl.config3_batch()

@@ -64,58 +64,79 @@ __global__ void __launch_bounds__(kSortBlock) radix_hist_kernel(const uint32_t* 
     counts[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Single-block exclusive scan of `m` u32 values in place, in chunks of 4 × blockDim.x: each chunk is loaded
-// coalesced into shared memory, every thread scans 4 consecutive values, a warp-shuffle + shared-memory scan combines
-// the threads, and a running carry links the chunks. Launch with 1024 threads.
+// Single-block exclusive scan of `m` u32 values in place, in chunks of 32768: thread t holds 8 rows of 4 consecutive
+// values (row k starts at chunk + 4096k + 4t), so one chunk is one round of coalesced 16-byte loads. The 8 rows are
+// scanned side by side: warp shuffles within each row, one shared-memory pass over the warps' row sums, and a running
+// carry over rows and chunks. Launch with 1024 threads.
 constexpr uint32_t kScanThreads = 1024;
+constexpr uint32_t kScanRows = 8;
+constexpr uint32_t kScanChunk = kScanThreads * 4 * kScanRows;
 __global__ void __launch_bounds__(kScanThreads) exclusive_scan_kernel(uint32_t* __restrict__ a, uint32_t m,
                                                                       uint32_t* __restrict__ total) {
-    __shared__ uint32_t s[4 * kScanThreads];
-    __shared__ uint32_t ws[32];
+    __shared__ uint32_t ws[kScanRows][32];  // warps' row sums, then their exclusive prefixes
+    __shared__ uint32_t rowtot[kScanRows];
     const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    const bool vec = (reinterpret_cast<uintptr_t>(a) & 15u) == 0;
     uint32_t carry = 0;
-    for (uint32_t base = 0; base < m; base += 4 * kScanThreads) {
+    for (uint32_t base = 0; base < m; base += kScanChunk) {
+        uint4 v[kScanRows];
 #pragma unroll
-        for (uint32_t k = 0; k < 4; ++k) {
-            const uint32_t i = base + k * kScanThreads + t;
-            s[k * kScanThreads + t] = i < m ? a[i] : 0u;
+        for (uint32_t k = 0; k < kScanRows; ++k) {
+            const uint32_t i = base + k * (4 * kScanThreads) + 4 * t;
+            if (vec && i + 3 < m && i + 3 > i) {
+                v[k] = *reinterpret_cast<const uint4*>(a + i);
+            } else {
+                v[k].x = i < m ? a[i] : 0u;
+                v[k].y = i + 1 < m ? a[i + 1] : 0u;
+                v[k].z = i + 2 < m ? a[i + 2] : 0u;
+                v[k].w = i + 3 < m ? a[i + 3] : 0u;
+            }
         }
-        __syncthreads();
-        const uint32_t v0 = s[4 * t], v1 = s[4 * t + 1], v2 = s[4 * t + 2], v3 = s[4 * t + 3];
-        const uint32_t sum = v0 + v1 + v2 + v3;
-        uint32_t incl = sum;
+        uint32_t incl[kScanRows];
+#pragma unroll
+        for (uint32_t k = 0; k < kScanRows; ++k) incl[k] = v[k].x + v[k].y + v[k].z + v[k].w;
+#pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t x = __shfl_up_sync(kFullMask, incl, o);
-            if (lane >= (uint32_t)o) incl += x;
+#pragma unroll
+            for (uint32_t k = 0; k < kScanRows; ++k) {
+                const uint32_t x = __shfl_up_sync(kFullMask, incl[k], o);
+                if (lane >= (uint32_t)o) incl[k] += x;
+            }
         }
-        if (lane == 31) ws[warp] = incl;
+        if (lane == 31) {
+#pragma unroll
+            for (uint32_t k = 0; k < kScanRows; ++k) ws[k][warp] = incl[k];
+        }
         __syncthreads();
-        if (warp == 0) {
-            const uint32_t v = ws[lane];
-            uint32_t inc2 = v;
+        if (warp < kScanRows) {
+            const uint32_t w = ws[warp][lane];
+            uint32_t inc2 = w;
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t x = __shfl_up_sync(kFullMask, inc2, o);
                 if (lane >= (uint32_t)o) inc2 += x;
             }
-            ws[lane] = inc2 - v;  // exclusive prefix of the warps' sums
-            if (lane == 31) s[0] = inc2;  // chunk total (s[0] is no longer read: v0 is in registers)
+            ws[warp][lane] = inc2 - w;
+            if (lane == 31) rowtot[warp] = inc2;
         }
-        __syncthreads();
-        const uint32_t ex = carry + ws[warp] + incl - sum;
-        const uint32_t chunk_total = s[0];
-        __syncthreads();  // everyone has read s[0] and ws before they are overwritten
-        s[4 * t] = ex;
-        s[4 * t + 1] = ex + v0;
-        s[4 * t + 2] = ex + v0 + v1;
-        s[4 * t + 3] = ex + v0 + v1 + v2;
         __syncthreads();
 #pragma unroll
-        for (uint32_t k = 0; k < 4; ++k) {
-            const uint32_t i = base + k * kScanThreads + t;
-            if (i < m) a[i] = s[k * kScanThreads + t];
+        for (uint32_t k = 0; k < kScanRows; ++k) {
+            const uint32_t i = base + k * (4 * kScanThreads) + 4 * t;
+            const uint32_t sum = v[k].x + v[k].y + v[k].z + v[k].w;
+            const uint32_t ex = carry + ws[k][warp] + incl[k] - sum;
+            const uint4 o = make_uint4(ex, ex + v[k].x, ex + v[k].x + v[k].y, ex + v[k].x + v[k].y + v[k].z);
+            if (vec && i + 3 < m && i + 3 > i) {
+                *reinterpret_cast<uint4*>(a + i) = o;
+            } else {
+                if (i < m) a[i] = o.x;
+                if (i + 1 < m) a[i + 1] = o.y;
+                if (i + 2 < m) a[i + 2] = o.z;
+                if (i + 3 < m) a[i + 3] = o.w;
+            }
+            carry += rowtot[k];
         }
-        carry += chunk_total;
-        __syncthreads();  // the next chunk's loads overwrite s
+        __syncthreads();  // ws and rowtot are rewritten by the next chunk
+        if (base + kScanChunk < base) break;
     }
     if (total && t == 0) *total = carry;
 }
@@ -263,7 +284,10 @@ cudaError_t collision_build(const XpbdWorld& W, const float4* pos, const Collisi
                             int sms, cudaStream_t st, uint64_t* launches) {
     cudaError_t e = launch_hash_keys(pos, W.n, inv_cell, B.table_bits, B.keys, B.vals, st);
     if (e != cudaSuccess) return e;
-    e = radix_sort_pairs(B.keys, B.vals, B.keys_sorted, B.vals_sorted, W.n, 4, B.sort_scratch,
+    // Keys are below 2^table_bits: the passes over the all-zero high digits would be identity permutations.
+    uint32_t passes = B.table_bits >= 32 ? 4u : (B.table_bits + 7u) / 8u;
+    if (passes < 1u) passes = 1u;
+    e = radix_sort_pairs(B.keys, B.vals, B.keys_sorted, B.vals_sorted, W.n, passes, B.sort_scratch,
                          B.sort_scratch_bytes, st, launches);
     if (e != cudaSuccess) return e;
     uint32_t grid = (W.n + 255) / 256;

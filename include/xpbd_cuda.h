@@ -227,7 +227,8 @@ int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* opts_out);
 
 /* ---- collision pipeline introspection (bit-exact parity tests) ---------------------------------------------- */
 /* Runs the spatial hash on the current positions: keys[i] = hash(cell(x_i)) & (2^bits-1); then the stable LSD
- * radix sort (4 × 8-bit passes) of (key, particle index). Any output may be NULL. */
+ * radix sort (8-bit digits, one pass per 8 bits of the table; the same order as 4 passes) of (key, particle
+ * index). Any output may be NULL. */
 int xpbd_collision_keys(xpbd_ctx* ctx, uint32_t* keys, uint32_t* sorted_keys, uint32_t* sorted_vals);
 /* Collision pairs (a<b, lexicographic) of the current positions under opts.collision; *count = total pairs,
  * at most `cap` written as (a,b) uint32 pairs. */

@@ -213,8 +213,9 @@ def _folded_state(sp, gap=0.03):
 
 
 def test_hash_keys_sorted_order_and_pairs_bit_exact():
-    """Spatial hash keys, stable 4x8-bit LSD radix sort and the collision pair list of a folded sheet, then the
-    collision-heavy trajectory from that state."""
+    """Spatial hash keys, stable 8-bit-digit LSD radix sort and the collision pair list of a folded sheet, then the
+    collision-heavy trajectory from that state. The GPU sorts only the passes that cover the table's bits; the oracle
+    runs all four, whose extra passes over all-zero digits leave the order unchanged."""
     sp, prm, cfg = _folding_sheet(64)
     plug = gpu_sim(sp, prm, cfg)
     xf = _folded_state(sp)
@@ -246,7 +247,10 @@ def test_radix_sort_primitive_matches_stable_argsort():
     from bevy_xpbd_b200 import _native as N
     L = N.load()
     rng = np.random.default_rng(0)
-    for n, hi in [(1, 5), (1000, 7), (300_000, 1 << 20), (70_001, 1 << 32)]:
+    # (n, key bound, passes): the 8-bit passes cover the keys' bits; 300k and 2M keys give 147 and 977 tiles, so the
+    # scan over the (digit, tile) counts runs over two and eight 32768-value chunks.
+    for n, hi, passes in [(1, 5, 4), (1000, 7, 1), (300_000, 1 << 20, 3), (70_001, 1 << 32, 4),
+                          (2_000_000, 1 << 16, 2), (262_144, 1 << 20, 3), (131_071, 1 << 24, 3)]:
         keys = rng.integers(0, hi, n, dtype=np.uint64).astype(np.uint32)
         kin = torch.from_numpy(keys.view(np.int32)).cuda()
         vin = torch.arange(n, dtype=torch.int32, device="cuda")
@@ -255,7 +259,7 @@ def test_radix_sort_primitive_matches_stable_argsort():
         nbytes = L.xpbd_radix_sort_scratch_bytes(n)
         scratch = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
         st = L.xpbd_radix_sort_pairs(C.c_void_p(kin.data_ptr()), C.c_void_p(vin.data_ptr()),
-                                     C.c_void_p(kout.data_ptr()), C.c_void_p(vout.data_ptr()), n, 4,
+                                     C.c_void_p(kout.data_ptr()), C.c_void_p(vout.data_ptr()), n, passes,
                                      C.c_void_p(scratch.data_ptr()), nbytes,
                                      C.c_void_p(torch.cuda.current_stream().cuda_stream))
         assert st == 0
