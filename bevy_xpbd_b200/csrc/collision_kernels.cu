@@ -355,17 +355,45 @@ __device__ __forceinline__ bool narrow_pair(const float4* __restrict__ src, cons
     return true;
 }
 
-// Visits every particle j != i in the (deduplicated) buckets of the 27 cells around i's cell.
+// Squared gaps, in cell units, from u = fl(p·inv_cell) to the lower and upper faces of its cell (f = floor(u)), each
+// shortened by a slack of (2|u| + reach + 2)·2^-20: eight times the rounding of u for both particles of a pair
+// (2^-23·|u| each) and of the gap itself.
+__device__ __forceinline__ void cell_face_gaps(float u, float f, float reach, float& lo2, float& hi2) {
+    const float slack = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(2.0f, fabsf(u)), reach), 2.0f), 0x1p-20f);
+    const float lo = fmaxf(__fsub_rn(__fsub_rn(u, f), slack), 0.0f);
+    const float hi = fmaxf(__fsub_rn(__fsub_rn(__fadd_rn(f, 1.0f), u), slack), 0.0f);
+    lo2 = __fmul_rn(lo, lo);
+    hi2 = __fmul_rn(hi, hi);
+}
+
+// Visits every particle j != i in the (deduplicated) buckets of the 27 cells around i's cell, leaving out the cells
+// that hold no particle within `thickness` of i. The narrow phase accepts only pairs at most `thickness` apart, so
+// when thickness is below the cell size (every accepted partner then lies in one of the 27 cells) the accepted
+// partners are the same; a left-out cell is not marked as seen, so its bucket is still visited through any other
+// cell that hashes to it. Partners are summed in index order, so the visiting order does not change a result.
 template <typename F>
 __device__ __forceinline__ void for_each_candidate(const float4* __restrict__ src, const CollisionBuffers& B,
-                                                   uint32_t n, uint32_t i, float inv_cell, F&& f) {
+                                                   uint32_t n, uint32_t i, float inv_cell, float thickness, F&& f) {
     const uint32_t mask = (B.table_bits >= 32) ? 0xFFFFFFFFu : ((1u << B.table_bits) - 1u);
-    const int3 c = cell_of(src[i], inv_cell);
+    const float4 p = src[i];
+    const float ux = __fmul_rn(p.x, inv_cell), uy = __fmul_rn(p.y, inv_cell), uz = __fmul_rn(p.z, inv_cell);
+    const float fx = floorf(ux), fy = floorf(uy), fz = floorf(uz);
+    const int3 c = make_int3((int)fx, (int)fy, (int)fz);  // == cell_of(p, inv_cell)
+    // Reach of the narrow phase in cell units; the gap test runs only while it is below one cell (NaN: never).
+    const float reach = fabsf(__fmul_rn(thickness, inv_cell));
+    const float reach2 = reach < 0.999f ? __fmul_rn(__fmul_rn(reach, reach), 1.001f) : __int_as_float(0x7f800000);
+    float xlo2, xhi2, ylo2, yhi2, zlo2, zhi2;
+    cell_face_gaps(ux, fx, reach, xlo2, xhi2);
+    cell_face_gaps(uy, fy, reach, ylo2, yhi2);
+    cell_face_gaps(uz, fz, reach, zlo2, zhi2);
     uint32_t seen[27];
     int nseen = 0;
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
+    for (int dz = -1; dz <= 1; ++dz) {
+        const float gz = dz < 0 ? zlo2 : (dz > 0 ? zhi2 : 0.0f);
+        for (int dy = -1; dy <= 1; ++dy) {
+            const float gyz = __fadd_rn(gz, dy < 0 ? ylo2 : (dy > 0 ? yhi2 : 0.0f));
             for (int dx = -1; dx <= 1; ++dx) {
+                if (__fadd_rn(gyz, dx < 0 ? xlo2 : (dx > 0 ? xhi2 : 0.0f)) > reach2) continue;
                 const uint32_t h = hash_cell(make_int3(c.x + dx, c.y + dy, c.z + dz), mask);
                 bool dup = false;
                 for (int q = 0; q < nseen; ++q) dup |= (seen[q] == h);
@@ -378,6 +406,8 @@ __device__ __forceinline__ void for_each_candidate(const float4* __restrict__ sr
                     if (j != i) f(j);
                 }
             }
+        }
+    }
 }
 
 constexpr int kPartnerCap = 24;
@@ -390,7 +420,7 @@ __device__ __forceinline__ bool collect_partners(const float4* __restrict__ src,
                                                  uint32_t* pj, F3c* pc, int& cnt) {
     cnt = 0;
     bool overflow = false;
-    for_each_candidate(src, B, n, i, inv_cell, [&](uint32_t j) {
+    for_each_candidate(src, B, n, i, inv_cell, thickness, [&](uint32_t j) {
         if ((long long)j <= lo) return;
         if (ONLY_GREATER && j < i) return;
         if (cnt == kPartnerCap && j > pj[kPartnerCap - 1]) {
@@ -425,7 +455,7 @@ __global__ void __launch_bounds__(128, 16) collision_resolve_kernel(XpbdWorld W,
     const XpbdDevParams& P = *W.params;
     const float thickness = P.thickness, coll_scale = P.coll_scale;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < W.n; p += gridDim.x * blockDim.x) {
-        const uint32_t i = B.vals_sorted[p];  // sorted order: neighbouring threads query neighbouring cells
+        const uint32_t i = p;  // mesh order: neighbouring threads query overlapping cells
         const float4 pi = src[i];
         if (pi.w <= 0.0f) {
             dst[i] = pi;
@@ -469,7 +499,7 @@ __global__ void pair_count_kernel(XpbdWorld W, const float4* __restrict__ src, C
     const XpbdDevParams& P = *W.params;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n; i += gridDim.x * blockDim.x) {
         uint32_t c = 0;
-        for_each_candidate(src, B, W.n, i, inv_cell, [&](uint32_t j) {
+        for_each_candidate(src, B, W.n, i, inv_cell, P.thickness, [&](uint32_t j) {
             if (j < i) return;
             F3c tmp;
             if (narrow_pair(src, W.rest, B, filter, P.thickness, P.coll_scale, i, j, i, tmp)) ++c;

@@ -181,6 +181,45 @@ def test_collision_two_particle_known_answer():
     assert np.array_equal(out, ref)
 
 
+@pytest.mark.parametrize("offset,thickness", [((0.0, 0.0, 0.0), 0.03), ((1000.0, -37.5, 250.0), 0.03),
+                                              ((-3.3, 0.7, -0.01), 0.02)])
+def test_collision_cell_reach_keeps_pairs_across_faces_edges_corners(offset, thickness):
+    """The 27-cell query leaves out cells beyond the narrow phase's reach. Pairs just inside the reach whose
+    particles sit a hair on either side of cell faces, along face, edge and corner directions, near the origin and at
+    large coordinates: the pair list equals the oracle's and one substep equals the oracle's all-pairs loop."""
+    cell = 0.04
+    rng = np.random.default_rng(11)
+    m = 1500
+    hair = rng.choice([0.0, 1e-7, 1e-6, 1e-4, 0.3 * cell], (m, 3)) * rng.choice([-1.0, 1.0], (m, 3))
+    base = rng.integers(-12, 12, (m, 3)) * cell + hair
+    axis = np.eye(3)[rng.integers(0, 3, m)] * rng.choice([-1.0, 1.0], (m, 1))
+    edge = rng.choice([-1.0, 0.0, 1.0], (m, 3))
+    edge[np.all(edge == 0, axis=1), 0] = 1.0
+    rand = rng.normal(size=(m, 3))
+    kind = rng.integers(0, 3, m)[:, None]
+    dirs = np.where(kind == 0, axis, np.where(kind == 1, edge, rand))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    dist = thickness * (1.0 - rng.choice([1e-6, 1e-4, 1e-2, 0.3], m))
+    x = (np.concatenate([base, base + dirs * dist[:, None]]) + np.asarray(offset)).astype(np.float32)
+    n = len(x)
+    g = np.arange(n)
+    rest = np.stack([g % 64, (g // 64) % 64, g // 4096], axis=1).astype(np.float32)  # rest distances >= 1
+    e0 = np.zeros(0, np.uint32)
+    spec = wl.ClothSpec(x, np.ones(n, np.float32), e0, e0, np.zeros(0, np.float32), np.zeros(0, np.float32), e0,
+                        rest)
+    prm = params_for(1, 0, 1.0, gravity=(0.0, 0.0, 0.0))
+    cfg = _cfg(solve_substeps=1, collision=P.COLLISION_REST_FILTER, thickness=thickness, coll_scale=0.38,
+               hash_cell=cell)
+    plug = gpu_sim(spec, prm, cfg)
+    o = oracle_sim(spec, prm, cfg)
+    pairs = plug.collision_pairs()
+    assert len(pairs) > m // 2
+    assert np.array_equal(pairs, o.collision_pairs())
+    plug.step(frames=1)
+    o.substeps(1, brute_force=True)
+    assert max_abs(plug.positions(), o.state()[0]) == 0.0
+
+
 def _folding_sheet(side=48, frames=40):
     sp = wl.config2_sheet(seed=2, side=side)
     prm = params_for(10, 10, 1.0)
