@@ -444,6 +444,100 @@ def run_warm_leg(args, device: int) -> dict:
 
 
 # ------------------------------------------------------------------------------------------------ CPU arm
+def run_prep_leg(device: int, reps: int = 5) -> dict:
+    """Mesh preparation of the c3 batch (256 cloths in one call): greedy coloring and neighbour table on the GPU
+    (inputs resident, CUDA events on the stream) against the host coloring on all host threads (one cloth per task,
+    as xpbd_commit runs it). The GPU coloring is checked against the host's before it is timed."""
+    import ctypes as C
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    from bevy_xpbd_b200 import _native as N
+    from bevy_xpbd_b200 import workloads as wl
+    L = N.load()
+    specs = wl.config3_batch()
+    voff = np.cumsum([0] + [s.num_particles for s in specs])
+    n, e = int(voff[-1]), sum(s.num_constraints for s in specs)
+    ci = np.concatenate([s.constraint_i + o for s, o in zip(specs, voff)]).astype(np.uint32)
+    cj = np.concatenate([s.constraint_j + o for s, o in zip(specs, voff)]).astype(np.uint32)
+    dev = f"cuda:{device}"
+    st = torch.cuda.current_stream(device)
+    sp = C.c_void_p(st.cuda_stream)
+    h2d0, h2d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hci = torch.from_numpy(ci.view(np.int32)).pin_memory()
+    hcj = torch.from_numpy(cj.view(np.int32)).pin_memory()
+    h2d0.record(st)
+    dci, dcj = hci.to(dev, non_blocking=True), hcj.to(dev, non_blocking=True)
+    h2d1.record(st)
+    perm = torch.empty(e, dtype=torch.int32, device=dev)
+    colors = torch.empty(e, dtype=torch.int32, device=dev)
+    offs = torch.empty(e + 2, dtype=torch.int32, device=dev)
+    cbytes = L.xpbd_color_constraints_device_scratch_bytes(n, e)
+    tbytes = L.xpbd_neighbor_table_device_scratch_bytes(n, e)
+    scratch = torch.empty(max(cbytes, tbytes), dtype=torch.uint8, device=dev)
+    row = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    other = torch.empty(2 * e, dtype=torch.int32, device=dev)
+    eid = torch.empty(2 * e, dtype=torch.int32, device=dev)
+    vp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    bc = C.c_uint32()
+
+    def color():
+        r = L.xpbd_color_constraints_device(n, e, vp(dci), vp(dcj), 0, vp(perm), vp(colors), vp(offs), C.byref(bc),
+                                            vp(scratch), cbytes, sp)
+        if r != 0:
+            raise RuntimeError(f"xpbd_color_constraints_device: {r}")
+
+    def table():
+        r = L.xpbd_neighbor_table_device(n, e, vp(dci), vp(dcj), vp(row), vp(other), vp(eid), vp(scratch), tbytes, sp)
+        if r != 0:
+            raise RuntimeError(f"xpbd_neighbor_table_device: {r}")
+
+    def timed(fn):
+        ts = []
+        for k in range(reps + 2):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(device)
+            a.record(st)
+            fn()
+            b.record(st)
+            torch.cuda.synchronize(device)
+            if k >= 2:
+                ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    color_ms = timed(color)
+    table_ms = timed(table)
+    # host coloring, one cloth per task on every host thread
+    eoff = np.cumsum([0] + [s.num_constraints for s in specs])
+
+    def host_one(k):
+        s = specs[k]
+        a = np.ascontiguousarray(s.constraint_i, np.uint32)
+        b = np.ascontiguousarray(s.constraint_j, np.uint32)
+        pm = np.zeros(s.num_constraints, np.uint32)
+        of = np.zeros(s.num_constraints + 2, np.uint32)
+        nb = C.c_uint32()
+        L.xpbd_color_constraints(s.num_particles, s.num_constraints, a.ctypes.data, b.ctypes.data, 0, pm.ctypes.data,
+                                 of.ctypes.data, C.byref(nb))
+        return pm, of[: nb.value + 1]
+
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        host = list(ex.map(host_one, range(len(specs))))
+    host_ms = (time.perf_counter() - t0) * 1e3
+    gcol = colors.cpu().numpy().view(np.uint32)
+    for k, (pm, of) in enumerate(host):
+        mine = gcol[eoff[k]:eoff[k + 1]][pm]
+        if np.any(np.diff(mine.astype(np.int64)) < 0) or not np.array_equal(np.searchsorted(mine, np.arange(len(of)), side="left"), of):
+            raise RuntimeError(f"device coloring differs from the host coloring on cloth {k}")
+    return {"workload": f"c3: {len(specs)} cloths in one call, {n} particles, {e} constraints",
+            "device_color_ms": round(color_ms, 2), "device_neighbor_table_ms": round(table_ms, 2),
+            "h2d_ms": round(h2d0.elapsed_time(h2d1), 2), "host_color_ms": round(host_ms, 1),
+            "host_threads": threads, "batches": bc.value, "identical_to_host": True}
+
+
 def cpu_oracle_run(w: dict, budget_s: float, max_cloths: int | None = None, min_frames: int = 1,
                    variant: str = "omp"):
     """Times the CPU restatement of xpbd_cpu.rs (OpenMP build, or the serial build with the reference's loop order)
@@ -515,6 +609,7 @@ def main():
     ap.add_argument("--no-warm", action="store_true", help="skip the learned-vs-plain convergence leg")
     ap.add_argument("--warm-frames", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-prep", action="store_true", help="skip the mesh-preparation leg (GPU vs host coloring)")
     ap.add_argument("--c3-cloths", type=int, default=0, help="first K cloths of c3 only (profiling cases)")
     ap.add_argument("--no-autotune", action="store_true", help="library default schedule")
     ap.add_argument("--jacobi-kernel", type=int, default=None, help="1 warp tiles, 2 spatial patches, 3 rows")
@@ -550,6 +645,8 @@ def main():
                            "clocks": b["clocks"]}
     if rank == 0 and world == 1 and not args.no_warm:
         line["warm_start"] = run_warm_leg(args, local)
+    if rank == 0 and world == 1 and not args.no_prep:
+        line["mesh_prep"] = run_prep_leg(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_oracle_run(w, args.cpu_seconds, max_cloths=16 if args.workload == "c3" else None)
         line["cpu_baseline"] = {"value": round(r["value"], 4), "unit": UNIT, "cores": r["cores"], "kind": "port",

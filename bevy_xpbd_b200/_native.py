@@ -37,7 +37,8 @@ EXPORTED = [
     "xpbd_converge_history", "xpbd_converge_cloth_iterations", "xpbd_selftest_division",
     "xpbd_mlp_minibatch_gradients", "xpbd_mlp_apply_gradients", "xpbd_set_triangles", "xpbd_read_normals",
     "xpbd_mesh_grid_hanging", "xpbd_mesh_from_obj", "xpbd_mesh_from_triangles", "xpbd_mesh_sizes", "xpbd_mesh_get",
-    "xpbd_mesh_free", "xpbd_set_cloth_grab",
+    "xpbd_mesh_free", "xpbd_set_cloth_grab", "xpbd_color_constraints_device_scratch_bytes",
+    "xpbd_color_constraints_device", "xpbd_neighbor_table_device_scratch_bytes", "xpbd_neighbor_table_device",
 ]
 MLP_PARAMS = 4865
 MLP_NORM = 20
@@ -131,6 +132,10 @@ def load():
         "xpbd_debug_force_barrier_timeout": (I, [P, C.c_float]),
         "xpbd_color_constraints": (I, [U, U, P, P, U, P, P, C.POINTER(U)]),
         "xpbd_radix_sort_pairs_noalloc": (I, [P, P, P, P, U, U, P]),
+        "xpbd_color_constraints_device_scratch_bytes": (C.c_size_t, [U, U]),
+        "xpbd_color_constraints_device": (I, [U, U, P, P, U, P, P, P, C.POINTER(U), P, C.c_size_t, P]),
+        "xpbd_neighbor_table_device_scratch_bytes": (C.c_size_t, [U, U]),
+        "xpbd_neighbor_table_device": (I, [U, U, P, P, P, P, P, P, C.c_size_t, P]),
         "xpbd_set_warm_lambda": (I, [P, U, P]),
         "xpbd_mlp_init": (I, [P, C.c_uint64, U]),
         "xpbd_mlp_set_params": (I, [P, P, P]),

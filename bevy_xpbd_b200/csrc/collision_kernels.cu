@@ -195,6 +195,12 @@ __global__ void __launch_bounds__(kSortBlock) radix_scatter_kernel(const uint32_
     }
 }
 
+cudaError_t launch_exclusive_scan(uint32_t* a, uint32_t m, uint32_t* total, cudaStream_t st) {
+    if (m == 0) return cudaSuccess;
+    exclusive_scan_kernel<<<1, kScanThreads, 0, st>>>(a, m, total);
+    return cudaGetLastError();
+}
+
 size_t radix_sort_scratch_bytes(uint32_t n) {
     size_t tiles = (n + kSortTile - 1) / kSortTile;
     if (tiles == 0) tiles = 1;

@@ -65,6 +65,8 @@ struct CollisionBuffers {
     const uint32_t* ring_off;  // n + 1 (ring filter)
     const uint32_t* ring_idx;
 };
+// Single-block exclusive scan of m u32 values in place; total (device, may be null) receives the sum.
+cudaError_t launch_exclusive_scan(uint32_t* a, uint32_t m, uint32_t* total, cudaStream_t st);
 size_t radix_sort_scratch_bytes(uint32_t n);
 cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                              uint32_t* vals_out, uint32_t n, uint32_t passes, void* scratch, size_t scratch_bytes,

@@ -251,6 +251,30 @@ int xpbd_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint
 #define XPBD_NOALLOC_SORT_MAX_KEYS (1u << 18)
 int xpbd_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                   uint32_t* vals_out, uint32_t n, uint32_t passes, void* stream);
+/* Greedy edge coloring on the GPU, bit-identical to the host coloring xpbd_color_constraints and so to
+ * partition_constraints_for_gs_batches (mesh_prep.rs:153-221): the same colors, the same (color, index) batch order.
+ * Device arrays: constraint_i/j[num_constraints]; perm[num_constraints] = input index of the k-th batch-sorted
+ * constraint; colors[num_constraints] (may be NULL) = color of each input constraint; offsets[num_constraints + 2]
+ * receives batch_count + 1 batch starts (no constraints: one empty batch, offsets {0, 0}). *batch_count is written on the host, so the call synchronises `stream`
+ * (twice); the rest of the work is enqueued on it. A batch of cloths with disjoint particle ranges may be colored in
+ * one call: each cloth gets the coloring it would get alone, and perm is then color-major across the cloths (the
+ * batch's Gauss–Seidel order). Endpoints out of range or i == j: XPBD_ERR_INDEX_RANGE. `scratch` (256-byte aligned)
+ * must hold xpbd_color_constraints_device_scratch_bytes(num_particles, num_constraints) bytes (about 48 bytes per
+ * constraint). */
+size_t xpbd_color_constraints_device_scratch_bytes(uint32_t num_particles, uint32_t num_constraints);
+int xpbd_color_constraints_device(uint32_t num_particles, uint32_t num_constraints, const uint32_t* constraint_i,
+                                  const uint32_t* constraint_j, uint32_t order, uint32_t* perm, uint32_t* colors,
+                                  uint32_t* offsets, uint32_t* batch_count, void* scratch, size_t scratch_bytes,
+                                  void* stream);
+/* Particle-major neighbour table of finalize_cloth_mesh (mesh_prep.rs:588-635) on the GPU, for constraints already in
+ * batch order (device arrays): row_off[num_particles + 1]; row p of other/eid[2 * num_constraints] lists, in
+ * increasing constraint position (i slot before j slot), the opposite endpoint and the constraint position of every
+ * constraint at p. Synchronises `stream` once (index check). `scratch` (256-byte aligned) must hold
+ * xpbd_neighbor_table_device_scratch_bytes(num_particles, num_constraints) bytes. */
+size_t xpbd_neighbor_table_device_scratch_bytes(uint32_t num_particles, uint32_t num_constraints);
+int xpbd_neighbor_table_device(uint32_t num_particles, uint32_t num_constraints, const uint32_t* constraint_i,
+                               const uint32_t* constraint_j, uint32_t* row_off, uint32_t* other, uint32_t* eid,
+                               void* scratch, size_t scratch_bytes, void* stream);
 /* keys[i] = prime-hash(floor(xyz_i * inv_cell)) & (2^bits - 1), positions as float4 (w ignored). */
 int xpbd_hash_keys(const float* xyzw, uint32_t n, float inv_cell, uint32_t table_bits, uint32_t* keys,
                    void* stream);
