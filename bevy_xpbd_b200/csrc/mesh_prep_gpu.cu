@@ -24,6 +24,9 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 
 #include "../../include/xpbd_cuda.h"
 #include "xpbd_internal.h"
@@ -35,24 +38,27 @@ namespace {
 constexpr unsigned kMask = 0xFFFFFFFFu;
 constexpr uint32_t kNoColor = 0xFFFFFFFFu;
 constexpr int kPrepBlock = 256;
-constexpr int kJpBlock = 256;
+constexpr int kJpBlock = 1024;
 constexpr unsigned long long kPrepBarrierTimeoutNs = 2000000000ull;
 
 // Control words at the start of the scratch.
 enum : uint32_t {
     kCtlCount0 = 0,  // frontier sizes, rotating over three words (round r reads word r % 3)
-    kCtlBarrier = 3,
     kCtlStatus = 4,  // XPBD_DEV_* bits
     kCtlRounds = 5,
     kCtlColors = 6,  // largest color + 1
     kCtlDone = 7,    // constraints colored
     kCtlMaxDeg = 8,
-    kCtlWords = 64,  // 256 bytes
+    kCtlT0 = 10,     // globaltimer stamps (two words each): kernel start, end of phase 0, end of the rounds
+    kCtlT1 = 12,
+    kCtlT2 = 14,
+    kCtlBarrier = 32,  // in its own 128-byte line, apart from the frontier counters
+    kCtlWords = 64,    // 256 bytes
 };
 constexpr uint32_t kStatusSchedule = 0x100u;  // a constraint was reached before an earlier-ranked neighbour
 
 struct ColorLayout {  // offsets in 32-bit words from the scratch base; every array starts on 256 bytes
-    size_t ctl, deg, cursor, adj, ka, va, kb, vb, rank, pending, color, front0, front1, radix;
+    size_t ctl, deg, cursor, adj, ka, va, kb, vb, rc, pending, front0, front1, radix;
     size_t radix_bytes, total_bytes;
 };
 
@@ -73,9 +79,8 @@ ColorLayout color_layout(uint32_t n, uint32_t e) {
     L.va = take_words(off, e);
     L.kb = take_words(off, e);
     L.vb = take_words(off, e);
-    L.rank = take_words(off, e);
+    L.rc = take_words(off, 2 * (size_t)e);
     L.pending = take_words(off, e);
-    L.color = take_words(off, e);
     L.front0 = take_words(off, e);
     L.front1 = take_words(off, e);
     L.radix = off;
@@ -154,15 +159,6 @@ __global__ void order_key_kernel(uint32_t stage, const uint32_t* __restrict__ ci
     }
 }
 
-__global__ void rank_kernel(const uint32_t* __restrict__ order, uint32_t e, uint32_t* __restrict__ rank) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < e; k += gridDim.x * blockDim.x)
-        rank[order ? order[k] : k] = k;
-}
-
-__global__ void iota_kernel(uint32_t* __restrict__ a, uint32_t m) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) a[k] = k;
-}
-
 __global__ void adjacency_kernel(const uint32_t* __restrict__ ci, const uint32_t* __restrict__ cj, uint32_t e,
                                  uint32_t* __restrict__ cursor, uint32_t* __restrict__ adj) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < e; k += gridDim.x * blockDim.x) {
@@ -222,41 +218,63 @@ struct JpArgs {
     const uint32_t* cj;
     const uint32_t* row_off;  // n + 1
     const uint32_t* adj;      // 2e constraint ids, row p = constraints at particle p
-    const uint32_t* rank;     // processing rank of each constraint
+    uint2* rc;                // per constraint {processing rank, color}; colors are written during the rounds
     uint32_t* pending;        // earlier-ranked neighbour slots not yet colored
-    uint32_t* color;
     uint32_t* front0;
     uint32_t* front1;
     uint32_t* ctl;
     uint32_t e;
 };
 
+constexpr uint32_t kGroup = 8;       // lanes per frontier constraint (4 constraints per warp)
+constexpr uint32_t kGroupSlots = 4;  // neighbour slots per lane kept in registers (degree sums up to 32)
+
 // Neighbour slot t of constraint k: row of its i endpoint first, then row of its j endpoint.
 __device__ __forceinline__ uint32_t slot_at(const JpArgs& a, uint32_t t, uint32_t b0, uint32_t l0, uint32_t b1) {
     return __ldg(&a.adj[t < l0 ? b0 + t : b1 + (t - l0)]);
 }
 
+// OR over the kGroup lanes of each group; every lane of the warp takes part.
+__device__ __forceinline__ unsigned long long group_or(unsigned long long m) {
+#pragma unroll
+    for (uint32_t o = 1; o < kGroup; o <<= 1) {
+        const uint32_t lo = __shfl_xor_sync(kMask, (uint32_t)m, o);
+        const uint32_t hi = __shfl_xor_sync(kMask, (uint32_t)(m >> 32), o);
+        m |= ((unsigned long long)hi << 32) | lo;
+    }
+    return m;
+}
+
+__device__ __forceinline__ void stamp(uint32_t* ctl, uint32_t word) {
+    const unsigned long long t = globaltimer_ns();
+    ctl[word] = (uint32_t)t;
+    ctl[word + 1] = (uint32_t)(t >> 32);
+}
+
 __global__ void __launch_bounds__(kJpBlock) jp_color_kernel(JpArgs a) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
-    // phase 0: pending counts and the first frontier
+    if (tid == 0) stamp(a.ctl, kCtlT0);
+    // phase 0: pending counts and the first frontier (nothing writes rc in this phase)
     for (uint32_t k = tid; k < a.e; k += nthr) {
-        const uint32_t r = __ldg(&a.rank[k]);
+        const uint32_t r = a.rc[k].x;
         const uint32_t p0 = __ldg(&a.ci[k]), p1 = __ldg(&a.cj[k]);
         uint32_t cnt = 0;
         for (uint32_t q = __ldg(&a.row_off[p0]), q1 = __ldg(&a.row_off[p0 + 1]); q < q1; ++q) {
             const uint32_t f = __ldg(&a.adj[q]);
-            cnt += (f != k && __ldg(&a.rank[f]) < r) ? 1u : 0u;
+            cnt += (f != k && a.rc[f].x < r) ? 1u : 0u;
         }
         for (uint32_t q = __ldg(&a.row_off[p1]), q1 = __ldg(&a.row_off[p1 + 1]); q < q1; ++q) {
             const uint32_t f = __ldg(&a.adj[q]);
-            cnt += (f != k && __ldg(&a.rank[f]) < r) ? 1u : 0u;
+            cnt += (f != k && a.rc[f].x < r) ? 1u : 0u;
         }
         a.pending[k] = cnt;
-        a.color[k] = kNoColor;
         if (cnt == 0) a.front0[atomicAdd(&a.ctl[kCtlCount0], 1u)] = k;
     }
     if (!prep_grid_barrier(a.ctl)) return;
-    const uint32_t lane = threadIdx.x & 31u, gw = tid >> 5, nw = nthr >> 5;
+    if (tid == 0) stamp(a.ctl, kCtlT1);
+    const uint32_t lane = threadIdx.x & 31u, sub = lane & (kGroup - 1u), gw = tid >> 5, nw = nthr >> 5;
+    constexpr uint32_t kPerWarp = 32u / kGroup;
+    uint32_t max_color = 0;  // largest color + 1 this thread wrote
     for (uint32_t round = 0;; ++round) {
         const uint32_t size = __ldcg(&a.ctl[kCtlCount0 + round % 3]);
         if (size == 0) break;
@@ -274,46 +292,110 @@ __global__ void __launch_bounds__(kJpBlock) jp_color_kernel(JpArgs a) {
         const uint32_t* cur = (round & 1u) ? a.front1 : a.front0;
         uint32_t* nxt = (round & 1u) ? a.front0 : a.front1;
         uint32_t* ncount = &a.ctl[kCtlCount0 + (round + 1) % 3];
-        for (uint32_t it = gw; it < size; it += nw) {  // warp-uniform loop
-            const uint32_t k = __ldcg(&cur[it]);
-            const uint32_t r = __ldg(&a.rank[k]);
-            const uint32_t p0 = __ldg(&a.ci[k]), p1 = __ldg(&a.cj[k]);
-            const uint32_t b0 = __ldg(&a.row_off[p0]), l0 = __ldg(&a.row_off[p0 + 1]) - b0;
-            const uint32_t b1 = __ldg(&a.row_off[p1]), l1 = __ldg(&a.row_off[p1 + 1]) - b1;
-            const uint32_t len = l0 + l1;
-            uint32_t col = 0;
+        for (uint32_t first = gw * kPerWarp; first < size; first += nw * kPerWarp) {  // warp-uniform loop
+            const uint32_t item = first + lane / kGroup;
+            const bool valid = item < size;
+            uint32_t k = 0, r = 0, b0 = 0, l0 = 0, b1 = 0, len = 0;
+            if (valid) {
+                k = __ldcg(&cur[item]);
+                r = __ldcg(&a.rc[k].x);
+                const uint32_t p0 = __ldg(&a.ci[k]), p1 = __ldg(&a.cj[k]);
+                b0 = __ldg(&a.row_off[p0]);
+                l0 = __ldg(&a.row_off[p0 + 1]) - b0;
+                b1 = __ldg(&a.row_off[p1]);
+                len = l0 + (__ldg(&a.row_off[p1 + 1]) - b1);
+            }
+            // colors of the earlier-ranked neighbours, first 64-color window
+            uint32_t fs[kGroupSlots], rs[kGroupSlots];
+            unsigned long long m = 0;
             bool missing = false;
-            for (uint32_t base = 0;; base += 64u) {
-                unsigned long long m = 0;
-                for (uint32_t t = lane; t < len; t += 32u) {
+#pragma unroll
+            for (uint32_t j = 0; j < kGroupSlots; ++j) {
+                const uint32_t t = sub + kGroup * j;
+                fs[j] = kNoColor;
+                rs[j] = 0;
+                if (t < len) {
                     const uint32_t f = slot_at(a, t, b0, l0, b1);
-                    if (f != k && __ldg(&a.rank[f]) < r) {
-                        const uint32_t c = __ldcg(&a.color[f]);
-                        if (c == kNoColor) missing = true;
-                        else if (c - base < 64u) m |= 1ull << (c - base);
+                    const uint2 v = __ldcg(&a.rc[f]);
+                    fs[j] = f;
+                    rs[j] = v.x;
+                    if (f != k && v.x < r) {
+                        if (v.y == kNoColor) missing = true;
+                        else if (v.y < 64u) m |= 1ull << v.y;
                     }
                 }
-                const uint32_t lo = __reduce_or_sync(kMask, (uint32_t)m);
-                const uint32_t hi = __reduce_or_sync(kMask, (uint32_t)(m >> 32));
-                const unsigned long long used = ((unsigned long long)hi << 32) | lo;
-                if (used != ~0ull) {
-                    col = base + (uint32_t)__ffsll((long long)~used) - 1u;
-                    break;
+            }
+            for (uint32_t t = sub + kGroup * kGroupSlots; t < len; t += kGroup) {
+                const uint32_t f = slot_at(a, t, b0, l0, b1);
+                const uint2 v = __ldcg(&a.rc[f]);
+                if (f != k && v.x < r) {
+                    if (v.y == kNoColor) missing = true;
+                    else if (v.y < 64u) m |= 1ull << v.y;
+                }
+            }
+            m = group_or(m);
+            bool need = valid && m == ~0ull;
+            uint32_t col = (valid && !need) ? (uint32_t)__ffsll((long long)~m) - 1u : 0u;
+            for (uint32_t base = 64u; __any_sync(kMask, need); base += 64u) {  // rare: 64 colors taken
+                unsigned long long w = 0;
+                if (need) {
+                    for (uint32_t t = sub; t < len; t += kGroup) {
+                        const uint32_t f = slot_at(a, t, b0, l0, b1);
+                        const uint2 v = __ldcg(&a.rc[f]);
+                        if (f != k && v.x < r && v.y != kNoColor && v.y - base < 64u) w |= 1ull << (v.y - base);
+                    }
+                }
+                w = group_or(w);
+                if (need && w != ~0ull) {
+                    col = base + (uint32_t)__ffsll((long long)~w) - 1u;
+                    need = false;
                 }
             }
             if (missing) atomicOr(&a.ctl[kCtlStatus], kStatusSchedule);
-            if (lane == 0) {
-                __stcg(&a.color[k], col);
-                atomicMax(&a.ctl[kCtlColors], col + 1u);
+            if (valid && sub == 0) {
+                __stcg(&a.rc[k].y, col);
+                max_color = max(max_color, col + 1u);
             }
-            for (uint32_t t = lane; t < len; t += 32u) {
-                const uint32_t f = slot_at(a, t, b0, l0, b1);
-                if (f != k && __ldg(&a.rank[f]) > r) {
-                    if (atomicSub(&a.pending[f], 1u) == 1u) __stcg(&nxt[atomicAdd(ncount, 1u)], f);
+            // release the later-ranked neighbours; the ones that become ready join the next frontier with one
+            // counter atomic per warp and slot
+#pragma unroll
+            for (uint32_t j = 0; j < kGroupSlots; ++j) {
+                const uint32_t f = fs[j];
+                const bool push = valid && f != kNoColor && f != k && rs[j] > r && atomicSub(&a.pending[f], 1u) == 1u;
+                const unsigned ballot = __ballot_sync(kMask, push);
+                if (ballot) {
+                    const uint32_t leader = (uint32_t)__ffs(ballot) - 1u;
+                    uint32_t at = 0;
+                    if (lane == leader) at = atomicAdd(ncount, (uint32_t)__popc(ballot));
+                    at = __shfl_sync(kMask, at, leader);
+                    if (push) __stcg(&nxt[at + (uint32_t)__popc(ballot & ((1u << lane) - 1u))], f);
                 }
+            }
+            if (!valid) continue;
+            for (uint32_t t = sub + kGroup * kGroupSlots; t < len; t += kGroup) {
+                const uint32_t f = slot_at(a, t, b0, l0, b1);
+                if (f != k && __ldcg(&a.rc[f].x) > r && atomicSub(&a.pending[f], 1u) == 1u)
+                    __stcg(&nxt[atomicAdd(ncount, 1u)], f);
             }
         }
         if (!prep_grid_barrier(a.ctl)) return;
+    }
+    max_color = __reduce_max_sync(kMask, max_color);
+    if (lane == 0 && max_color) atomicMax(&a.ctl[kCtlColors], max_color);
+    if (tid == 0) stamp(a.ctl, kCtlT2);
+}
+
+// rc[k] = {rank, no color}: rank[order[k]] = k (order == nullptr: index order).
+__global__ void rank_kernel(const uint32_t* __restrict__ order, uint32_t e, uint2* __restrict__ rc) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < e; k += gridDim.x * blockDim.x)
+        rc[order ? order[k] : k] = make_uint2(k, kNoColor);
+}
+
+__global__ void color_extract_kernel(const uint2* __restrict__ rc, uint32_t e, uint32_t* __restrict__ color,
+                                     uint32_t* __restrict__ iota) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < e; k += gridDim.x * blockDim.x) {
+        color[k] = rc[k].y;
+        iota[k] = k;
     }
 }
 
@@ -355,6 +437,26 @@ cudaError_t read_ctl(const uint32_t* ctl, uint32_t* host, cudaStream_t st) {
     return cudaStreamSynchronize(st);
 }
 
+// XPBD_TRACE=1 in the environment: the device coloring synchronises after each phase and prints its host time
+// (and the rounds kernel's own phase times) to stderr. Off, it adds nothing.
+struct PrepTrace {
+    bool on;
+    cudaStream_t st;
+    std::chrono::steady_clock::time_point t;
+    explicit PrepTrace(cudaStream_t s) : st(s), t(std::chrono::steady_clock::now()) {
+        const char* v = getenv("XPBD_TRACE");
+        on = v && *v && *v != '0';
+    }
+    void mark(const char* phase) {
+        if (!on) return;
+        cudaStreamSynchronize(st);
+        const auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "[xpbd] device coloring  %-28s %8.2f ms\n", phase,
+                std::chrono::duration<double, std::milli>(now - t).count());
+        t = now;
+    }
+};
+
 int status_to_error(uint32_t status) {
     if (status & XPBD_DEV_INDEX) return XPBD_ERR_INDEX_RANGE;
     if (status & XPBD_DEV_BARRIER_TIMEOUT) return XPBD_ERR_BARRIER_TIMEOUT;
@@ -392,9 +494,9 @@ extern "C" int xpbd_color_constraints_device(uint32_t n, uint32_t e, const uint3
     uint32_t* ctl = base + L.ctl;
     uint32_t* deg = base + L.deg;
     uint32_t *ka = base + L.ka, *va = base + L.va, *kb = base + L.kb, *vb = base + L.vb;
-    uint32_t* rank = base + L.rank;
-    uint32_t* color = base + L.color;
+    uint2* rc = reinterpret_cast<uint2*>(base + L.rc);
     void* radix = base + L.radix;
+    PrepTrace trace(st);
     uint32_t h[kCtlWords];
     cudaError_t err = cudaSuccess;
 #define PREP_CK(x)                                     \
@@ -409,6 +511,7 @@ extern "C" int xpbd_color_constraints_device(uint32_t n, uint32_t e, const uint3
     PREP_CK(cudaGetLastError());
     PREP_CK(read_ctl(ctl, h, st));
     if (h[kCtlStatus]) return status_to_error(h[kCtlStatus]);
+    trace.mark("degrees");
     // ---- processing rank
     const uint32_t ge = grid_for(e, kPrepBlock);
     if (order == XPBD_ORDER_COLOR_REFERENCE) {
@@ -419,22 +522,24 @@ extern "C" int xpbd_color_constraints_device(uint32_t n, uint32_t e, const uint3
         PREP_CK(radix_sort_pairs(ka, va, kb, vb, e, pn, radix, L.radix_bytes, st, nullptr));
         order_key_kernel<<<ge, kPrepBlock, 0, st>>>(2, ci, cj, deg, h[kCtlMaxDeg], vb, ka, va, e);
         PREP_CK(radix_sort_pairs(ka, va, kb, vb, e, passes_for(h[kCtlMaxDeg]), radix, L.radix_bytes, st, nullptr));
-        rank_kernel<<<ge, kPrepBlock, 0, st>>>(vb, e, rank);
+        rank_kernel<<<ge, kPrepBlock, 0, st>>>(vb, e, rc);
     } else {
-        rank_kernel<<<ge, kPrepBlock, 0, st>>>(nullptr, e, rank);
+        rank_kernel<<<ge, kPrepBlock, 0, st>>>(nullptr, e, rc);
     }
+    trace.mark("processing rank (3 sorts)");
     // ---- particle → constraint adjacency (row order is irrelevant to the coloring)
     PREP_CK(launch_exclusive_scan(deg, n + 1, nullptr, st));
     PREP_CK(cudaMemcpyAsync(base + L.cursor, deg, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     adjacency_kernel<<<ge, kPrepBlock, 0, st>>>(ci, cj, e, base + L.cursor, base + L.adj);
     PREP_CK(cudaGetLastError());
+    trace.mark("adjacency");
     // ---- Jones–Plassmann rounds, one cooperative launch
     int dev = 0, sms = 0, per_sm = 0;
     PREP_CK(cudaGetDevice(&dev));
     PREP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     PREP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jp_color_kernel, kJpBlock, 0));
     if (per_sm < 1) return XPBD_ERR_UNSUPPORTED;
-    JpArgs a{ci, cj, deg, base + L.adj, rank, base + L.pending, color, base + L.front0, base + L.front1, ctl, e};
+    JpArgs a{ci, cj, deg, base + L.adj, rc, base + L.pending, base + L.front0, base + L.front1, ctl, e};
     void* args[] = {&a};
     PREP_CK(cudaLaunchCooperativeKernel((const void*)jp_color_kernel, dim3((unsigned)(sms * per_sm)),
                                         dim3(kJpBlock), args, 0, st));
@@ -442,12 +547,22 @@ extern "C" int xpbd_color_constraints_device(uint32_t n, uint32_t e, const uint3
     if (h[kCtlStatus]) return status_to_error(h[kCtlStatus]);
     if (h[kCtlDone] != e) return XPBD_ERR_INDEX_RANGE;
     const uint32_t ncolors = h[kCtlColors];
+    if (trace.on) {
+        auto span = [&](uint32_t w0, uint32_t w1) {
+            const uint64_t t0 = h[w0] | ((uint64_t)h[w0 + 1] << 32), t1 = h[w1] | ((uint64_t)h[w1 + 1] << 32);
+            return (double)(t1 - t0) * 1e-6;
+        };
+        fprintf(stderr, "[xpbd] device coloring  pending counts %8.2f ms, %u rounds %8.2f ms (%u blocks x %d)\n",
+                span(kCtlT0, kCtlT1), h[kCtlRounds], span(kCtlT1, kCtlT2), (unsigned)(sms * per_sm), kJpBlock);
+    }
+    trace.mark("rounds (one launch)");
     // ---- (color, index) batch order and offsets
-    iota_kernel<<<ge, kPrepBlock, 0, st>>>(va, e);
-    PREP_CK(radix_sort_pairs(color, va, kb, perm, e, passes_for(ncolors - 1), radix, L.radix_bytes, st, nullptr));
+    color_extract_kernel<<<ge, kPrepBlock, 0, st>>>(rc, e, ka, va);
+    PREP_CK(radix_sort_pairs(ka, va, kb, perm, e, passes_for(ncolors - 1), radix, L.radix_bytes, st, nullptr));
     batch_offsets_kernel<<<ge, kPrepBlock, 0, st>>>(kb, e, ncolors, offsets);
-    if (colors) PREP_CK(cudaMemcpyAsync(colors, color, (size_t)e * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    if (colors) PREP_CK(cudaMemcpyAsync(colors, ka, (size_t)e * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     PREP_CK(cudaGetLastError());
+    trace.mark("batch order");
     *batch_count = ncolors;
     return XPBD_OK;
 #undef PREP_CK
