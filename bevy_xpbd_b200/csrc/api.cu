@@ -42,6 +42,7 @@ struct ClothHost {
     std::vector<uint32_t> lambda_gs;   // per input constraint: position in the color-major table
     std::vector<uint32_t> lambda_patch;  // per input constraint: patch slot holding its λ, or UINT32_MAX
     std::vector<uint32_t> inc_i, inc_j;  // per input constraint: incidence in the i / j particle's row (or MAX)
+    std::vector<uint32_t> pal_idx;       // per input constraint: index of its compliance in the cloth's palette
     std::vector<uint32_t> tris;          // render triangles (local vertex indices), for the vertex normals
 };
 
@@ -78,7 +79,8 @@ struct xpbd_ctx {
     bool coop = false;
     uint32_t cl = 0;                 // >0: Gauss–Seidel runs in one cluster of `cl` CTAs
     uint32_t kernel = 0;             // solver kernel id (0 Jacobi tiles, 1 Gauss–Seidel, 2 Jacobi patches)
-    bool patches_ok = false;
+    bool patches_ok = false;         // patch tables built and usable (built on first use by ensure_patches)
+    bool patches_tried = false;
     std::vector<uint4> con_host;     // color-major constraint table (host copy, for the cluster table)
     std::vector<uint32_t> color_off_host;
     ClusterTable ct{};
@@ -392,9 +394,6 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     struct ClothTables {
         std::vector<uint2> inc;         // this cloth's incidences (rows in particle order)
         std::vector<uint32_t> row_off;  // local row starts (n)
-        PatchArrays patches;
-        std::vector<uint32_t> slot;     // sorted constraint → local patch slot
-        bool patches_ok = false;
         bool palette_ok = true;
     };
     std::vector<ClothTables> ct(C);
@@ -409,7 +408,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
         }
         // compliance palette
         std::vector<float> pal;
-        std::vector<uint32_t> pidx(c.e);
+        std::vector<uint32_t>& pidx = c.pal_idx;
+        pidx.assign(c.e, 0);
         for (uint32_t e = 0; e < c.e; ++e) {
             uint32_t bits;
             memcpy(&bits, &c.comp[e], 4);
@@ -437,17 +437,6 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
         }
         std::vector<uint32_t> roff, other, eid;
         neighbor_csr(c.n, c.e, si.data(), sj.data(), roff, other, eid);
-        {  // spatial patches for the shared-memory Jacobi kernel
-            std::vector<float> srest(c.e);
-            std::vector<uint32_t> spal(c.e);
-            for (uint32_t k = 0; k < c.e; ++k) {
-                srest[k] = c.rest[c.perm[k]];
-                spal[k] = pidx[c.perm[k]];
-            }
-            t.patches_ok = build_cloth_patches(c.n, c.rest_pos.data(), c.w.data(), c.e, si.data(), sj.data(),
-                                               srest.data(), spal.data(), roff, other, eid, c.vtx_off, ci_, 256,
-                                               4096, t.patches, t.slot);
-        }
         c.lambda_inc.assign(c.e, 0xFFFFFFFFu);
         c.inc_i.assign(c.e, 0xFFFFFFFFu);
         c.inc_j.assign(c.e, 0xFFFFFFFFu);
@@ -472,26 +461,29 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
             con_in[c.con_off + e] = make_uint4(c.ci[e] + c.vtx_off, c.cj[e] + c.vtx_off, rb, cb);
         }
     });
-    bool patches_ok = true;
-    for (uint32_t ci_ = 0; ci_ < C; ++ci_) {
+    for (uint32_t ci_ = 0; ci_ < C; ++ci_)
         if (!ct[ci_].palette_ok)
             return fail(ctx, XPBD_ERR_UNSUPPORTED, "more than 16 distinct compliance values in one cloth");
-        patches_ok = patches_ok && ct[ci_].patches_ok;
-    }
-    inc.reserve(2 * (size_t)E);
-    PatchArrays patch_arrays;
-    for (uint32_t ci_ = 0; ci_ < C; ++ci_) {
+    // cloth k's incidences start at the total of the cloths before it; each cloth copies and rebases its own slice
+    std::vector<size_t> inc_base(C + 1, 0);
+    for (uint32_t ci_ = 0; ci_ < C; ++ci_) inc_base[ci_ + 1] = inc_base[ci_] + ct[ci_].inc.size();
+    inc.resize(inc_base[C]);
+    parallel_for(C, [&](uint32_t ci_) {
         ClothHost& c = ctx->cloths[ci_];
         ClothTables& t = ct[ci_];
-        const uint32_t base = (uint32_t)inc.size();
+        const uint32_t base = (uint32_t)inc_base[ci_];
         for (uint32_t i = 0; i < c.n; ++i) row_off[c.vtx_off + i] = base + t.row_off[i];
         for (uint32_t e = 0; e < c.e; ++e) {
             if (c.lambda_inc[e] != 0xFFFFFFFFu) c.lambda_inc[e] += base;
             if (c.inc_i[e] != 0xFFFFFFFFu) c.inc_i[e] += base;
             if (c.inc_j[e] != 0xFFFFFFFFu) c.inc_j[e] += base;
         }
-        inc.insert(inc.end(), t.inc.begin(), t.inc.end());
+        std::copy(t.inc.begin(), t.inc.end(), inc.begin() + base);
         std::vector<uint2>().swap(t.inc);
+        c.lambda_patch.assign(c.e, 0xFFFFFFFFu);
+    });
+    for (uint32_t ci_ = 0; ci_ < C; ++ci_) {
+        const ClothHost& c = ctx->cloths[ci_];
         for (uint32_t first = 0; first < c.n; first += 32) {
             XpbdTile tile;
             tile.first = c.vtx_off + first;
@@ -499,49 +491,36 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
             tile.cloth = (uint16_t)ci_;
             tiles.push_back(tile);
         }
-        c.lambda_patch.assign(c.e, 0xFFFFFFFFu);
-        if (patches_ok) {  // append this cloth's patches, rebasing their offsets into the batch arrays
-            PatchArrays& a = patch_arrays;
-            const PatchArrays& b = t.patches;
-            const uint32_t parts0 = (uint32_t)a.parts.size(), con0 = (uint32_t)(a.con.size() / 2),
-                           gofs0 = (uint32_t)a.gofs.size(), slots0 = (uint32_t)a.slots.size();
-            for (size_t h = 0; h < b.header.size(); h += 6) {
-                const uint32_t hd[6] = {b.header[h] + parts0, b.header[h + 1] + con0, b.header[h + 2] + gofs0,
-                                        b.header[h + 3], b.header[h + 4], b.header[h + 5]};
-                a.header.insert(a.header.end(), hd, hd + 6);
-            }
-            a.parts.insert(a.parts.end(), b.parts.begin(), b.parts.end());
-            a.con.insert(a.con.end(), b.con.begin(), b.con.end());
-            for (uint32_t g : b.gofs) a.gofs.push_back(g + slots0);
-            a.slots.insert(a.slots.end(), b.slots.begin(), b.slots.end());
-            a.max_local = std::max(a.max_local, b.max_local);
-            a.max_con = std::max(a.max_con, b.max_con);
-            for (uint32_t k = 0; k < c.e; ++k)
-                if (t.slot[k] != 0xFFFFFFFFu) c.lambda_patch[c.perm[k]] = t.slot[k] + con0;
-        }
-        t.patches = PatchArrays();
     }
     row_off[N] = (uint32_t)inc.size();
-    mark("neighbour tables, patches");
-    // ---- Gauss–Seidel table, color-major across cloths
+    mark("neighbour tables");
+    // ---- Gauss–Seidel table, color-major across cloths: segment (color, cloth) starts after every earlier color
+    // and, within its color, after the earlier cloths; each cloth fills its own segments
     std::vector<uint4> con(E);
     std::vector<uint32_t> color_off(max_colors + 1, 0);
     {
-        uint32_t pos = 0;
-        for (uint32_t col = 0; col < max_colors; ++col) {
-            color_off[col] = pos;
-            for (auto& c : ctx->cloths) {
-                if (col + 1 >= c.batch_off.size()) continue;
-                if (c.lambda_gs.empty()) c.lambda_gs.assign(c.e, 0);
-                for (uint32_t k = c.batch_off[col]; k < c.batch_off[col + 1]; ++k) {
-                    const uint32_t e_in = c.perm[k];
+        std::vector<uint32_t> seg((size_t)max_colors * C + 1, 0);
+        for (uint32_t col = 0; col < max_colors; ++col)
+            for (uint32_t k = 0; k < C; ++k) {
+                const ClothHost& c = ctx->cloths[k];
+                const uint32_t cnt = col + 1 < c.batch_off.size() ? c.batch_off[col + 1] - c.batch_off[col] : 0u;
+                seg[(size_t)col * C + k + 1] = seg[(size_t)col * C + k] + cnt;
+            }
+        for (uint32_t col = 0; col < max_colors; ++col) color_off[col] = seg[(size_t)col * C];
+        color_off[max_colors] = seg[(size_t)max_colors * C];
+        parallel_for(C, [&](uint32_t k) {
+            ClothHost& c = ctx->cloths[k];
+            if (c.lambda_gs.empty()) c.lambda_gs.assign(c.e, 0);
+            for (uint32_t col = 0; col + 1 < c.batch_off.size() && col < max_colors; ++col) {
+                uint32_t pos = seg[(size_t)col * C + k];
+                for (uint32_t q = c.batch_off[col]; q < c.batch_off[col + 1]; ++q) {
+                    const uint32_t e_in = c.perm[q];
                     con[pos] = con_in[c.con_off + e_in];
                     c.lambda_gs[e_in] = pos;
                     ++pos;
                 }
             }
-        }
-        color_off[max_colors] = pos;
+        });
     }
     mark("Gauss-Seidel table");
     // ---- device buffers
@@ -682,68 +661,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
         if (E) H2D(inc_of_con_d, ioc.data(), ioc.size() * 4);
         CK(cudaStreamSynchronize(st), "commit sync");
     }
-    ctx->patches_ok = patches_ok && !patch_arrays.header.empty();
-    if (ctx->patches_ok) {
-        // one contiguous 16-byte aligned blob per patch: parts | con | gofs (patch-relative) | slots
-        const size_t np_ = patch_arrays.header.size() / 6;
-        std::vector<XpbdPatch> ph(np_);
-        std::vector<uint32_t> words;  // blob storage in u32 words (16-byte = 4 words granularity)
-        uint32_t max_blob = 0;
-        auto pad16 = [&]() {
-            while (words.size() % 4) words.push_back(0);
-        };
-        for (size_t k = 0; k < np_; ++k) {
-            const uint32_t* h = &patch_arrays.header[6 * k];
-            const uint32_t parts_off = h[0], con_off = h[1], gofs_off = h[2];
-            const uint32_t npo = h[3] & 0xFFFF, nh = h[3] >> 16, nc = h[4];
-            const size_t start_w = words.size();
-            for (uint32_t t = 0; t < npo + nh; ++t) words.push_back(patch_arrays.parts[parts_off + t]);
-            pad16();
-            for (uint32_t c = 0; c < nc; ++c) {
-                words.push_back(patch_arrays.con[2 * (con_off + c)]);
-                words.push_back(patch_arrays.con[2 * (con_off + c) + 1]);
-            }
-            pad16();
-            const uint32_t s0 = patch_arrays.gofs[gofs_off], s1 = patch_arrays.gofs[gofs_off + npo];
-            for (uint32_t t = 0; t <= npo; ++t) words.push_back(patch_arrays.gofs[gofs_off + t] - s0);
-            pad16();
-            for (uint32_t q = s0; q < s1; q += 2) {
-                const uint32_t lo = patch_arrays.slots[q];
-                const uint32_t hi = (q + 1 < s1) ? patch_arrays.slots[q + 1] : 0u;
-                words.push_back(lo | (hi << 16));
-            }
-            pad16();
-            const uint32_t bytes = (uint32_t)((words.size() - start_w) * 4);
-            ph[k].off16 = (uint32_t)(start_w / 4);
-            ph[k].bytes = bytes;
-            ph[k].nc = nc;
-            ph[k].lam_off = con_off;
-            ph[k].np = (uint16_t)npo;
-            ph[k].nh = (uint16_t)nh;
-            ph[k].cloth = (uint16_t)h[5];
-            ph[k].pad = 0;
-            max_blob = std::max(max_blob, bytes);
-        }
-        XpbdPatch* d_ph;
-        uint4* d_blob;
-        float* d_plam;
-        const size_t ncon = patch_arrays.con.size() / 2;
-        ALLOC(d_ph, XpbdPatch, np_);
-        ALLOC(d_blob, uint4, words.size() / 4);
-        ALLOC(d_plam, float, ncon);
-        H2D(d_ph, ph.data(), np_ * sizeof(XpbdPatch));
-        H2D(d_blob, words.data(), words.size() * 4);
-        CK(cudaMemsetAsync(d_plam, 0, std::max<size_t>(ncon, 1) * 4, st), "memset");
-        CK(cudaStreamSynchronize(st), "commit sync");
-        W.n_patches = (uint32_t)np_;
-        W.patch_max_local = patch_arrays.max_local;
-        W.patch_max_con = std::max<uint32_t>(patch_arrays.max_con, 1);
-        W.patch_con_total = (uint32_t)ncon;
-        W.patch_max_blob = max_blob;
-        W.patches = d_ph;
-        W.patch_blob = d_blob;
-        W.patch_lambda = d_plam;
-    }
+    ctx->patches_ok = false;  // the spatial-patch tables are built on first use (ensure_patches)
+    ctx->patches_tried = false;
     CK(cudaMemsetAsync(sync, 0, sizeof(XpbdGridSync), st), "memset");
     CK(cudaStreamSynchronize(st), "commit sync");
     W.x = x;
@@ -860,6 +779,128 @@ static bool build_cluster_table(xpbd_ctx* ctx, uint32_t cl) {
     return true;
 }
 
+// Spatial patches for the shared-memory Jacobi kernel (jacobi_kernel 2), built on first use rather than in
+// xpbd_commit: only that kernel reads them, and for large batches they are the costliest host table. Per cloth on
+// parallel host threads, then concatenated in cloth order into one contiguous 16-byte aligned blob per patch
+// (parts | con | gofs (patch-relative) | slots). Returns false when a cloth cannot be split into patches (the
+// schedule then keeps the thread-per-particle kernel); allocation failures are errors.
+static int ensure_patches(xpbd_ctx* ctx, bool* usable) {
+    *usable = ctx->patches_ok;
+    if (ctx->patches_ok || ctx->patches_tried) return XPBD_OK;
+    ctx->patches_tried = true;
+    const uint32_t C = (uint32_t)ctx->cloths.size();
+    std::vector<PatchArrays> per(C);
+    std::vector<std::vector<uint32_t>> slot(C);
+    std::vector<char> ok(C, 0);
+    parallel_for(C, [&](uint32_t k) {
+        ClothHost& c = ctx->cloths[k];
+        std::vector<uint32_t> si(c.e), sj(c.e), spal(c.e);
+        std::vector<float> srest(c.e);
+        for (uint32_t q = 0; q < c.e; ++q) {
+            si[q] = c.ci[c.perm[q]];
+            sj[q] = c.cj[c.perm[q]];
+            srest[q] = c.rest[c.perm[q]];
+            spal[q] = c.pal_idx[c.perm[q]];
+        }
+        std::vector<uint32_t> roff, other, eid;
+        neighbor_csr(c.n, c.e, si.data(), sj.data(), roff, other, eid);
+        ok[k] = build_cloth_patches(c.n, c.rest_pos.data(), c.w.data(), c.e, si.data(), sj.data(), srest.data(),
+                                    spal.data(), roff, other, eid, c.vtx_off, k, 256, 4096, per[k], slot[k]);
+    });
+    for (uint32_t k = 0; k < C; ++k)
+        if (!ok[k]) return XPBD_OK;
+    PatchArrays patch_arrays;
+    std::vector<std::vector<uint32_t>> lambda_patch(C);
+    for (uint32_t k = 0; k < C; ++k) {  // append, rebasing offsets into the batch arrays
+        const ClothHost& c = ctx->cloths[k];
+        PatchArrays& a = patch_arrays;
+        const PatchArrays& b = per[k];
+        const uint32_t parts0 = (uint32_t)a.parts.size(), con0 = (uint32_t)(a.con.size() / 2),
+                       gofs0 = (uint32_t)a.gofs.size(), slots0 = (uint32_t)a.slots.size();
+        for (size_t h = 0; h < b.header.size(); h += 6) {
+            const uint32_t hd[6] = {b.header[h] + parts0, b.header[h + 1] + con0, b.header[h + 2] + gofs0,
+                                    b.header[h + 3], b.header[h + 4], b.header[h + 5]};
+            a.header.insert(a.header.end(), hd, hd + 6);
+        }
+        a.parts.insert(a.parts.end(), b.parts.begin(), b.parts.end());
+        a.con.insert(a.con.end(), b.con.begin(), b.con.end());
+        for (uint32_t g : b.gofs) a.gofs.push_back(g + slots0);
+        a.slots.insert(a.slots.end(), b.slots.begin(), b.slots.end());
+        a.max_local = std::max(a.max_local, b.max_local);
+        a.max_con = std::max(a.max_con, b.max_con);
+        lambda_patch[k].assign(c.e, 0xFFFFFFFFu);
+        for (uint32_t q = 0; q < c.e; ++q)
+            if (slot[k][q] != 0xFFFFFFFFu) lambda_patch[k][c.perm[q]] = slot[k][q] + con0;
+        per[k] = PatchArrays();
+    }
+    if (patch_arrays.header.empty()) return XPBD_OK;
+    const size_t np_ = patch_arrays.header.size() / 6;
+    std::vector<XpbdPatch> ph(np_);
+    std::vector<uint32_t> words;  // blob storage in u32 words (16-byte = 4 words granularity)
+    uint32_t max_blob = 0;
+    auto pad16 = [&]() {
+        while (words.size() % 4) words.push_back(0);
+    };
+    for (size_t k = 0; k < np_; ++k) {
+        const uint32_t* h = &patch_arrays.header[6 * k];
+        const uint32_t parts_off = h[0], con_off = h[1], gofs_off = h[2];
+        const uint32_t npo = h[3] & 0xFFFF, nh = h[3] >> 16, nc = h[4];
+        const size_t start_w = words.size();
+        for (uint32_t t = 0; t < npo + nh; ++t) words.push_back(patch_arrays.parts[parts_off + t]);
+        pad16();
+        for (uint32_t c = 0; c < nc; ++c) {
+            words.push_back(patch_arrays.con[2 * (con_off + c)]);
+            words.push_back(patch_arrays.con[2 * (con_off + c) + 1]);
+        }
+        pad16();
+        const uint32_t s0 = patch_arrays.gofs[gofs_off], s1 = patch_arrays.gofs[gofs_off + npo];
+        for (uint32_t t = 0; t <= npo; ++t) words.push_back(patch_arrays.gofs[gofs_off + t] - s0);
+        pad16();
+        for (uint32_t q = s0; q < s1; q += 2) {
+            const uint32_t lo = patch_arrays.slots[q];
+            const uint32_t hi = (q + 1 < s1) ? patch_arrays.slots[q + 1] : 0u;
+            words.push_back(lo | (hi << 16));
+        }
+        pad16();
+        const uint32_t bytes = (uint32_t)((words.size() - start_w) * 4);
+        ph[k].off16 = (uint32_t)(start_w / 4);
+        ph[k].bytes = bytes;
+        ph[k].nc = nc;
+        ph[k].lam_off = con_off;
+        ph[k].np = (uint16_t)npo;
+        ph[k].nh = (uint16_t)nh;
+        ph[k].cloth = (uint16_t)h[5];
+        ph[k].pad = 0;
+        max_blob = std::max(max_blob, bytes);
+    }
+    const size_t ncon = patch_arrays.con.size() / 2;
+    cudaError_t err = cudaSuccess;
+    XpbdPatch* d_ph = dev_alloc<XpbdPatch>(ctx, np_, &err);
+    if (err != cudaSuccess) return cuda_fail(ctx, err, "cudaMalloc (patches)");
+    uint4* d_blob = dev_alloc<uint4>(ctx, words.size() / 4, &err);
+    if (err != cudaSuccess) return cuda_fail(ctx, err, "cudaMalloc (patches)");
+    float* d_plam = dev_alloc<float>(ctx, ncon, &err);
+    if (err != cudaSuccess) return cuda_fail(ctx, err, "cudaMalloc (patches)");
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(d_ph, ph.data(), np_ * sizeof(XpbdPatch), cudaMemcpyHostToDevice, st), "upload");
+    CK(cudaMemcpyAsync(d_blob, words.data(), words.size() * 4, cudaMemcpyHostToDevice, st), "upload");
+    CK(cudaMemsetAsync(d_plam, 0, std::max<size_t>(ncon, 1) * 4, st), "memset");
+    CK(cudaStreamSynchronize(st), "patch upload");
+    XpbdWorld& W = ctx->W;
+    W.n_patches = (uint32_t)np_;
+    W.patch_max_local = patch_arrays.max_local;
+    W.patch_max_con = std::max<uint32_t>(patch_arrays.max_con, 1);
+    W.patch_con_total = (uint32_t)ncon;
+    W.patch_max_blob = max_blob;
+    W.patches = d_ph;
+    W.patch_blob = d_blob;
+    W.patch_lambda = d_plam;
+    for (uint32_t k = 0; k < C; ++k) ctx->cloths[k].lambda_patch.swap(lambda_patch[k]);
+    ctx->patches_ok = true;
+    *usable = true;
+    return XPBD_OK;
+}
+
 // Cluster path: Gauss–Seidel, λ cleared per iteration, every particle fits in the cluster's shared memory.
 static uint32_t pick_cluster(xpbd_ctx* ctx, uint32_t want, uint32_t block) {
     if (ctx->opts.solver != XPBD_SOLVER_GAUSS_SEIDEL || ctx->opts.lambda_mode != XPBD_LAMBDA_RESET_PER_ITERATION)
@@ -874,6 +915,15 @@ static uint32_t pick_cluster(xpbd_ctx* ctx, uint32_t want, uint32_t block) {
         cudaGetLastError();
     }
     return 0;
+}
+
+// Spatial patches for jacobi_kernel 2, built now if needed; false if they cannot be used (the schedule then runs the
+// thread-per-particle kernel and the reason is kept in last_error).
+static bool patches_usable(xpbd_ctx* ctx) {
+    bool usable = false;
+    if (ensure_patches(ctx, &usable) != XPBD_OK) return false;
+    if (!usable) ctx->last_error = "spatial patches unavailable for this batch: thread-per-particle Jacobi used";
+    return usable;
 }
 
 static void choose_schedule(xpbd_ctx* ctx) {
@@ -898,10 +948,10 @@ static void choose_schedule(xpbd_ctx* ctx) {
         ctx->kernel = 1;
     else if (ctx->opts.jacobi_kernel == 1)
         ctx->kernel = 0;
-    else if (ctx->opts.jacobi_kernel == 3)
-        ctx->kernel = 5;
+    else if (ctx->opts.jacobi_kernel == 2 && patches_usable(ctx))
+        ctx->kernel = 2;
     else
-        ctx->kernel = 5;  // thread per particle: measured fastest on the sheets and batches benchmarked
+        ctx->kernel = 5;  // thread per particle (default): measured fastest on the sheets and batches benchmarked
     int maxb = max_blocks_per_sm(ctx->kernel, block, ctx->W);
     if (maxb < 1) maxb = 1;
     int bps = ctx->opts.blocks_per_sm ? (int)ctx->opts.blocks_per_sm : maxb;
@@ -1476,7 +1526,7 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
     const uint32_t jks[3] = {2, 3, 1};
     for (uint32_t jk : jks) {
         if (base.solver != XPBD_SOLVER_JACOBI && jk != 1) continue;
-        if (jk == 2 && !ctx->patches_ok) continue;
+        if (jk == 2 && !ctx->patches_ok) continue;  // tried only when the caller already built the patches
         const uint32_t kid = base.solver == XPBD_SOLVER_JACOBI ? (jk == 2 ? 2u : (jk == 3 ? 5u : 0u)) : 1u;
         for (uint32_t blk : blocks) {
             int maxb = max_blocks_per_sm(kid, blk, ctx->W);

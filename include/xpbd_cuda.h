@@ -103,7 +103,9 @@ typedef struct xpbd_solver_opts {
     uint32_t blocks_per_sm;           /* 0 = autotuned / default */
     uint32_t warm_start;              /* convergence solve start: XPBD_WARM_* (0 = plain, λ = 0) */
     uint32_t cluster_ctas;            /* Gauss–Seidel in one thread-block cluster: 0 auto, 1 off, 8 or 16 CTAs */
-    uint32_t jacobi_kernel;           /* Jacobi: 0 default (= 3), 1 warp tiles, 2 shared-memory patches, 3 thread per particle */
+    uint32_t jacobi_kernel;           /* Jacobi: 0 default (= 3), 1 warp tiles, 2 shared-memory patches (their tables
+                                         are built by the first call that selects them; xpbd_autotune tries them only
+                                         once built), 3 thread per particle */
     float tolerance;                  /* > 0 (or warm_start != 0): convergence solve — Jacobi, λ kept per substep,
                                          iterate until max |C + α̃λ|/rest <= tolerance, at most inner_iterations */
     uint32_t reserved[3];

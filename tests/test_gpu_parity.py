@@ -386,6 +386,8 @@ def test_jacobi_execution_paths_bit_exact(kernel, lam):
                jacobi_kernel=kernel)
     plug = gpu_sim(specs, prm, cfg)
     plug.step(frames=6)
+    # the requested execution ran: kernel ids 0 warp tiles, 2 spatial patches, 5 thread per particle
+    assert plug.stats()["solver_kernel"] == {1: 0, 2: 2, 3: 5}[kernel]
     for k, sp in enumerate(specs):
         o = oracle_sim(sp, prm, cfg)
         o.substeps(60)
