@@ -132,8 +132,8 @@ def load():
         "xpbd_debug_force_barrier_timeout": (I, [P, C.c_float]),
         "xpbd_color_constraints": (I, [U, U, P, P, U, P, P, C.POINTER(U)]),
         "xpbd_radix_sort_pairs_noalloc": (I, [P, P, P, P, U, U, P]),
-        "xpbd_color_constraints_device_scratch_bytes": (C.c_size_t, [U, U]),
-        "xpbd_color_constraints_device": (I, [U, U, P, P, U, P, P, P, C.POINTER(U), P, C.c_size_t, P]),
+        "xpbd_color_constraints_device_scratch_bytes": (C.c_size_t, [U, U, U]),
+        "xpbd_color_constraints_device": (I, [U, U, P, P, U, U, P, P, P, P, C.POINTER(U), P, C.c_size_t, P]),
         "xpbd_neighbor_table_device_scratch_bytes": (C.c_size_t, [U, U]),
         "xpbd_neighbor_table_device": (I, [U, U, P, P, P, P, P, P, C.c_size_t, P]),
         "xpbd_set_warm_lambda": (I, [P, U, P]),

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <vector>
 #include <cstdio>
 #include <cstdlib>
 
@@ -52,13 +53,15 @@ enum : uint32_t {
     kCtlT0 = 10,     // globaltimer stamps (two words each): kernel start, end of phase 0, end of the rounds
     kCtlT1 = 12,
     kCtlT2 = 14,
+    kCtlQueue = 16,    // per-cloth schedule: next entry of the cloth queue
     kCtlBarrier = 32,  // in its own 128-byte line, apart from the frontier counters
     kCtlWords = 64,    // 256 bytes
 };
 constexpr uint32_t kStatusSchedule = 0x100u;  // a constraint was reached before an earlier-ranked neighbour
+constexpr uint32_t kStatusCloth = 0x200u;     // per-cloth schedule: two cloths share a particle
 
 struct ColorLayout {  // offsets in 32-bit words from the scratch base; every array starts on 256 bytes
-    size_t ctl, deg, cursor, adj, ka, va, kb, vb, rc, pending, front0, front1, radix;
+    size_t ctl, deg, cursor, adj, ka, va, kb, vb, rc, pending, front0, front1, coff, queue, radix;
     size_t radix_bytes, total_bytes;
 };
 
@@ -68,7 +71,7 @@ size_t take_words(size_t& off, size_t words) {
     return o;
 }
 
-ColorLayout color_layout(uint32_t n, uint32_t e) {
+ColorLayout color_layout(uint32_t n, uint32_t e, uint32_t num_cloths) {
     ColorLayout L{};
     size_t off = 0;
     L.ctl = take_words(off, kCtlWords);
@@ -83,6 +86,8 @@ ColorLayout color_layout(uint32_t n, uint32_t e) {
     L.pending = take_words(off, e);
     L.front0 = take_words(off, e);
     L.front1 = take_words(off, e);
+    L.coff = take_words(off, (size_t)num_cloths + 1);
+    L.queue = take_words(off, num_cloths);
     L.radix = off;
     L.radix_bytes = radix_sort_scratch_bytes(std::max<uint32_t>(e, 1u));
     L.total_bytes = off * 4 + L.radix_bytes;
@@ -228,6 +233,7 @@ struct JpArgs {
 
 constexpr uint32_t kGroup = 8;       // lanes per frontier constraint (4 constraints per warp)
 constexpr uint32_t kGroupSlots = 4;  // neighbour slots per lane kept in registers (degree sums up to 32)
+constexpr uint32_t kPerWarp = 32u / kGroup;
 
 // Neighbour slot t of constraint k: row of its i endpoint first, then row of its j endpoint.
 __device__ __forceinline__ uint32_t slot_at(const JpArgs& a, uint32_t t, uint32_t b0, uint32_t l0, uint32_t b1) {
@@ -251,6 +257,113 @@ __device__ __forceinline__ void stamp(uint32_t* ctl, uint32_t word) {
     ctl[word + 1] = (uint32_t)(t >> 32);
 }
 
+// Loads and stores of the state that changes during a launch (frontiers, colors): across the CTAs of a grid they go
+// to L2 (ld.cg / st.cg: another SM's L1 may hold a stale line); inside one CTA, __syncthreads orders them and the
+// SM's own L1 is coherent for its threads, so plain accesses serve.
+template <bool GRID, typename T>
+__device__ __forceinline__ T ld_shared_state(const T* p) {
+    if constexpr (GRID) return __ldcg(p);
+    else return *p;
+}
+template <bool GRID>
+__device__ __forceinline__ void st_shared_state(uint32_t* p, uint32_t v) {
+    if constexpr (GRID) __stcg(p, v);
+    else *p = v;
+}
+
+// One step of a round for one warp: colors the frontier entries first .. first + 3 of `cur` (one per 8-lane group;
+// entries at or beyond `size` are idle) and appends the later-ranked neighbours that become ready to `nxt`, counting
+// them in *ncount (global or shared memory). Warp-collective: every lane calls it with the same first and size.
+template <bool GRID>
+__device__ __forceinline__ void jp_color_group(const JpArgs& a, const uint32_t* cur, uint32_t first, uint32_t size,
+                                               uint32_t* nxt, uint32_t* ncount, uint32_t lane, uint32_t& max_color) {
+    const uint32_t sub = lane & (kGroup - 1u);
+    const uint32_t item = first + lane / kGroup;
+    const bool valid = item < size;
+    uint32_t k = 0, r = 0, b0 = 0, l0 = 0, b1 = 0, len = 0;
+    if (valid) {
+        k = ld_shared_state<GRID>(&cur[item]);
+        r = ld_shared_state<GRID>(&a.rc[k].x);
+        const uint32_t p0 = __ldg(&a.ci[k]), p1 = __ldg(&a.cj[k]);
+        b0 = __ldg(&a.row_off[p0]);
+        l0 = __ldg(&a.row_off[p0 + 1]) - b0;
+        b1 = __ldg(&a.row_off[p1]);
+        len = l0 + (__ldg(&a.row_off[p1 + 1]) - b1);
+    }
+    // colors of the earlier-ranked neighbours, first 64-color window
+    uint32_t fs[kGroupSlots], rs[kGroupSlots];
+    unsigned long long m = 0;
+    bool missing = false;
+#pragma unroll
+    for (uint32_t j = 0; j < kGroupSlots; ++j) {
+        const uint32_t t = sub + kGroup * j;
+        fs[j] = kNoColor;
+        rs[j] = 0;
+        if (t < len) {
+            const uint32_t f = slot_at(a, t, b0, l0, b1);
+            const uint2 v = ld_shared_state<GRID>(&a.rc[f]);
+            fs[j] = f;
+            rs[j] = v.x;
+            if (f != k && v.x < r) {
+                if (v.y == kNoColor) missing = true;
+                else if (v.y < 64u) m |= 1ull << v.y;
+            }
+        }
+    }
+    for (uint32_t t = sub + kGroup * kGroupSlots; t < len; t += kGroup) {
+        const uint32_t f = slot_at(a, t, b0, l0, b1);
+        const uint2 v = ld_shared_state<GRID>(&a.rc[f]);
+        if (f != k && v.x < r) {
+            if (v.y == kNoColor) missing = true;
+            else if (v.y < 64u) m |= 1ull << v.y;
+        }
+    }
+    m = group_or(m);
+    bool need = valid && m == ~0ull;
+    uint32_t col = (valid && !need) ? (uint32_t)__ffsll((long long)~m) - 1u : 0u;
+    for (uint32_t base = 64u; __any_sync(kMask, need); base += 64u) {  // rare: 64 colors taken
+        unsigned long long w = 0;
+        if (need) {
+            for (uint32_t t = sub; t < len; t += kGroup) {
+                const uint32_t f = slot_at(a, t, b0, l0, b1);
+                const uint2 v = ld_shared_state<GRID>(&a.rc[f]);
+                if (f != k && v.x < r && v.y != kNoColor && v.y - base < 64u) w |= 1ull << (v.y - base);
+            }
+        }
+        w = group_or(w);
+        if (need && w != ~0ull) {
+            col = base + (uint32_t)__ffsll((long long)~w) - 1u;
+            need = false;
+        }
+    }
+    if (missing) atomicOr(&a.ctl[kCtlStatus], kStatusSchedule);
+    if (valid && sub == 0) {
+        st_shared_state<GRID>(&a.rc[k].y, col);
+        max_color = max(max_color, col + 1u);
+    }
+    // release the later-ranked neighbours; the ones that become ready join the next frontier with one
+    // counter atomic per warp and slot
+#pragma unroll
+    for (uint32_t j = 0; j < kGroupSlots; ++j) {
+        const uint32_t f = fs[j];
+        const bool push = valid && f != kNoColor && f != k && rs[j] > r && atomicSub(&a.pending[f], 1u) == 1u;
+        const unsigned ballot = __ballot_sync(kMask, push);
+        if (ballot) {
+            const uint32_t leader = (uint32_t)__ffs(ballot) - 1u;
+            uint32_t at = 0;
+            if (lane == leader) at = atomicAdd(ncount, (uint32_t)__popc(ballot));
+            at = __shfl_sync(kMask, at, leader);
+            if (push) st_shared_state<GRID>(&nxt[at + (uint32_t)__popc(ballot & ((1u << lane) - 1u))], f);
+        }
+    }
+    if (!valid) return;
+    for (uint32_t t = sub + kGroup * kGroupSlots; t < len; t += kGroup) {
+        const uint32_t f = slot_at(a, t, b0, l0, b1);
+        if (f != k && ld_shared_state<GRID>(&a.rc[f].x) > r && atomicSub(&a.pending[f], 1u) == 1u)
+            st_shared_state<GRID>(&nxt[atomicAdd(ncount, 1u)], f);
+    }
+}
+
 __global__ void __launch_bounds__(kJpBlock) jp_color_kernel(JpArgs a) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
     if (tid == 0) stamp(a.ctl, kCtlT0);
@@ -272,8 +385,7 @@ __global__ void __launch_bounds__(kJpBlock) jp_color_kernel(JpArgs a) {
     }
     if (!prep_grid_barrier(a.ctl)) return;
     if (tid == 0) stamp(a.ctl, kCtlT1);
-    const uint32_t lane = threadIdx.x & 31u, sub = lane & (kGroup - 1u), gw = tid >> 5, nw = nthr >> 5;
-    constexpr uint32_t kPerWarp = 32u / kGroup;
+    const uint32_t lane = threadIdx.x & 31u, gw = tid >> 5, nw = nthr >> 5;
     uint32_t max_color = 0;  // largest color + 1 this thread wrote
     for (uint32_t round = 0;; ++round) {
         const uint32_t size = __ldcg(&a.ctl[kCtlCount0 + round % 3]);
@@ -292,97 +404,90 @@ __global__ void __launch_bounds__(kJpBlock) jp_color_kernel(JpArgs a) {
         const uint32_t* cur = (round & 1u) ? a.front1 : a.front0;
         uint32_t* nxt = (round & 1u) ? a.front0 : a.front1;
         uint32_t* ncount = &a.ctl[kCtlCount0 + (round + 1) % 3];
-        for (uint32_t first = gw * kPerWarp; first < size; first += nw * kPerWarp) {  // warp-uniform loop
-            const uint32_t item = first + lane / kGroup;
-            const bool valid = item < size;
-            uint32_t k = 0, r = 0, b0 = 0, l0 = 0, b1 = 0, len = 0;
-            if (valid) {
-                k = __ldcg(&cur[item]);
-                r = __ldcg(&a.rc[k].x);
-                const uint32_t p0 = __ldg(&a.ci[k]), p1 = __ldg(&a.cj[k]);
-                b0 = __ldg(&a.row_off[p0]);
-                l0 = __ldg(&a.row_off[p0 + 1]) - b0;
-                b1 = __ldg(&a.row_off[p1]);
-                len = l0 + (__ldg(&a.row_off[p1 + 1]) - b1);
-            }
-            // colors of the earlier-ranked neighbours, first 64-color window
-            uint32_t fs[kGroupSlots], rs[kGroupSlots];
-            unsigned long long m = 0;
-            bool missing = false;
-#pragma unroll
-            for (uint32_t j = 0; j < kGroupSlots; ++j) {
-                const uint32_t t = sub + kGroup * j;
-                fs[j] = kNoColor;
-                rs[j] = 0;
-                if (t < len) {
-                    const uint32_t f = slot_at(a, t, b0, l0, b1);
-                    const uint2 v = __ldcg(&a.rc[f]);
-                    fs[j] = f;
-                    rs[j] = v.x;
-                    if (f != k && v.x < r) {
-                        if (v.y == kNoColor) missing = true;
-                        else if (v.y < 64u) m |= 1ull << v.y;
-                    }
-                }
-            }
-            for (uint32_t t = sub + kGroup * kGroupSlots; t < len; t += kGroup) {
-                const uint32_t f = slot_at(a, t, b0, l0, b1);
-                const uint2 v = __ldcg(&a.rc[f]);
-                if (f != k && v.x < r) {
-                    if (v.y == kNoColor) missing = true;
-                    else if (v.y < 64u) m |= 1ull << v.y;
-                }
-            }
-            m = group_or(m);
-            bool need = valid && m == ~0ull;
-            uint32_t col = (valid && !need) ? (uint32_t)__ffsll((long long)~m) - 1u : 0u;
-            for (uint32_t base = 64u; __any_sync(kMask, need); base += 64u) {  // rare: 64 colors taken
-                unsigned long long w = 0;
-                if (need) {
-                    for (uint32_t t = sub; t < len; t += kGroup) {
-                        const uint32_t f = slot_at(a, t, b0, l0, b1);
-                        const uint2 v = __ldcg(&a.rc[f]);
-                        if (f != k && v.x < r && v.y != kNoColor && v.y - base < 64u) w |= 1ull << (v.y - base);
-                    }
-                }
-                w = group_or(w);
-                if (need && w != ~0ull) {
-                    col = base + (uint32_t)__ffsll((long long)~w) - 1u;
-                    need = false;
-                }
-            }
-            if (missing) atomicOr(&a.ctl[kCtlStatus], kStatusSchedule);
-            if (valid && sub == 0) {
-                __stcg(&a.rc[k].y, col);
-                max_color = max(max_color, col + 1u);
-            }
-            // release the later-ranked neighbours; the ones that become ready join the next frontier with one
-            // counter atomic per warp and slot
-#pragma unroll
-            for (uint32_t j = 0; j < kGroupSlots; ++j) {
-                const uint32_t f = fs[j];
-                const bool push = valid && f != kNoColor && f != k && rs[j] > r && atomicSub(&a.pending[f], 1u) == 1u;
-                const unsigned ballot = __ballot_sync(kMask, push);
-                if (ballot) {
-                    const uint32_t leader = (uint32_t)__ffs(ballot) - 1u;
-                    uint32_t at = 0;
-                    if (lane == leader) at = atomicAdd(ncount, (uint32_t)__popc(ballot));
-                    at = __shfl_sync(kMask, at, leader);
-                    if (push) __stcg(&nxt[at + (uint32_t)__popc(ballot & ((1u << lane) - 1u))], f);
-                }
-            }
-            if (!valid) continue;
-            for (uint32_t t = sub + kGroup * kGroupSlots; t < len; t += kGroup) {
-                const uint32_t f = slot_at(a, t, b0, l0, b1);
-                if (f != k && __ldcg(&a.rc[f].x) > r && atomicSub(&a.pending[f], 1u) == 1u)
-                    __stcg(&nxt[atomicAdd(ncount, 1u)], f);
-            }
-        }
+        for (uint32_t first = gw * kPerWarp; first < size; first += nw * kPerWarp)  // warp-uniform loop
+            jp_color_group<true>(a, cur, first, size, nxt, ncount, lane, max_color);
         if (!prep_grid_barrier(a.ctl)) return;
     }
     max_color = __reduce_max_sync(kMask, max_color);
     if (lane == 0 && max_color) atomicMax(&a.ctl[kCtlColors], max_color);
     if (tid == 0) stamp(a.ctl, kCtlT2);
+}
+
+// Per-cloth schedule, for batches whose cloths (contiguous constraint ranges) share no particle: one CTA colors one
+// cloth at a time, taking cloths from a queue (largest first), with the frontier counters in shared memory and
+// __syncthreads between rounds instead of a grid barrier — a round costs the CTA's own dependent accesses only, and
+// no CTA ever waits for another.
+__global__ void __launch_bounds__(kJpBlock) jp_cloth_kernel(JpArgs a, const uint32_t* __restrict__ coff,
+                                                             const uint32_t* __restrict__ queue,
+                                                             uint32_t num_cloths) {
+    __shared__ uint32_t s_cnt[3];
+    __shared__ uint32_t s_cloth;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31u, wid = tid >> 5, nw = nthr >> 5;
+    if (blockIdx.x == 0 && tid == 0) {
+        stamp(a.ctl, kCtlT0);
+        stamp(a.ctl, kCtlT1);
+    }
+    uint32_t max_color = 0;
+    for (;;) {
+        if (tid == 0) s_cloth = atomicAdd(&a.ctl[kCtlQueue], 1u);
+        if (tid < 3) s_cnt[tid] = 0;
+        __syncthreads();
+        const uint32_t qi = s_cloth;
+        if (qi >= num_cloths) break;
+        const uint32_t cl = queue[qi], c0 = coff[cl], c1 = coff[cl + 1];
+        uint32_t* f0 = a.front0 + c0;
+        uint32_t* f1 = a.front1 + c0;
+        // pending counts and the first frontier; every neighbour must belong to this cloth
+        bool foreign = false;
+        for (uint32_t k = c0 + tid; k < c1; k += nthr) {
+            const uint32_t r = a.rc[k].x;
+            const uint32_t p0 = __ldg(&a.ci[k]), p1 = __ldg(&a.cj[k]);
+            uint32_t cnt = 0;
+            for (uint32_t q = __ldg(&a.row_off[p0]), q1 = __ldg(&a.row_off[p0 + 1]); q < q1; ++q) {
+                const uint32_t f = __ldg(&a.adj[q]);
+                foreign |= f < c0 || f >= c1;
+                cnt += (f != k && a.rc[f].x < r) ? 1u : 0u;
+            }
+            for (uint32_t q = __ldg(&a.row_off[p1]), q1 = __ldg(&a.row_off[p1 + 1]); q < q1; ++q) {
+                const uint32_t f = __ldg(&a.adj[q]);
+                foreign |= f < c0 || f >= c1;
+                cnt += (f != k && a.rc[f].x < r) ? 1u : 0u;
+            }
+            a.pending[k] = cnt;
+            if (cnt == 0) f0[atomicAdd(&s_cnt[0], 1u)] = k;
+        }
+        // a cloth sharing a particle with another is not colored (its rounds could release the other cloth's
+        // constraints into this cloth's frontier range); adjacency is symmetric, so the other cloth stops too
+        if (__syncthreads_or(foreign)) {
+            if (tid == 0) atomicOr(&a.ctl[kCtlStatus], kStatusCloth);
+            continue;
+        }
+        uint32_t round = 0;
+        for (;; ++round) {
+            const uint32_t size = s_cnt[round % 3];
+            if (size == 0) break;
+            if (round > c1 - c0) {  // every round colors at least one constraint: never taken; bounds the loop
+                if (tid == 0) atomicOr(&a.ctl[kCtlStatus], kStatusSchedule);
+                break;
+            }
+            // word (round + 2) % 3 held the size of round - 1, read before the last __syncthreads; it counts the
+            // frontier of round + 2, first incremented in round + 1
+            if (tid == 0) {
+                s_cnt[(round + 2) % 3] = 0;
+                atomicAdd(&a.ctl[kCtlDone], size);
+            }
+            const uint32_t* cur = (round & 1u) ? f1 : f0;
+            uint32_t* nxt = (round & 1u) ? f0 : f1;
+            for (uint32_t first = wid * kPerWarp; first < size; first += nw * kPerWarp)  // warp-uniform loop
+                jp_color_group<false>(a, cur, first, size, nxt, &s_cnt[(round + 1) % 3], lane, max_color);
+            __syncthreads();
+        }
+        if (tid == 0) atomicMax(&a.ctl[kCtlRounds], round);
+        __syncthreads();  // s_cnt and s_cloth are rewritten for the next cloth
+    }
+    max_color = __reduce_max_sync(kMask, max_color);
+    if (lane == 0 && max_color) atomicMax(&a.ctl[kCtlColors], max_color);
+    if (tid == 0) atomicMax(reinterpret_cast<unsigned long long*>(&a.ctl[kCtlT2]), globaltimer_ns());
 }
 
 // rc[k] = {rank, no color}: rank[order[k]] = k (order == nullptr: index order).
@@ -460,6 +565,7 @@ struct PrepTrace {
 int status_to_error(uint32_t status) {
     if (status & XPBD_DEV_INDEX) return XPBD_ERR_INDEX_RANGE;
     if (status & XPBD_DEV_BARRIER_TIMEOUT) return XPBD_ERR_BARRIER_TIMEOUT;
+    if (status & kStatusCloth) return XPBD_ERR_INVALID_ARGUMENT;
     return status ? XPBD_ERR_STATE : XPBD_OK;
 }
 
@@ -468,17 +574,25 @@ int status_to_error(uint32_t status) {
 
 using namespace xpbd;
 
-extern "C" size_t xpbd_color_constraints_device_scratch_bytes(uint32_t num_particles, uint32_t num_constraints) {
-    return color_layout(num_particles, num_constraints).total_bytes;
+extern "C" size_t xpbd_color_constraints_device_scratch_bytes(uint32_t num_particles, uint32_t num_constraints,
+                                                              uint32_t num_cloths) {
+    return color_layout(num_particles, num_constraints, num_cloths).total_bytes;
 }
 
 extern "C" int xpbd_color_constraints_device(uint32_t n, uint32_t e, const uint32_t* ci, const uint32_t* cj,
-                                             uint32_t order, uint32_t* perm, uint32_t* colors, uint32_t* offsets,
-                                             uint32_t* batch_count, void* scratch, size_t scratch_bytes,
-                                             void* stream) {
+                                             uint32_t order, uint32_t num_cloths,
+                                             const uint32_t* cloth_constraint_offsets, uint32_t* perm,
+                                             uint32_t* colors, uint32_t* offsets, uint32_t* batch_count,
+                                             void* scratch, size_t scratch_bytes, void* stream) {
     if (!batch_count || !offsets || (e && (!ci || !cj || !perm))) return XPBD_ERR_INVALID_ARGUMENT;
     if (order != XPBD_ORDER_COLOR_REFERENCE && order != XPBD_ORDER_COLOR_INDEX) return XPBD_ERR_INVALID_ARGUMENT;
     if (e > 0x7FFFFFFFu) return XPBD_ERR_CAPACITY;
+    if (num_cloths) {  // cloth ranges: contiguous, covering every constraint
+        const uint32_t* co = cloth_constraint_offsets;
+        if (!co || co[0] != 0 || co[num_cloths] != e) return XPBD_ERR_INVALID_ARGUMENT;
+        for (uint32_t k = 0; k < num_cloths; ++k)
+            if (co[k + 1] < co[k]) return XPBD_ERR_INVALID_ARGUMENT;
+    }
     cudaStream_t st = (cudaStream_t)stream;
     if (e == 0) {  // one empty batch, as the host coloring
         const uint32_t zero[2] = {0, 0};
@@ -488,7 +602,7 @@ extern "C" int xpbd_color_constraints_device(uint32_t n, uint32_t e, const uint3
         *batch_count = 1;
         return XPBD_OK;
     }
-    const ColorLayout L = color_layout(n, e);
+    const ColorLayout L = color_layout(n, e, num_cloths);
     if (!scratch || scratch_bytes < L.total_bytes || ((uintptr_t)scratch & 255u)) return XPBD_ERR_INVALID_ARGUMENT;
     uint32_t* base = (uint32_t*)scratch;
     uint32_t* ctl = base + L.ctl;
@@ -533,16 +647,34 @@ extern "C" int xpbd_color_constraints_device(uint32_t n, uint32_t e, const uint3
     adjacency_kernel<<<ge, kPrepBlock, 0, st>>>(ci, cj, e, base + L.cursor, base + L.adj);
     PREP_CK(cudaGetLastError());
     trace.mark("adjacency");
-    // ---- Jones–Plassmann rounds, one cooperative launch
+    // ---- Jones–Plassmann rounds: per cloth (one CTA each, largest first) when the caller gives the cloth ranges,
+    // else over the whole grid (one cooperative launch, grid barrier per round)
     int dev = 0, sms = 0, per_sm = 0;
     PREP_CK(cudaGetDevice(&dev));
     PREP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    PREP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jp_color_kernel, kJpBlock, 0));
-    if (per_sm < 1) return XPBD_ERR_UNSUPPORTED;
     JpArgs a{ci, cj, deg, base + L.adj, rc, base + L.pending, base + L.front0, base + L.front1, ctl, e};
-    void* args[] = {&a};
-    PREP_CK(cudaLaunchCooperativeKernel((const void*)jp_color_kernel, dim3((unsigned)(sms * per_sm)),
-                                        dim3(kJpBlock), args, 0, st));
+    uint32_t blocks = 0;
+    if (num_cloths) {
+        std::vector<uint32_t> queue(num_cloths);
+        for (uint32_t k = 0; k < num_cloths; ++k) queue[k] = k;
+        const uint32_t* co = cloth_constraint_offsets;
+        std::stable_sort(queue.begin(), queue.end(),
+                         [&](uint32_t x, uint32_t y) { return co[x + 1] - co[x] > co[y + 1] - co[y]; });
+        PREP_CK(cudaMemcpyAsync(base + L.coff, co, ((size_t)num_cloths + 1) * 4, cudaMemcpyHostToDevice, st));
+        PREP_CK(cudaMemcpyAsync(base + L.queue, queue.data(), (size_t)num_cloths * 4, cudaMemcpyHostToDevice, st));
+        PREP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jp_cloth_kernel, kJpBlock, 0));
+        if (per_sm < 1) return XPBD_ERR_UNSUPPORTED;
+        blocks = std::min<uint32_t>(num_cloths, (uint32_t)(sms * per_sm));
+        jp_cloth_kernel<<<blocks, kJpBlock, 0, st>>>(a, base + L.coff, base + L.queue, num_cloths);
+        PREP_CK(cudaGetLastError());
+        PREP_CK(cudaStreamSynchronize(st));  // the host queue array must outlive its copy
+    } else {
+        PREP_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jp_color_kernel, kJpBlock, 0));
+        if (per_sm < 1) return XPBD_ERR_UNSUPPORTED;
+        blocks = (uint32_t)(sms * per_sm);
+        void* args[] = {&a};
+        PREP_CK(cudaLaunchCooperativeKernel((const void*)jp_color_kernel, dim3(blocks), dim3(kJpBlock), args, 0, st));
+    }
     PREP_CK(read_ctl(ctl, h, st));
     if (h[kCtlStatus]) return status_to_error(h[kCtlStatus]);
     if (h[kCtlDone] != e) return XPBD_ERR_INDEX_RANGE;
@@ -553,7 +685,7 @@ extern "C" int xpbd_color_constraints_device(uint32_t n, uint32_t e, const uint3
             return (double)(t1 - t0) * 1e-6;
         };
         fprintf(stderr, "[xpbd] device coloring  pending counts %8.2f ms, %u rounds %8.2f ms (%u blocks x %d)\n",
-                span(kCtlT0, kCtlT1), h[kCtlRounds], span(kCtlT1, kCtlT2), (unsigned)(sms * per_sm), kJpBlock);
+                span(kCtlT0, kCtlT1), h[kCtlRounds], span(kCtlT1, kCtlT2), blocks, kJpBlock);
     }
     trace.mark("rounds (one launch)");
     // ---- (color, index) batch order and offsets

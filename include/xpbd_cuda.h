@@ -257,15 +257,21 @@ int xpbd_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_
  * partition_constraints_for_gs_batches (mesh_prep.rs:153-221): the same colors, the same (color, index) batch order.
  * Device arrays: constraint_i/j[num_constraints]; perm[num_constraints] = input index of the k-th batch-sorted
  * constraint; colors[num_constraints] (may be NULL) = color of each input constraint; offsets[num_constraints + 2]
- * receives batch_count + 1 batch starts (no constraints: one empty batch, offsets {0, 0}). *batch_count is written on the host, so the call synchronises `stream`
- * (twice); the rest of the work is enqueued on it. A batch of cloths with disjoint particle ranges may be colored in
- * one call: each cloth gets the coloring it would get alone, and perm is then color-major across the cloths (the
- * batch's Gauss–Seidel order). Endpoints out of range or i == j: XPBD_ERR_INDEX_RANGE. `scratch` (256-byte aligned)
- * must hold xpbd_color_constraints_device_scratch_bytes(num_particles, num_constraints) bytes (about 48 bytes per
- * constraint). */
-size_t xpbd_color_constraints_device_scratch_bytes(uint32_t num_particles, uint32_t num_constraints);
+ * receives batch_count + 1 batch starts (no constraints: one empty batch, offsets {0, 0}). *batch_count is written on
+ * the host, so the call synchronises `stream`; the rest of the work is enqueued on it.
+ * A batch of cloths with disjoint particle ranges may be colored in one call: each cloth gets the coloring it would
+ * get alone, and perm is then color-major across the cloths (the batch's Gauss–Seidel order). Give the cloths'
+ * constraint ranges when they are known — cloth_constraint_offsets (host, num_cloths + 1 entries, from 0 to
+ * num_constraints): each cloth is then colored by one thread block of its own, much faster than the schedule over
+ * the whole grid used for num_cloths = 0 (one graph of unknown structure). Constraints of different cloths sharing a
+ * particle: XPBD_ERR_INVALID_ARGUMENT. Endpoints out of range or i == j: XPBD_ERR_INDEX_RANGE. `scratch` (256-byte
+ * aligned) must hold xpbd_color_constraints_device_scratch_bytes(num_particles, num_constraints, num_cloths) bytes
+ * (about 56 bytes per constraint). */
+size_t xpbd_color_constraints_device_scratch_bytes(uint32_t num_particles, uint32_t num_constraints,
+                                                   uint32_t num_cloths);
 int xpbd_color_constraints_device(uint32_t num_particles, uint32_t num_constraints, const uint32_t* constraint_i,
-                                  const uint32_t* constraint_j, uint32_t order, uint32_t* perm, uint32_t* colors,
+                                  const uint32_t* constraint_j, uint32_t order, uint32_t num_cloths,
+                                  const uint32_t* cloth_constraint_offsets, uint32_t* perm, uint32_t* colors,
                                   uint32_t* offsets, uint32_t* batch_count, void* scratch, size_t scratch_bytes,
                                   void* stream);
 /* Particle-major neighbour table of finalize_cloth_mesh (mesh_prep.rs:588-635) on the GPU, for constraints already in

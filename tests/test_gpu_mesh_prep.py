@@ -32,7 +32,8 @@ def _host(t):
     return t.cpu().numpy().view(np.uint32)
 
 
-def color_device(n, ci, cj, order=REF):
+def color_device(n, ci, cj, order=REF, cloths=None):
+    """cloths: None = one graph (schedule over the whole grid); a list of constraint offsets = one CTA per cloth."""
     import torch
     L = N.load()
     e = len(ci)
@@ -40,11 +41,13 @@ def color_device(n, ci, cj, order=REF):
     perm = torch.empty(max(e, 1), dtype=torch.int32, device="cuda")
     colors = torch.empty(max(e, 1), dtype=torch.int32, device="cuda")
     offs = torch.empty(e + 2, dtype=torch.int32, device="cuda")
-    nbytes = L.xpbd_color_constraints_device_scratch_bytes(n, e)
+    nc = 0 if cloths is None else len(cloths) - 1
+    coff = np.ascontiguousarray(cloths if cloths is not None else [0], np.uint32)
+    nbytes = L.xpbd_color_constraints_device_scratch_bytes(n, e, nc)
     scratch = torch.empty(max(nbytes, 1), dtype=torch.uint8, device="cuda")
     bc = C.c_uint32()
-    st = L.xpbd_color_constraints_device(n, e, _vp(dci), _vp(dcj), order, _vp(perm), _vp(colors), _vp(offs),
-                                         C.byref(bc), _vp(scratch), nbytes,
+    st = L.xpbd_color_constraints_device(n, e, _vp(dci), _vp(dcj), order, nc, coff.ctypes.data if nc else None,
+                                         _vp(perm), _vp(colors), _vp(offs), C.byref(bc), _vp(scratch), nbytes,
                                          C.c_void_p(torch.cuda.current_stream().cuda_stream))
     torch.cuda.synchronize()
     return st, _host(perm)[:e], _host(colors)[:e], _host(offs)[: bc.value + 1], bc.value
@@ -65,15 +68,17 @@ def color_host(n, ci, cj, order=REF):
 
 
 def check_coloring(n, ci, cj, order=REF):
-    st, perm, colors, offs, nb = color_device(n, ci, cj, order)
-    assert st == 0
+    """Both schedules — over the whole grid, and the graph as one cloth of its own CTA — against host and oracle."""
     hperm, hoffs, hnb = color_host(n, ci, cj, order)
     operm, ocolors, ooffs = orc.partition(n, ci, cj, order == INDEX)
-    assert nb == hnb == len(ooffs) - 1
-    assert np.array_equal(perm, hperm) and np.array_equal(perm, operm)
-    assert np.array_equal(offs, hoffs) and np.array_equal(offs, ooffs)
-    assert np.array_equal(colors[perm], ocolors)
-    return nb
+    for cloths in (None, [0, len(ci)]):
+        st, perm, colors, offs, nb = color_device(n, ci, cj, order, cloths)
+        assert st == 0
+        assert nb == hnb == len(ooffs) - 1
+        assert np.array_equal(perm, hperm) and np.array_equal(perm, operm)
+        assert np.array_equal(offs, hoffs) and np.array_equal(offs, ooffs)
+        assert np.array_equal(colors[perm], ocolors)
+    return hnb
 
 
 @pytest.mark.parametrize("side", [2, 3, 32, 256])
@@ -96,14 +101,15 @@ def test_hanging_grid_coloring_matches_oracle():
     check_coloring(mesh.num_particles, mesh.constraint_i[p], mesh.constraint_j[p])
 
 
-def test_batch_coloring_equals_per_cloth_coloring():
+@pytest.mark.parametrize("per_cloth", [False, True], ids=["grid", "cta_per_cloth"])
+def test_batch_coloring_equals_per_cloth_coloring(per_cloth):
     specs = wl.config3_batch()[:24]
     offs_v = np.cumsum([0] + [s.num_particles for s in specs])
     ci = np.concatenate([s.constraint_i + o for s, o in zip(specs, offs_v)]).astype(np.uint32)
     cj = np.concatenate([s.constraint_j + o for s, o in zip(specs, offs_v)]).astype(np.uint32)
-    st, perm, colors, offs, nb = color_device(int(offs_v[-1]), ci, cj)
-    assert st == 0
     eoff = np.cumsum([0] + [s.num_constraints for s in specs])
+    st, perm, colors, offs, nb = color_device(int(offs_v[-1]), ci, cj, cloths=list(eoff) if per_cloth else None)
+    assert st == 0
     for k, s in enumerate(specs):
         operm, ocolors, _ = orc.partition(s.num_particles, s.constraint_i, s.constraint_j)
         mine = colors[eoff[k]:eoff[k + 1]]
@@ -144,8 +150,16 @@ def test_coloring_edge_cases():
     offs = torch.empty(2, dtype=torch.int32, device="cuda")
     scratch = torch.empty(256, dtype=torch.uint8, device="cuda")
     bc = C.c_uint32()
-    assert L.xpbd_color_constraints_device(2, 1, _vp(ci), _vp(cj), REF, _vp(perm), None, _vp(offs), C.byref(bc),
-                                           _vp(scratch), 256, None) == N.ERR_INVALID_ARGUMENT
+    assert L.xpbd_color_constraints_device(2, 1, _vp(ci), _vp(cj), REF, 0, None, _vp(perm), None, _vp(offs),
+                                           C.byref(bc), _vp(scratch), 256, None) == N.ERR_INVALID_ARGUMENT
+    # cloth ranges that do not cover the constraints, or that decrease, are refused
+    ci3, cj3 = np.array([0, 1, 2], np.uint32), np.array([1, 2, 3], np.uint32)
+    assert color_device(4, ci3, cj3, cloths=[0, 2])[0] == N.ERR_INVALID_ARGUMENT
+    assert color_device(4, ci3, cj3, cloths=[0, 2, 1, 3])[0] == N.ERR_INVALID_ARGUMENT
+    # two "cloths" that share particle 1 (and 2): refused, nothing colored out of range
+    assert color_device(4, ci3, cj3, cloths=[0, 1, 3])[0] == N.ERR_INVALID_ARGUMENT
+    # the same constraints as one cloth are fine
+    assert color_device(4, ci3, cj3, cloths=[0, 3])[0] == 0
 
 
 def neighbor_table_device(n, ci, cj):
