@@ -361,6 +361,7 @@ def test_gauss_seidel_execution_paths_bit_exact(cluster):
     st = plug.stats()
     if cluster > 1:
         assert st["grid_blocks"] == cluster
+    assert st["solver_kernel"] == (3 if cluster > 1 else 1)  # the requested execution ran
     plug.step(frames=6)
     o = oracle_sim(sp, prm, cfg)
     o.substeps(60)

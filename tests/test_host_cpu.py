@@ -93,6 +93,27 @@ def test_color_constraints_rejects_bad_indices():
     assert st == N.ERR_INDEX_RANGE
 
 
+def test_device_coloring_validates_cloth_ranges_before_any_device_work():
+    """The GPU coloring checks its host arguments first: cloth ranges that do not start at 0, do not end at the
+    constraint count, or decrease are refused before any CUDA call (the device pointers are never touched)."""
+    L = N.load()
+    fake = C.c_void_p(0x1000)  # never dereferenced: the call returns before using it
+    nb = C.c_uint32()
+    n, e = 10, 6
+    for bad in ([0, 4], [1, 3, 6], [0, 4, 3, 6], [0, 7]):
+        offs = np.array(bad, np.uint32)
+        st = L.xpbd_color_constraints_device(n, e, fake, fake, 0, len(bad) - 1, offs.ctypes.data, fake, None, fake,
+                                             C.byref(nb), fake, 1 << 30, None)
+        assert st == N.ERR_INVALID_ARGUMENT, bad
+    st = L.xpbd_color_constraints_device(n, e, fake, fake, 7, 0, None, fake, None, fake, C.byref(nb), fake, 1 << 30,
+                                         None)
+    assert st == N.ERR_INVALID_ARGUMENT  # unknown order
+    # scratch grows with the constraints and (a little) with the cloth count
+    a = L.xpbd_color_constraints_device_scratch_bytes(1000, 5000, 0)
+    b = L.xpbd_color_constraints_device_scratch_bytes(1000, 5000, 100)
+    assert 5000 * 48 < a < b
+
+
 @pytest.mark.parametrize("s", [3, 4, 16, 32, 256])
 def test_sheet_constraint_count(s):
     ci, cj, ct = wl.sheet_constraints(s)
