@@ -359,7 +359,8 @@ def run_warm_leg(args, device: int) -> dict:
     """Convergence solve, learned vs plain (and previous-substep λ) warm start.
 
     Per substep, Jacobi (degree-averaged) iterates each cloth until its max residual |C + α̃λ|/rest — the strain
-    |‖xi−xj‖−rest|/rest for the rigid (α = 0) constraints — is at or below 1e-4, capped at 1024 passes. Cloths: the
+    |‖xi−xj‖−rest|/rest for the rigid (α = 0) constraints — is at or below 1e-4, capped at 4096 passes (the library's
+    maximum; at 1024 the plain start hit the cap on 94 % of cloth-substeps, which bounds the ratio). Cloths: the
     config-3 generator (sides 16..96, random pins, stretch compliance 10^U(-8,-3)), 48 for training (seed 31) and a
     different 48 for the measurement (seed 32). Training data: 60 plain substeps of the training batch, every 28th
     constraint; the MLP (BF16 tensor-core kernels) is fitted with 4000 Adam steps of 4096 samples. Measurement:
@@ -369,7 +370,7 @@ def run_warm_leg(args, device: int) -> dict:
 
     from bevy_xpbd_b200 import plugin as P
     from bevy_xpbd_b200 import workloads as wl
-    cap, tol = 1024, 1e-4
+    cap, tol = 4096, 1e-4
     dt, inv_dt = wl.substep_dt(10)
     prm = P.XpbdCpuTimeStepParams(float(dt), float(inv_dt), 1.0, cap, linear_drag_per_sec=0.01)
 

@@ -629,15 +629,18 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     H2D(tiles_d, tiles.data(), tiles.size() * sizeof(XpbdTile));
     {
         std::vector<uint16_t> rc(N);
-        for (uint32_t k = 0; k < C; ++k)
+        parallel_for(C, [&](uint32_t k) {
             for (uint32_t i = 0; i < ctx->cloths[k].n; ++i) rc[ctx->cloths[k].vtx_off + i] = (uint16_t)k;
+        });
         H2D(rcloth_d, rc.data(), N * sizeof(uint16_t));
         CK(cudaStreamSynchronize(st), "commit sync");
     }
     H2D(pal_d, palette.data(), palette.size() * sizeof(float));
     std::vector<uint8_t> ctypes(E);
-    for (auto& c : ctx->cloths)
+    parallel_for(C, [&](uint32_t k) {
+        const ClothHost& c = ctx->cloths[k];
         for (uint32_t e = 0; e < c.e; ++e) ctypes[c.con_off + e] = (uint8_t)std::min<uint32_t>(c.ctype[e], 2);
+    });
     if (E) {
         H2D(con_d, con.data(), E * sizeof(uint4));
         H2D(con_in_d, con_in.data(), E * sizeof(uint4));
@@ -653,11 +656,13 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     CK(cudaMemsetAsync(cstats_d, 0, sizeof(XpbdConvergeStats), st), "memset");
     {
         std::vector<uint32_t> ioc(2 * (size_t)E);
-        for (auto& c : ctx->cloths)
+        parallel_for(C, [&](uint32_t k) {
+            const ClothHost& c = ctx->cloths[k];
             for (uint32_t e = 0; e < c.e; ++e) {
                 ioc[2 * ((size_t)c.con_off + e)] = c.inc_i[e];
                 ioc[2 * ((size_t)c.con_off + e) + 1] = c.inc_j[e];
             }
+        });
         if (E) H2D(inc_of_con_d, ioc.data(), ioc.size() * 4);
         CK(cudaStreamSynchronize(st), "commit sync");
     }
