@@ -1510,6 +1510,13 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
     int r = check_ready(ctx);
     if (r != XPBD_OK) return r;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    // plain Jacobi: the spatial-patch kernel is one of the candidates, so its tables are built now if they are not yet
+    // (a batch that cannot be split into patches simply has no patch candidates)
+    if (ctx->opts.solver == XPBD_SOLVER_JACOBI && !(ctx->opts.tolerance > 0.f || ctx->opts.warm_start)) {
+        bool usable = false;
+        r = ensure_patches(ctx, &usable);
+        if (r != XPBD_OK) return r;
+    }
     const uint32_t N = ctx->W.n;
     float4 *sx = nullptr, *sv = nullptr;
     CK(cudaMalloc(&sx, (size_t)N * sizeof(float4)), "snapshot");
@@ -1531,7 +1538,7 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
     const uint32_t jks[3] = {2, 3, 1};
     for (uint32_t jk : jks) {
         if (base.solver != XPBD_SOLVER_JACOBI && jk != 1) continue;
-        if (jk == 2 && !ctx->patches_ok) continue;  // tried only when the caller already built the patches
+        if (jk == 2 && !ctx->patches_ok) continue;
         const uint32_t kid = base.solver == XPBD_SOLVER_JACOBI ? (jk == 2 ? 2u : (jk == 3 ? 5u : 0u)) : 1u;
         for (uint32_t blk : blocks) {
             int maxb = max_blocks_per_sm(kid, blk, ctx->W);

@@ -104,8 +104,8 @@ typedef struct xpbd_solver_opts {
     uint32_t warm_start;              /* convergence solve start: XPBD_WARM_* (0 = plain, λ = 0) */
     uint32_t cluster_ctas;            /* Gauss–Seidel in one thread-block cluster: 0 auto, 1 off, 8 or 16 CTAs */
     uint32_t jacobi_kernel;           /* Jacobi: 0 default (= 3), 1 warp tiles, 2 shared-memory patches (their tables
-                                         are built by the first call that selects them; xpbd_autotune tries them only
-                                         once built), 3 thread per particle */
+                                         are built by the first call that selects them, or by xpbd_autotune, which
+                                         tries them for plain Jacobi), 3 thread per particle */
     float tolerance;                  /* > 0 (or warm_start != 0): convergence solve — Jacobi, λ kept per substep,
                                          iterate until max |C + α̃λ|/rest <= tolerance, at most inner_iterations */
     uint32_t reserved[3];
@@ -223,8 +223,10 @@ int xpbd_color_constraints(uint32_t num_particles, uint32_t num_constraints, con
                            uint32_t* batch_count);
 
 /* ---- autotuning -------------------------------------------------------------------------------------------- */
-/* Times `frames` frames per candidate schedule (block size × resident blocks per SM) on a snapshot of the state,
- * restores the state and keeps the fastest. Writes the chosen block_threads / blocks_per_sm to opts_out. */
+/* Times `frames` frames per candidate schedule on a snapshot of the state, restores the state and keeps the fastest.
+ * Candidates: Jacobi execution (spatial patches — their tables built here if needed —, thread per particle, warp
+ * tiles) × block size × resident blocks per SM; Gauss–Seidel: grid kernel × block × blocks per SM, and clusters of 16
+ * or 8 CTAs. Writes the chosen block_threads / blocks_per_sm / cluster_ctas / jacobi_kernel to opts_out. */
 int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* opts_out);
 
 /* ---- collision pipeline introspection (bit-exact parity tests) ---------------------------------------------- */
