@@ -149,6 +149,22 @@ def _u32(a):
     return np.ascontiguousarray(a, np.uint32)
 
 
+def mlp_scale_change(params, norm, factor: float):
+    """Parameters of the warm-start network whose predicted change of the multiplier is `factor` times the given one's.
+
+    The network predicts, standardised, the change of t = λ·(wi + wj + α̃)/rest over the previous substep:
+    λ0 = (y·tstd + tmean + t_prev)·rest/(wi + wj + α̃), with y linear in the output layer (w3, b3). Scaling w3, b3 and
+    tmean by `factor` scales the change y·tstd + tmean and nothing else: factor 1 is the network as trained, 0 the
+    previous substep's multiplier. A factor below 1 shrinks the prediction toward the previous multiplier, which lowers
+    the worst-constraint error that the convergence test is bound by; choose it on the training cloths."""
+    p = np.array(params, np.float32, copy=True)
+    n = np.array(norm, np.float32, copy=True)
+    w3 = N.MLP_PARAMS - 65  # w3[64] then b3 at the end of the parameter vector
+    p[w3:] *= np.float32(factor)
+    n[18] *= np.float32(factor)
+    return p, n
+
+
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 

@@ -49,3 +49,22 @@ def test_features_hand_computed():
     assert list(f[0, 5:]) == [0.0, 1.0, 0.0, 1.0]
     t = MO.targets([3.0], [1.0], [1e-6], [1.0, 0.0], [0], [1], 100.0)
     np.testing.assert_allclose(t, [3.0 * 1.01], rtol=1e-6)
+
+
+def test_scaled_change_scales_the_predicted_change():
+    """mlp_scale_change: the change y·tstd + tmean that the network adds to the previous multiplier scales by the
+    factor (exactly for a power of two, where the fp32 parameters scale without rounding)."""
+    from bevy_xpbd_b200.plugin import mlp_scale_change
+    rng = np.random.default_rng(4)
+    p = (rng.normal(size=MO.N_PARAMS) * 0.2).astype(np.float32)
+    nm = np.concatenate([rng.normal(size=9), np.abs(rng.normal(size=9)) + 0.5, [0.3, 1.7]]).astype(np.float32)
+    f = rng.normal(size=(50, MO.N_FEATURES)).astype(np.float32)
+
+    def change(pp, nn):
+        return MO.forward(pp, nn, f, rounding=False) * float(nn[19]) + float(nn[18])
+
+    base = change(p, nm)
+    for factor, tol in ((0.5, 0.0), (0.0, 0.0), (0.35, 1e-6)):
+        p2, n2 = mlp_scale_change(p, nm, factor)
+        assert np.array_equal(p2[:-65], p[:-65]) and np.array_equal(n2[:18], nm[:18]) and n2[19] == nm[19]
+        np.testing.assert_allclose(change(p2, n2), factor * base, rtol=tol, atol=tol)
