@@ -12,10 +12,12 @@
 // relative order inside a cloth is unchanged by the cloth's particle offset, so each cloth gets its own coloring.
 //
 // Steps: degrees (atomics) → processing rank by three stable LSD radix sorts (max endpoint, then min endpoint, then
-// degree descending) → particle → constraint adjacency → one cooperative persistent kernel (per constraint the number
-// of earlier-ranked neighbour slots; then rounds over a frontier, a warp per constraint: OR of the neighbours' colors
-// in 64-color windows, the smallest free color, release of later-ranked neighbours whose count reaches zero) →
-// stable sort by color (the (color, index) batch order) → batch offsets.
+// degree descending) → particle → constraint adjacency → the rounds: per constraint the number of earlier-ranked
+// neighbour slots, then rounds over a frontier (four frontier constraints per warp, 8 lanes each: OR of the
+// neighbours' colors in 64-color windows, the smallest free color, release of later-ranked neighbours whose count
+// reaches zero) — per cloth in one CTA each when the caller gives the cloths' constraint ranges (jp_cloth_kernel,
+// __syncthreads between rounds), else over the whole grid in one cooperative launch (jp_color_kernel, grid barrier
+// between rounds) → stable sort by color (the (color, index) batch order) → batch offsets.
 //
 // Neighbour table. Row p lists the constraints at particle p in increasing constraint position, the i slot of a
 // constraint before its j slot — the order of the reference's cursor scatter. That is a stable sort of the 2E
