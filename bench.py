@@ -571,10 +571,10 @@ def run_prep_leg(device: int, reps: int = 5) -> dict:
 
 
 def cpu_oracle_run(w: dict, budget_s: float, max_cloths: int | None = None, min_frames: int = 1,
-                   variant: str = "omp"):
+                   variant: str = "omp", warmup_frames: int = 1):
     """Times the CPU restatement of xpbd_cpu.rs (OpenMP build, or the serial build with the reference's loop order)
     on a bounded sample of workload `w`: every `len/max_cloths`-th cloth, as many whole frames as fit in `budget_s`
-    (at least `min_frames`)."""
+    (at least `min_frames`), after `warmup_frames` untimed frames."""
     from oracle import oracle as orc
     from tests.helpers import oracle_params
     orc.select(variant)
@@ -591,8 +591,11 @@ def cpu_oracle_run(w: dict, budget_s: float, max_cloths: int | None = None, min_
         s.set_batches(offs)
         sims.append(s)
     S = w["cfg"].solve_substeps
+    for _ in range(max(warmup_frames, 1) - 1):  # untimed warm-up frames
+        for s in sims:
+            s.substeps(S)
     t0 = time.perf_counter()
-    for s in sims:  # one untimed frame: warm-up and per-frame estimate
+    for s in sims:  # the last untimed frame also gives the per-frame estimate
         s.substeps(S)
     per_frame = time.perf_counter() - t0
     frames = max(min_frames, int(budget_s / max(per_frame, 1e-6)))
@@ -611,11 +614,11 @@ def run_reference(args, rank: int, world: int):
         return
     w = make_workload(args.workload, 0, 1)
     max_cloths = 16 if args.workload == "c3" else None
-    res = cpu_oracle_run(w, budget_s=0.0, max_cloths=max_cloths, min_frames=args.steps)
+    res = cpu_oracle_run(w, budget_s=0.0, max_cloths=max_cloths, min_frames=args.steps, warmup_frames=args.warmup)
     sample = (f"{res['frames']} frames of {res['cloths']} of the workload's {len(w['specs'])} cloths"
               if max_cloths else f"{res['frames']} frames of the workload")
     line = {"metric": METRIC, "value": round(res["value"], 4), "unit": UNIT, "n_gpus": world,
-            "steps": res["frames"], "warmup": 1, "ms_per_step": round(res["per_frame_s"] * 1e3, 3),
+            "steps": res["frames"], "warmup": max(args.warmup, 1), "ms_per_step": round(res["per_frame_s"] * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
             "data": "synthetic: seeded procedural sheets (no dataset)",
             "config": {"workload": w["desc"], "particles": w["n"], "constraints": w["e"]},
