@@ -49,12 +49,16 @@ __device__ __forceinline__ bool fpdiv3_by_length_fast(float ax, float ay, float 
 // magnitude in [2^-37, 2^58] (see coord_outside_fast_range), every nonzero difference of two coordinates is a
 // multiple of 2^-60 (so |a_k| >= 2^-60), every length of a used term is in [1e-8, 2^60), and the quotients are in
 // [2^-120, 1 + 2^-23] — all normal, so the result is RN(a_k / b).
+// A zero numerator gives a zero of either sign here (the remainder step runs for it too, saving the select): RN(a_k / b)
+// up to the sign of a zero. Its caller multiplies the quotient into a term that is added to a sum started at +0, where
+// a zero of either sign leaves the sum unchanged, so the result is the same bits.
 __device__ __forceinline__ void fpdiv3_unchecked(float ax, float ay, float az, float b, float& qx, float& qy,
                                                  float& qz) {
     const float y = __frcp_rn(b);
-    qx = fpdiv_step(ax, b, y);
-    qy = fpdiv_step(ay, b, y);
-    qz = fpdiv_step(az, b, y);
+    const float px = __fmul_rn(ax, y), py = __fmul_rn(ay, y), pz = __fmul_rn(az, y);
+    qx = __fmaf_rn(__fmaf_rn(-b, px, ax), y, px);
+    qy = __fmaf_rn(__fmaf_rn(-b, py, ay), y, py);
+    qz = __fmaf_rn(__fmaf_rn(-b, pz, az), y, pz);
 }
 
 // True when a coordinate breaks the fpdiv3_unchecked invariant: nonzero and below 2^-37 in magnitude, above 2^58,
