@@ -87,8 +87,9 @@ def make_workload(name: str, rank: int = 0, world: int = 1, c3_cloths: int = 0) 
     S, I = cfg.solve_substeps, prm.inner_iterations
     # algorithmic bytes per frame (fp32): S*(100N + I*(28N + 16E)); see DESIGN.md
     bytes_alg = S * (100 * n + I * (28 * n + 16 * e))
+    full_launch = name != "c3" or (not c3_cloths and world == 1)
     return dict(name=name, specs=specs, params=prm, cfg=cfg, desc=desc, n=n, e=e, cloths=len(specs),
-                total_cloths=total_cloths, bytes_per_frame=bytes_alg)
+                total_cloths=total_cloths, bytes_per_frame=bytes_alg, full_launch=full_launch)
 
 
 def working_set_bytes(w: dict) -> int:
@@ -285,7 +286,9 @@ def time_e2e(w: dict, plug, steps: int, warmup: int, world: int):
 
 def roofline(w: dict, mean_ms: float, kernel: str, peaks: dict) -> dict:
     achieved = w["bytes_per_frame"] / (mean_ms * 1e-3) / 1e9
-    traffic = load_traffic(kernel, w["name"])
+    # the committed per-launch traffic is of the full single-GPU workload: a sample of c3's cloths (--c3-cloths) or a
+    # rank's shard of them launches less, and gets none
+    traffic = load_traffic(kernel, w["name"]) if w["full_launch"] else None
     return {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
             "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peaks["source"],
             "alg_bytes_per_launch": int(w["bytes_per_frame"]), "traffic": traffic}
