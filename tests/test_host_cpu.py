@@ -147,3 +147,13 @@ def test_product_never_imports_the_oracle():
             if f.endswith((".py", ".cu", ".cpp", ".h")):
                 text = open(os.path.join(dirpath, f)).read()
                 assert "import oracle" not in text and "from oracle" not in text and "xpbd_oracle" not in text, f
+
+
+def test_bench_reports_committed_traffic_only_for_the_full_launch():
+    """The committed ncu traffic per launch is of the full single-GPU workload: a sample of c3's cloths or a rank's
+    shard of them launches less work and must not be reported with it; single-sheet replicas launch the same."""
+    import bench
+    assert bench.make_workload("c3", 0, 1)["full_launch"]
+    assert not bench.make_workload("c3", 0, 1, c3_cloths=8)["full_launch"]
+    assert not bench.make_workload("c3", 1, 2)["full_launch"]
+    assert bench.make_workload("c0", 1, 2)["full_launch"]
