@@ -85,7 +85,8 @@ def make_workload(name: str, rank: int = 0, world: int = 1, c3_cloths: int = 0) 
     n = sum(s.num_particles for s in specs)
     e = sum(s.num_constraints for s in specs)
     S, I = cfg.solve_substeps, prm.inner_iterations
-    # algorithmic bytes per frame (fp32): S*(100N + I*(28N + 16E)); see DESIGN.md
+    # algorithmic bytes per frame (fp32): S*(100N + I*(28N + 16E)) — per pass x read+write and inverse mass (28 B per
+    # particle) plus i, j, rest, compliance (16 B per constraint); per substep 100 B per particle for predict + velocity
     bytes_alg = S * (100 * n + I * (28 * n + 16 * e))
     full_launch = name != "c3" or (not c3_cloths and world == 1)
     return dict(name=name, specs=specs, params=prm, cfg=cfg, desc=desc, n=n, e=e, cloths=len(specs),
