@@ -73,7 +73,9 @@ def make_workload(name: str, rank: int = 0, world: int = 1, c3_cloths: int = 0) 
         allspecs = wl.config3_batch()
         if c3_cloths:
             allspecs = allspecs[:c3_cloths]
-        specs = [s for k, s in enumerate(allspecs) if k % world == rank]
+        from bevy_xpbd_b200.sharding import shard_by_constraints
+        mine = shard_by_constraints([s.num_constraints for s in allspecs], world)[rank]
+        specs = [allspecs[k] for k in mine]
         prm = P.XpbdCpuTimeStepParams(float(dt), float(inv_dt), 1.0, 10)
         cfg = P.ClothSimConfig(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
         desc = (f"c3: {len(allspecs)} cloths, sides seeded uniform 16..192 vertices, random pins and stretch compliance, "
@@ -91,6 +93,27 @@ def make_workload(name: str, rank: int = 0, world: int = 1, c3_cloths: int = 0) 
     full_launch = name != "c3" or (not c3_cloths and world == 1)
     return dict(name=name, specs=specs, params=prm, cfg=cfg, desc=desc, n=n, e=e, cloths=len(specs),
                 total_cloths=total_cloths, bytes_per_frame=bytes_alg, full_launch=full_launch)
+
+
+_CONFIGS: dict = {}
+
+
+def workload_config(name: str, world: int) -> dict:
+    """The `config` object of both arms' JSON lines: the whole job's workload (every rank's cloths), how it is split
+    over ranks, and the L2 policy of the timed region; identical for the GPU arm and the reference arm."""
+    if (name, world) in _CONFIGS:
+        return dict(_CONFIGS[(name, world)])
+    w = make_workload(name, 0, 1)
+    reps = world if name != "c3" else 1
+    flush = working_set_bytes(w) < L2_BYTES
+    _CONFIGS[(name, world)] = {"workload": w["desc"], "cloths": w["total_cloths"] * reps, "particles": w["n"] * reps,
+            "constraints": w["e"] * reps, "substeps": w["cfg"].solve_substeps,
+            "iterations": w["params"].inner_iterations,
+            "parallelism": ("replicas" if name != "c3" else "cloth shards balanced by constraints") + f" x{world}",
+            "l2": ("GPU arm: L2 flushed between timed steps (256 MiB write outside the events); CPU arm: n/a" if flush
+                   else f"GPU arm: inputs larger than L2 (working set {working_set_bytes(w) / 1e6:.0f} MB); "
+                        "CPU arm: n/a")}
+    return dict(_CONFIGS[(name, world)])
 
 
 def working_set_bytes(w: dict) -> int:
@@ -335,15 +358,13 @@ def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks:
         "ms_per_step": round(mean_ms, 4),
         "steps": steps,
         "gpu_launches": launches,
-        "config": {"workload": w["desc"], "particles": w["n"], "constraints": w["e"], "cloths": w["cloths"],
-                   "substeps": w["cfg"].solve_substeps, "iterations": w["params"].inner_iterations,
-                   "colors": st["num_colors"], "block_threads": st["block_threads"], "grid_blocks": st["grid_blocks"],
-                   "blocks_per_sm_tuned": tuned.blocks_per_sm, "solver_kernel": kernel,
-                   "cluster_ctas": st["cluster_ctas"], "cuda_graph": bool(st["graph_captured"]),
-                   "cooperative_launch": bool(st["cooperative_launch"]),
-                   "l2": ("flushed between timed steps (256 MiB write outside the events)" if flush
-                          else f"inputs larger than L2 (working set {working_set_bytes(w) / 1e6:.0f} MB)"),
-                   "setup_s": round(setup_s, 2)},
+        "config": workload_config(name, world),
+        "schedule": {"rank0_cloths": w["cloths"], "rank0_particles": w["n"], "rank0_constraints": w["e"],
+                     "colors": st["num_colors"], "block_threads": st["block_threads"],
+                     "grid_blocks": st["grid_blocks"], "blocks_per_sm_tuned": tuned.blocks_per_sm,
+                     "solver_kernel": kernel, "cluster_ctas": st["cluster_ctas"],
+                     "cuda_graph": bool(st["graph_captured"]), "cooperative_launch": bool(st["cooperative_launch"]),
+                     "setup_s": round(setup_s, 2)},
         "roofline": roofline(w, mean_ms, kernel, peaks) if w["cfg"].collision == 0 else None,
         "clocks": clocks,
         "step_ms_min_max": [round(min(per), 4), round(max(per), 4)],
@@ -625,7 +646,7 @@ def run_reference(args, rank: int, world: int):
             "steps": res["frames"], "warmup": max(args.warmup, 1), "ms_per_step": round(res["per_frame_s"] * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
             "data": "synthetic: seeded procedural sheets (no dataset)",
-            "config": {"workload": w["desc"], "particles": w["n"], "constraints": w["e"]},
+            "config": workload_config(args.workload, world),
             "cpu_baseline": {"value": round(res["value"], 4), "unit": UNIT, "cores": res["cores"], "kind": "port",
                              "sample": sample + ", OpenMP build of the oracle"},
             "e2e": {"value": round(res["value"], 4), "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -671,16 +692,17 @@ def main():
             "warmup": args.warmup, "ms_per_step": main_res["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded procedural sheets (no dataset)", "config": main_res["config"],
+            "schedule": main_res["schedule"],
             "roofline": main_res["roofline"], "e2e": main_res.get("e2e"), "gpu_launches": main_res["gpu_launches"],
             "clocks": main_res["clocks"], "step_ms_min_max": main_res["step_ms_min_max"],
             "substeps_per_s": round(main_res["value"] * w["cfg"].solve_substeps, 1)}
-    line["config"]["parallelism"] = ("replicas" if args.workload != "c3" else "cloth shards") + f" x{world}"
     if not args.no_batched and args.workload != "c3":
         b = run_gpu_workload("c3", args, rank, world, local, peaks, with_e2e=False)
         b.pop("_w")
         line["batched"] = {"value": b["value"], "unit": UNIT, "ms_per_step": b["ms_per_step"], "steps": b["steps"],
                            "substeps_per_s": round(b["value"] * 10, 1),
-                           "config": b["config"], "roofline": b["roofline"], "gpu_launches": b["gpu_launches"],
+                           "config": b["config"], "schedule": b["schedule"], "roofline": b["roofline"],
+                           "gpu_launches": b["gpu_launches"],
                            "clocks": b["clocks"]}
     if rank == 0 and world == 1 and not args.no_warm:
         line["warm_start"] = run_warm_leg(args, local)

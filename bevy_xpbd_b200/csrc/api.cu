@@ -1149,6 +1149,12 @@ extern "C" int xpbd_set_params(xpbd_ctx* ctx, const xpbd_time_step_params* param
     return XPBD_OK;
 }
 
+// Errors with which the runtime refuses a cooperative launch (as opposed to a failure of the work itself).
+static bool coop_refused(cudaError_t e) {
+    return e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported ||
+           e == cudaErrorStreamCaptureUnsupported || e == cudaErrorNotPermitted;
+}
+
 static int run_frames(xpbd_ctx* ctx, uint32_t frames) {
     cudaStream_t st = ctx->stream;
     if (ctx->opts.use_graphs) {
@@ -1164,7 +1170,9 @@ static int run_frames(xpbd_ctx* ctx, uint32_t frames) {
             if (e != cudaSuccess || e2 != cudaSuccess) {
                 if (g) cudaGraphDestroy(g);
                 cudaGetLastError();
-                if (ctx->coop) {  // retry without the cooperative attribute (bounded barriers still hold)
+                // nothing of a failed capture ran: if the cooperative attribute was refused, capture again without
+                // it (the bounded barriers still hold; stats.cooperative_launch then reads 0)
+                if (ctx->coop && coop_refused(e != cudaSuccess ? e : e2)) {
                     ctx->coop = false;
                     return run_frames(ctx, frames);
                 }
@@ -1183,9 +1191,13 @@ static int run_frames(xpbd_ctx* ctx, uint32_t frames) {
         for (uint32_t f = 0; f < frames; ++f) {
             uint64_t launches = 0;
             cudaError_t e = enqueue_frame(ctx, st, &launches);
-            if (e != cudaSuccess && ctx->coop) {
+            // Retry without the cooperative attribute only when the refused launch was the frame's first (the
+            // solver launch of every schedule but the convergence solve, which predicts first): then nothing of
+            // the frame has been queued and running it again cannot advance the state twice.
+            if (e != cudaSuccess && ctx->coop && coop_refused(e) && launches <= 1 && ctx->kernel != 6) {
                 cudaGetLastError();
                 ctx->coop = false;
+                launches = 0;
                 e = enqueue_frame(ctx, st, &launches);
             }
             if (e != cudaSuccess) return cuda_fail(ctx, e, "frame launch");
@@ -1637,6 +1649,8 @@ extern "C" int xpbd_collision_pairs(xpbd_ctx* ctx, uint32_t* pairs, uint64_t cap
 }
 
 // ------------------------------------------------------------------------------------------------- primitives
+bool xpbd_sort_arrays_overlap(const void* keys_in, const void* vals_in, const void* keys_out, const void* vals_out,
+                              uint32_t n);
 extern "C" size_t xpbd_radix_sort_scratch_bytes(uint32_t n) { return radix_sort_scratch_bytes(n); }
 
 extern "C" int xpbd_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
@@ -1644,8 +1658,9 @@ extern "C" int xpbd_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* va
                                      size_t scratch_bytes, void* stream) {
     if (n && (!keys_in || !vals_in || !keys_out || !vals_out || !scratch)) return XPBD_ERR_INVALID_ARGUMENT;
     if (passes < 1 || passes > 4) return XPBD_ERR_INVALID_ARGUMENT;
+    if (n > XPBD_RADIX_SORT_MAX_KEYS) return XPBD_ERR_CAPACITY;
     if (scratch_bytes < radix_sort_scratch_bytes(n)) return XPBD_ERR_INVALID_ARGUMENT;
-    if (keys_in == keys_out || vals_in == vals_out) return XPBD_ERR_INVALID_ARGUMENT;
+    if (n && xpbd_sort_arrays_overlap(keys_in, vals_in, keys_out, vals_out, n)) return XPBD_ERR_INVALID_ARGUMENT;
     cudaError_t e = radix_sort_pairs(keys_in, vals_in, keys_out, vals_out, n, passes, scratch, scratch_bytes,
                                      (cudaStream_t)stream, nullptr);
     return e == cudaSuccess ? XPBD_OK : XPBD_ERR_CUDA;

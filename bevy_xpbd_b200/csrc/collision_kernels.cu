@@ -202,7 +202,8 @@ cudaError_t launch_exclusive_scan(uint32_t* a, uint32_t m, uint32_t* total, cuda
 }
 
 size_t radix_sort_scratch_bytes(uint32_t n) {
-    size_t tiles = (n + kSortTile - 1) / kSortTile;
+    if (n > XPBD_RADIX_SORT_MAX_KEYS) return 0;
+    size_t tiles = ((size_t)n + kSortTile - 1) / kSortTile;
     if (tiles == 0) tiles = 1;
     size_t counts = 256 * tiles * sizeof(uint32_t);
     size_t tmp = 2 * (size_t)n * sizeof(uint32_t);  // ping-pong keys/vals for even pass counts
@@ -212,10 +213,10 @@ size_t radix_sort_scratch_bytes(uint32_t n) {
 cudaError_t radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                              uint32_t* vals_out, uint32_t n, uint32_t passes, void* scratch, size_t scratch_bytes,
                              cudaStream_t st, uint64_t* launches) {
-    if (passes < 1 || passes > 4) return cudaErrorInvalidValue;
+    if (passes < 1 || passes > 4 || n > XPBD_RADIX_SORT_MAX_KEYS) return cudaErrorInvalidValue;
     if (n == 0) return cudaSuccess;
     if (scratch_bytes < radix_sort_scratch_bytes(n)) return cudaErrorInvalidValue;
-    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    const uint32_t tiles = (uint32_t)(((size_t)n + kSortTile - 1) / kSortTile);  // <= 2^20 for n <= 2^31
     size_t counts_bytes = ((256 * (size_t)tiles * sizeof(uint32_t)) + 255) & ~(size_t)255;
     uint32_t* counts = (uint32_t*)scratch;
     uint32_t* tmp_k = (uint32_t*)((char*)scratch + counts_bytes);
@@ -248,21 +249,50 @@ constexpr size_t noalloc_scratch_bytes(uint32_t n) {
 constexpr size_t kNoAllocScratchBytes = noalloc_scratch_bytes(XPBD_NOALLOC_SORT_MAX_KEYS);
 static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[kNoAllocScratchBytes];
 
-// Device address of the scratch array on the current device. The array's name is only a host-side stand-in, so the
-// address is looked up once per device (with that device current) and cached.
+// Identity of the current context (cuCtxGetId: unique over the process's lifetime, never reused), through the
+// runtime's driver entry points so that the library does not link libcuda; 0 when unavailable.
+static unsigned long long current_context_id() {
+    typedef int (*CtxGetCurrent)(void**);
+    typedef int (*CtxGetId)(void*, unsigned long long*);
+    static CtxGetCurrent get_current = nullptr;
+    static CtxGetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (CtxGetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetId)f;
+    });
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of the scratch array in the current context. The array's name is only a host-side stand-in, so the
+// address is looked up with the device current and cached per device together with the context it belongs to; a
+// re-created context (after cudaDeviceReset) gets a fresh lookup.
 static cudaError_t noalloc_scratch(void** out) {
     static std::mutex mu;
     static void* cache[64] = {nullptr};
+    static unsigned long long cache_ctx[64] = {0};
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(mu);
-    if (!cache[dev]) {
+    const unsigned long long ctx = current_context_id();  // 0 before the runtime made a context current
+    if (!cache[dev] || ctx == 0 || cache_ctx[dev] != ctx) {
         void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
+        e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);  // makes the device's context current if needed
         if (e != cudaSuccess) return e;
         cache[dev] = p;
+        cache_ctx[dev] = current_context_id();
     }
     *out = cache[dev];
     return cudaSuccess;
@@ -561,11 +591,23 @@ cudaError_t collision_pairs(const XpbdWorld& W, const float4* pos, const Collisi
 
 }  // namespace xpbd
 
+// True when the output arrays of a sort of n keys overlap each other or an input array.
+bool xpbd_sort_arrays_overlap(const void* keys_in, const void* vals_in, const void* keys_out, const void* vals_out,
+                              uint32_t n) {
+    const uintptr_t b = 4 * (uintptr_t)n;
+    auto meet = [b](const void* p, const void* q) {
+        const uintptr_t a = (uintptr_t)p, c = (uintptr_t)q;
+        return a < c + b && c < a + b;
+    };
+    return meet(keys_out, vals_out) || meet(keys_out, keys_in) || meet(keys_out, vals_in) ||
+           meet(vals_out, keys_in) || meet(vals_out, vals_in);
+}
+
 extern "C" int xpbd_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                              uint32_t* vals_out, uint32_t n, uint32_t passes, void* stream) {
     if (n && (!keys_in || !vals_in || !keys_out || !vals_out)) return XPBD_ERR_INVALID_ARGUMENT;
     if (passes < 1 || passes > 4) return XPBD_ERR_INVALID_ARGUMENT;
-    if (keys_in == keys_out || vals_in == vals_out) return XPBD_ERR_INVALID_ARGUMENT;
+    if (n && xpbd_sort_arrays_overlap(keys_in, vals_in, keys_out, vals_out, n)) return XPBD_ERR_INVALID_ARGUMENT;
     if (n > XPBD_NOALLOC_SORT_MAX_KEYS) return XPBD_ERR_CAPACITY;
     if (n == 0) return XPBD_OK;
     void* scratch = nullptr;

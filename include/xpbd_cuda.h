@@ -240,7 +240,10 @@ int xpbd_collision_pairs(xpbd_ctx* ctx, uint32_t* pairs, uint64_t cap, uint64_t*
 
 /* ---- standalone device primitives (device pointers, caller stream) ----------------------------------------- */
 /* Stable LSD radix sort of 32-bit keys with 32-bit payload, 8-bit digits, `passes` (1..4) passes from the least
- * significant digit. keys_in/vals_in are not modified. `scratch` must hold xpbd_radix_sort_scratch_bytes(n). */
+ * significant digit. keys_in/vals_in are not modified. `scratch` must hold xpbd_radix_sort_scratch_bytes(n).
+ * n may be at most XPBD_RADIX_SORT_MAX_KEYS (larger n: XPBD_ERR_CAPACITY, and a scratch size of 0). The two output
+ * arrays must not overlap each other or either input array (XPBD_ERR_INVALID_ARGUMENT); the inputs may overlap. */
+#define XPBD_RADIX_SORT_MAX_KEYS (1u << 31)
 size_t xpbd_radix_sort_scratch_bytes(uint32_t n);
 int xpbd_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
                           uint32_t n, uint32_t passes, void* scratch, size_t scratch_bytes, void* stream);
@@ -249,9 +252,11 @@ int xpbd_radix_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint
  * application that reserves all device memory through its own pool, or in a plugin that may not grow the process's
  * footprint). No counterpart in the reference. It allocates nothing: its scratch is a fixed device array built into
  * the library, sized for at most XPBD_NOALLOC_SORT_MAX_KEYS keys (about 2.2 MB, held on every GPU that loads the
- * library until the process exits); larger n returns XPBD_ERR_CAPACITY. The first call on a device looks up the
- * array's device address (make it before any stream capture on that device). Every call shares the one array, so
- * calls whose work overlaps on the GPU (other streams, other host threads) race; serialise them. */
+ * library until the process exits); larger n returns XPBD_ERR_CAPACITY. The array overlap rules are those of
+ * xpbd_radix_sort_pairs. The first call on a device looks up the array's device address in the current context
+ * (make it before any stream capture on that device); after the context is re-created (cudaDeviceReset), the next
+ * call looks it up again. Every call shares the one array, so calls whose work overlaps on the GPU (other streams,
+ * other host threads) race; serialise them. */
 #define XPBD_NOALLOC_SORT_MAX_KEYS (1u << 18)
 int xpbd_radix_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
                                   uint32_t* vals_out, uint32_t n, uint32_t passes, void* stream);

@@ -172,7 +172,7 @@ class OracleSim:
     """Single cloth, FP32 (fp64=False: the reference's arithmetic) or FP64 accuracy build."""
 
     def __init__(self, x, inv_mass, ci, cj, rest, comp, v=None, rest_pos=None, ctype=None, fp64=False):
-        L = lib()
+        L = self.L = lib()
         self.n = len(inv_mass)
         self.e = len(ci)
         keep = [np.ascontiguousarray(x, np.float32).reshape(-1), np.ascontiguousarray(inv_mass, np.float32),
@@ -186,60 +186,60 @@ class OracleSim:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().oracle_sim_free(self.h)
+            self.L.oracle_sim_free(self.h)
             self.h = None
 
     def set_params(self, params: dict):
         self._p = make_params(params)
-        lib().oracle_sim_set_params(self.h, C.byref(self._p))
+        self.L.oracle_sim_set_params(self.h, C.byref(self._p))
 
     def substeps(self, count: int, brute_force: bool = False):
-        lib().oracle_sim_substeps(self.h, count, int(brute_force))
+        self.L.oracle_sim_substeps(self.h, count, int(brute_force))
 
     def substeps_converge(self, count: int):
         """Convergence solve (extension); returns (update passes, fallback flag) per substep."""
         it = np.zeros(count, np.uint32)
         fb = np.zeros(count, np.uint32)
-        lib().oracle_sim_substeps_converge(self.h, count, _ptr(it), _ptr(fb))
+        self.L.oracle_sim_substeps_converge(self.h, count, _ptr(it), _ptr(fb))
         return it, fb
 
     def state(self):
         x = np.zeros((self.n, 3), np.float64)
         v = np.zeros((self.n, 3), np.float64)
-        lib().oracle_sim_get(self.h, _ptr(x), _ptr(v))
+        self.L.oracle_sim_get(self.h, _ptr(x), _ptr(v))
         return x, v
 
     def set_state(self, x=None, v=None):
         xx = None if x is None else np.ascontiguousarray(x, np.float32).reshape(-1)
         vv = None if v is None else np.ascontiguousarray(v, np.float32).reshape(-1)
-        lib().oracle_sim_set_state(self.h, _ptr(xx), _ptr(vv))
+        self.L.oracle_sim_set_state(self.h, _ptr(xx), _ptr(vv))
 
     def predicted(self):
         """Positions after the next substep's prediction step (xpbd_cpu.rs:251-260), state unchanged."""
         out = np.zeros((self.n, 3), np.float64)
-        lib().oracle_sim_predicted(self.h, out.reshape(-1))
+        self.L.oracle_sim_predicted(self.h, out.reshape(-1))
         return out
 
     def lambdas(self):
         out = np.zeros(self.e, np.float64)
-        lib().oracle_sim_get_lambda(self.h, out)
+        self.L.oracle_sim_get_lambda(self.h, out)
         return out
 
     def set_warm_lambda(self, lam):
         self._warm = None if lam is None else np.ascontiguousarray(lam, np.float32)
-        lib().oracle_sim_set_warm_lambda(self.h, _ptr(self._warm))
+        self.L.oracle_sim_set_warm_lambda(self.h, _ptr(self._warm))
 
     def set_batches(self, offsets):
         """Color-batch offsets of the (batch-sorted) constraints: lets the OpenMP build sweep a batch in parallel."""
         self._batches = np.ascontiguousarray(offsets, np.uint32)
-        lib().oracle_sim_set_batches(self.h, _ptr(self._batches), len(self._batches) - 1)
+        self.L.oracle_sim_set_batches(self.h, _ptr(self._batches), len(self._batches) - 1)
 
     def strain_residual(self) -> float:
-        return float(lib().oracle_sim_strain_residual(self.h))
+        return float(self.L.oracle_sim_strain_residual(self.h))
 
     def collision_pairs(self, cap: int = 1 << 22):
         buf = np.zeros(2 * cap, np.uint32)
-        cnt = int(lib().oracle_sim_collision_pairs(self.h, buf, cap))
+        cnt = int(self.L.oracle_sim_collision_pairs(self.h, buf, cap))
         if cnt > cap:
             return self.collision_pairs(cnt)
         return buf[: 2 * cnt].reshape(-1, 2).copy()

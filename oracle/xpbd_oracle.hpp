@@ -14,8 +14,9 @@
 //
 // Pinning: the reference cannot be built here (Rust toolchain and its crates.io dependencies are absent), and it
 // ships no golden vectors. The restatement is pinned by porting every known-answer and invariant test of the
-// reference for this path (xpbd_cpu.rs:751-1128, cloth_compute.rs:1528-1577) plus the reference asset
-// assets/cloth.obj parsed through parse_welded_obj; see tests/test_oracle_reference_tests.py.
+// reference for this path (xpbd_cpu.rs:751-1128, cloth_compute.rs:1528-1577; tests/test_oracle_reference_tests.py)
+// and by the reference's one input fixture, assets/cloth.obj (copied to tests/golden/), whose parse_welded_obj result
+// is checked against the structure the reference source implies (tests/test_golden_cpu.py).
 //
 // Additions that have no reference counterpart (marked "extension"): per-substep λ mode, degree-averaged
 // Jacobi relaxation, strain residual, the spatial-hash collision specification (prime hash, stable LSD radix

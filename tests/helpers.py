@@ -17,13 +17,23 @@ def oracle_params(params: P.XpbdCpuTimeStepParams, cfg: P.ClothSimConfig) -> dic
     return d
 
 
-def oracle_sim(spec, params, cfg, fp64=False, order_by_index=False):
-    """Oracle fed the batch-sorted constraints (as finalize_cloth_mesh hands them to the solver)."""
-    perm, _, _ = orc.partition(spec.num_particles, spec.constraint_i, spec.constraint_j, order_by_index)
-    s = orc.OracleSim(spec.positions, spec.inv_mass, spec.constraint_i[perm], spec.constraint_j[perm],
-                      spec.rest_len[perm], spec.compliance[perm], v=spec.velocities, rest_pos=spec.rest_positions,
-                      ctype=spec.constraint_type[perm], fp64=fp64)
+def oracle_sim(spec, params, cfg, fp64=False, order_by_index=False, omp=False):
+    """Oracle fed the batch-sorted constraints (as finalize_cloth_mesh hands them to the solver). omp=True builds it
+    on the OpenMP library (independent loops and each color batch in parallel; bit-identical to the serial build,
+    tests/test_host_cpu.py), for the full-size comparisons."""
+    perm, _, offs = orc.partition(spec.num_particles, spec.constraint_i, spec.constraint_j, order_by_index)
+    if omp:
+        orc.select("omp")
+    try:
+        s = orc.OracleSim(spec.positions, spec.inv_mass, spec.constraint_i[perm], spec.constraint_j[perm],
+                          spec.rest_len[perm], spec.compliance[perm], v=spec.velocities,
+                          rest_pos=spec.rest_positions, ctype=spec.constraint_type[perm], fp64=fp64)
+    finally:
+        if omp:
+            orc.select("serial")
     s.set_params(oracle_params(params, cfg))
+    if omp:
+        s.set_batches(offs)
     return s
 
 
@@ -45,3 +55,13 @@ def params_for(substeps=10, iterations=10, omega=1.0, drag=0.0, gravity=(0.0, -9
 
 def max_abs(a, b) -> float:
     return float(np.max(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64))))
+
+
+def folded_state(sp, gap=0.03):
+    """The sheet folded in half along its middle row: the upper half lies `gap` above the lower half."""
+    s = sp.side
+    x = sp.positions.reshape(s, s, 3).astype(np.float64).copy()
+    zf = x[s // 2, 0, 2]
+    x[s // 2:, :, 2] = 2 * zf - x[s // 2:, :, 2]
+    x[s // 2:, :, 1] += gap
+    return x.reshape(-1, 3).astype(np.float32)

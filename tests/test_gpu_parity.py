@@ -10,7 +10,7 @@ import pytest
 from bevy_xpbd_b200 import plugin as P
 from bevy_xpbd_b200 import workloads as wl
 from oracle import oracle as orc
-from tests.helpers import gpu_sim, max_abs, oracle_sim, params_for
+from tests.helpers import folded_state, gpu_sim, max_abs, oracle_sim, params_for
 
 pytestmark = pytest.mark.gpu
 
@@ -241,23 +241,13 @@ def test_self_collision_ring_filter_trajectory_bit_exact():
     assert plug.positions()[:, 1].min() >= 0.0
 
 
-def _folded_state(sp, gap=0.03):
-    """The sheet folded in half along its middle row: the upper half lies `gap` above the lower half."""
-    s = sp.side
-    x = sp.positions.reshape(s, s, 3).astype(np.float64).copy()
-    zf = x[s // 2, 0, 2]
-    x[s // 2:, :, 2] = 2 * zf - x[s // 2:, :, 2]
-    x[s // 2:, :, 1] += gap
-    return x.reshape(-1, 3).astype(np.float32)
-
-
 def test_hash_keys_sorted_order_and_pairs_bit_exact():
     """Spatial hash keys, stable 8-bit-digit LSD radix sort and the collision pair list of a folded sheet, then the
     collision-heavy trajectory from that state. The GPU sorts only the passes that cover the table's bits; the oracle
     runs all four, whose extra passes over all-zero digits leave the order unchanged."""
     sp, prm, cfg = _folding_sheet(64)
     plug = gpu_sim(sp, prm, cfg)
-    xf = _folded_state(sp)
+    xf = folded_state(sp)
     plug.write_state(xf, np.zeros_like(xf))
     x = plug.positions()
     assert np.array_equal(x, xf)

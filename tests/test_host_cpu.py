@@ -157,3 +157,24 @@ def test_bench_reports_committed_traffic_only_for_the_full_launch():
     assert not bench.make_workload("c3", 0, 1, c3_cloths=8)["full_launch"]
     assert not bench.make_workload("c3", 1, 2)["full_launch"]
     assert bench.make_workload("c0", 1, 2)["full_launch"]
+
+
+def test_sort_entry_points_refuse_overlap_and_oversize_before_touching_the_device():
+    """Argument checks of both sort entry points run on the host before any CUDA call (no device here): overlapping
+    output arrays, and more keys than the stated maximums."""
+    L = N.load()
+    n = 1000
+    base = 1 << 40  # fake device addresses: never dereferenced, the checks return first
+    ki, vi, ko, vo = base, base + 4 * n, base + 8 * n, base + 12 * n
+    big = L.xpbd_radix_sort_scratch_bytes(n)
+    assert big > 0
+    P = C.c_void_p
+    for a, b, c, d in [(ki, vi, ko, ko), (ki, vi, ki, vo), (ki, vi, vi, vo), (ki, vi, ko, ki), (ki, vi, ko, vi),
+                       (ki, vi, ko, ko + 4 * n - 4), (ki, vi, vi - 4, vo)]:
+        assert L.xpbd_radix_sort_pairs(P(a), P(b), P(c), P(d), n, 4, P(base + (1 << 30)), big, None) == \
+            N.ERR_INVALID_ARGUMENT
+        assert L.xpbd_radix_sort_pairs_noalloc(P(a), P(b), P(c), P(d), n, 4, None) == N.ERR_INVALID_ARGUMENT
+    assert L.xpbd_radix_sort_scratch_bytes((1 << 31) + 1) == 0
+    far = [base + k * (1 << 36) for k in range(4)]  # disjoint for any n below 2^34
+    assert L.xpbd_radix_sort_pairs(*map(P, far), (1 << 31) + 1, 4, P(base), 1 << 40, None) == -9
+    assert L.xpbd_radix_sort_pairs_noalloc(*map(P, far), (1 << 18) + 1, 4, None) == -9

@@ -1,5 +1,6 @@
 """Multi-rank host logic on CPU (gloo, world size 2): the batch is sharded by cloth with no collective inside a step,
-every cloth is owned by exactly one rank, the shards are balanced, and timing is reduced as the max over ranks."""
+every cloth is owned by exactly one rank, the shards are balanced by constraint count, and timing is reduced as the
+max over ranks."""
 import os
 import socket
 
@@ -31,7 +32,7 @@ def _worker(rank: int, world: int, port: int, out):
         # max-over-ranks timing as bench.py reduces it (gloo has MAX too)
         t = torch.tensor([float(rank + 1)], dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        out[rank] = dict(seeds=sorted(torch.cat(gathered).tolist()), n=w["n"], total=w["total_cloths"],
+        out[rank] = dict(seeds=sorted(torch.cat(gathered).tolist()), n=w["n"], e=w["e"], total=w["total_cloths"],
                          tmax=float(t.item()), mine=len(ids))
     finally:
         dist.destroy_process_group()
@@ -53,5 +54,17 @@ def test_cloth_sharding_two_ranks():
     assert r0["seeds"] == r1["seeds"]                       # both ranks see the same global set
     assert len(set(r0["seeds"])) == 256 == r0["total"]      # every cloth exactly once
     assert r0["mine"] + r1["mine"] == 256
-    assert abs(r0["n"] - r1["n"]) / max(r0["n"], r1["n"]) < 0.15  # particle balance of the k % N split
+    assert abs(r0["e"] - r1["e"]) / max(r0["e"], r1["e"]) < 0.05  # constraint balance of the shards
     assert r0["tmax"] == r1["tmax"] == 2.0
+
+
+def test_shard_by_constraints_balances_and_covers():
+    from bevy_xpbd_b200 import workloads as wl
+    from bevy_xpbd_b200.sharding import shard_by_constraints
+    counts = [s.num_constraints for s in wl.config3_batch()]
+    for world in (1, 2, 4, 8):
+        shards = shard_by_constraints(counts, world)
+        assert sorted(k for s in shards for k in s) == list(range(len(counts)))
+        loads = [sum(counts[k] for k in s) for s in shards]
+        assert (max(loads) - min(loads)) / max(loads) < 0.05, (world, loads)
+    assert shard_by_constraints([5, 3, 3, 1], 2) == [[0, 3], [1, 2]]
