@@ -90,9 +90,16 @@ def make_workload(name: str, rank: int = 0, world: int = 1, c3_cloths: int = 0) 
     # algorithmic bytes per frame (fp32): S*(100N + I*(28N + 16E)) — per pass x read+write and inverse mass (28 B per
     # particle) plus i, j, rest, compliance (16 B per constraint); per substep 100 B per particle for predict + velocity
     bytes_alg = S * (100 * n + I * (28 * n + 16 * e))
+    if cfg.collision:
+        # self collision every substep, 124 B per particle: hash keys (read x 16, write key + value 8), three 8-bit
+        # radix passes (histogram reads keys 4, scatter reads and writes key + value 16 -> 60), bucket starts (read
+        # sorted keys 4, write 4), resolve (read and write the position once each, 32)
+        bytes_alg += S * 124 * n
     full_launch = name != "c3" or (not c3_cloths and world == 1)
+    # c2 is timed after the sheet has folded onto the ground (60 untimed frames of the 240), not during the free fall
+    pre_frames = 60 if name == "c2" else 0
     return dict(name=name, specs=specs, params=prm, cfg=cfg, desc=desc, n=n, e=e, cloths=len(specs),
-                total_cloths=total_cloths, bytes_per_frame=bytes_alg, full_launch=full_launch)
+                total_cloths=total_cloths, bytes_per_frame=bytes_alg, full_launch=full_launch, pre_frames=pre_frames)
 
 
 _CONFIGS: dict = {}
@@ -258,6 +265,8 @@ def time_device(w: dict, plug, steps: int, warmup: int, world: int, device: int,
     stream = torch.cuda.Stream()  # a real stream handle: the library launches on it, the events are recorded on it
     plug.set_stream(stream.cuda_stream)
     flush_buf = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda") if flush else None
+    if w.get("pre_frames"):
+        plug.step(frames=w["pre_frames"])
     for _ in range(warmup):
         plug.step(frames=1)
     plug.sync()
@@ -352,7 +361,8 @@ def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks:
     mean_ms = total_ms / steps
     cloth_steps = w["total_cloths"] * steps
     kernel = {0: "jacobi_persistent_kernel", 1: "gs_persistent_kernel", 2: "jacobi_patch_kernel",
-              3: "gs_cluster_kernel", 5: "jacobi_row_kernel", 6: "jacobi_converge_kernel"}[st["solver_kernel"]]
+              3: "gs_cluster_kernel", 5: "jacobi_row_kernel", 6: "jacobi_converge_kernel",
+              7: "jacobi_cloth_kernel"}[st["solver_kernel"]]
     res = {
         "value": round(cloth_steps / (total_ms * 1e-3), 2),
         "ms_per_step": round(mean_ms, 4),
@@ -365,7 +375,7 @@ def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks:
                      "solver_kernel": kernel, "cluster_ctas": st["cluster_ctas"],
                      "cuda_graph": bool(st["graph_captured"]), "cooperative_launch": bool(st["cooperative_launch"]),
                      "setup_s": round(setup_s, 2)},
-        "roofline": roofline(w, mean_ms, kernel, peaks) if w["cfg"].collision == 0 else None,
+        "roofline": roofline(w, mean_ms, kernel, peaks),
         "clocks": clocks,
         "step_ms_min_max": [round(min(per), 4), round(max(per), 4)],
     }
@@ -374,6 +384,8 @@ def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks:
         res["e2e"] = {"value": round(cloth_steps / (e2e_ms * 1e-3), 2), "unit": UNIT,
                       "h2d_bytes_per_step": DEV_PARAMS_BYTES, "d2h_bytes_per_step": 12 * w["n"],
                       "ms_per_step": round(e2e_ms / steps, 4)}
+    if w["cloths"] == 1:
+        res["_state"] = (plug.positions(), plug.velocities())
     plug.close()
     res["_w"] = w
     return res
@@ -596,10 +608,11 @@ def run_prep_leg(device: int, reps: int = 5) -> dict:
 
 
 def cpu_oracle_run(w: dict, budget_s: float, max_cloths: int | None = None, min_frames: int = 1,
-                   variant: str = "omp", warmup_frames: int = 1):
+                   variant: str = "omp", warmup_frames: int = 1, state=None):
     """Times the CPU restatement of xpbd_cpu.rs (OpenMP build, or the serial build with the reference's loop order)
     on a bounded sample of workload `w`: every `len/max_cloths`-th cloth, as many whole frames as fit in `budget_s`
-    (at least `min_frames`), after `warmup_frames` untimed frames."""
+    (at least `min_frames`), after `warmup_frames` untimed frames. `state` = (positions, velocities) of a one-cloth
+    workload to start from (the GPU arm's state after its untimed frames)."""
     from oracle import oracle as orc
     from tests.helpers import oracle_params
     orc.select(variant)
@@ -614,6 +627,8 @@ def cpu_oracle_run(w: dict, budget_s: float, max_cloths: int | None = None, min_
                           ctype=sp.constraint_type[perm])
         s.set_params(oracle_params(w["params"], w["cfg"]))
         s.set_batches(offs)
+        if state is not None and len(specs) == 1:
+            s.set_state(state[0], state[1])
         sims.append(s)
     S = w["cfg"].solve_substeps
     for _ in range(max(warmup_frames, 1) - 1):  # untimed warm-up frames
@@ -669,6 +684,7 @@ def main():
     ap.add_argument("--no-warm", action="store_true", help="skip the learned-vs-plain convergence leg")
     ap.add_argument("--warm-frames", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-legs", action="store_true", help="skip the c0 and c2 legs")
     ap.add_argument("--no-prep", action="store_true", help="skip the mesh-preparation leg (GPU vs host coloring)")
     ap.add_argument("--c3-cloths", type=int, default=0, help="first K cloths of c3 only (profiling cases)")
     ap.add_argument("--no-autotune", action="store_true", help="library default schedule")
@@ -688,6 +704,7 @@ def main():
     peaks = load_peaks()
     main_res = run_gpu_workload(args.workload, args, rank, world, local, peaks, with_e2e=not args.no_e2e)
     w = main_res.pop("_w")
+    main_state = main_res.pop("_state", None)
     line = {"metric": METRIC, "value": main_res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": main_res["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -704,12 +721,31 @@ def main():
                            "config": b["config"], "schedule": b["schedule"], "roofline": b["roofline"],
                            "gpu_launches": b["gpu_launches"],
                            "clocks": b["clocks"]}
+    if world == 1 and not args.no_legs:
+        # the other single-sheet configurations: 32x32 Jacobi (c0) and the 512x512 self-collision sheet (c2)
+        for name in ("c0", "c2"):
+            if name == args.workload:
+                continue
+            r = run_gpu_workload(name, args, rank, world, local, peaks, with_e2e=True)
+            wx = r.pop("_w")
+            stx = r.pop("_state", None)
+            leg = {k: r[k] for k in ("value", "ms_per_step", "steps", "config", "schedule", "roofline", "e2e",
+                                     "gpu_launches", "clocks")}
+            leg["unit"] = UNIT
+            if not args.no_cpu_baseline:
+                c = cpu_oracle_run(wx, args.cpu_seconds / 2, state=stx)
+                leg["cpu_baseline"] = {"value": round(c["value"], 4), "unit": UNIT, "cores": c["cores"],
+                                       "kind": "port",
+                                       "sample": f"{c['frames']} frames, {c['seconds']:.1f} s, OpenMP build of the "
+                                                 "oracle" + (", from the GPU arm's final state" if stx else "")}
+            line[name] = leg
     if rank == 0 and world == 1 and not args.no_warm:
         line["warm_start"] = run_warm_leg(args, local)
     if rank == 0 and world == 1 and not args.no_prep:
         line["mesh_prep"] = run_prep_leg(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_oracle_run(w, args.cpu_seconds, max_cloths=16 if args.workload == "c3" else None)
+        r = cpu_oracle_run(w, args.cpu_seconds, max_cloths=16 if args.workload == "c3" else None,
+                           state=main_state if args.workload == "c2" else None)
         line["cpu_baseline"] = {"value": round(r["value"], 4), "unit": UNIT, "cores": r["cores"], "kind": "port",
                                 "sample": f"{r['frames']} frames of {r['cloths']} cloth(s) of the workload, "
                                           f"{r['seconds']:.1f} s, OpenMP build of the oracle"}

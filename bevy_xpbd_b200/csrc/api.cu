@@ -107,6 +107,14 @@ struct xpbd_ctx {
     float norm[XPBD_MLP_NORM] = {0};
     std::vector<XpbdGrab> grabs;  // per cloth (host copy)
     float forced_timeout_ms = 0.f;
+    // cloth-resident Jacobi (kernel id 7): per launch class the cloths it solves; side streams run the classes
+    // concurrently (fork / join events on the context stream)
+    bool wide_palette = false;       // a cloth has more than 16 compliance values: per-incidence compliances
+    bool cloth_ok = false, cloth_tried = false;
+    ClothSolveTable cloth_tab[kClothClasses] = {};
+    cudaStream_t cls_stream[kClothClasses] = {};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[kClothClasses] = {};
 };
 
 // ------------------------------------------------------------------------------------------------- helpers
@@ -237,6 +245,11 @@ extern "C" void xpbd_destroy(xpbd_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_device(ctx);
+    for (int t = 0; t < kClothClasses; ++t) {
+        if (ctx->cls_stream[t]) cudaStreamDestroy(ctx->cls_stream[t]);
+        if (ctx->ev_join[t]) cudaEventDestroy(ctx->ev_join[t]);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }
@@ -393,20 +406,15 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     std::vector<uint4> con_in(E);
     struct ClothTables {
         std::vector<uint2> inc;         // this cloth's incidences (rows in particle order)
+        std::vector<float> inc_comp;    // their compliances (only when some cloth has more than 16 values)
         std::vector<uint32_t> row_off;  // local row starts (n)
         bool palette_ok = true;
     };
     std::vector<ClothTables> ct(C);
+    // compliance palettes: up to 16 distinct values per cloth are named by 4 bits of the incidence record; a cloth
+    // with more makes the whole batch carry a per-incidence compliance array instead
     parallel_for(C, [&](uint32_t ci_) {
         ClothHost& c = ctx->cloths[ci_];
-        ClothTables& t = ct[ci_];
-        for (uint32_t i = 0; i < c.n; ++i) {
-            hx[c.vtx_off + i] = make_float4(c.pos[3 * i], c.pos[3 * i + 1], c.pos[3 * i + 2], c.w[i]);
-            hv[c.vtx_off + i] = make_float4(c.vel[3 * i], c.vel[3 * i + 1], c.vel[3 * i + 2], 0.f);
-            hrest[c.vtx_off + i] =
-                make_float4(c.rest_pos[3 * i], c.rest_pos[3 * i + 1], c.rest_pos[3 * i + 2], 0.f);
-        }
-        // compliance palette
         std::vector<float> pal;
         std::vector<uint32_t>& pidx = c.pal_idx;
         pidx.assign(c.e, 0);
@@ -421,7 +429,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
             }
             if (k == pal.size()) {
                 if (pal.size() == XPBD_PALETTE) {
-                    t.palette_ok = false;
+                    ct[ci_].palette_ok = false;
+                    pidx.assign(c.e, 0);
                     return;
                 }
                 pal.push_back(c.comp[e]);
@@ -429,6 +438,20 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
             pidx[e] = (uint32_t)k;
         }
         for (size_t k = 0; k < pal.size(); ++k) palette[(size_t)ci_ * XPBD_PALETTE + k] = pal[k];
+    });
+    bool wide = false;
+    for (uint32_t ci_ = 0; ci_ < C; ++ci_) wide = wide || !ct[ci_].palette_ok;
+    ctx->wide_palette = wide;
+    parallel_for(C, [&](uint32_t ci_) {
+        ClothHost& c = ctx->cloths[ci_];
+        ClothTables& t = ct[ci_];
+        for (uint32_t i = 0; i < c.n; ++i) {
+            hx[c.vtx_off + i] = make_float4(c.pos[3 * i], c.pos[3 * i + 1], c.pos[3 * i + 2], c.w[i]);
+            hv[c.vtx_off + i] = make_float4(c.vel[3 * i], c.vel[3 * i + 1], c.vel[3 * i + 2], 0.f);
+            hrest[c.vtx_off + i] =
+                make_float4(c.rest_pos[3 * i], c.rest_pos[3 * i + 1], c.rest_pos[3 * i + 2], 0.f);
+        }
+        const std::vector<uint32_t>& pidx = c.pal_idx;
         // batch-sorted constraints and the neighbour table in reference order
         std::vector<uint32_t> si(c.e), sj(c.e);
         for (uint32_t k = 0; k < c.e; ++k) {
@@ -452,6 +475,7 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
                 if (c.lambda_inc[e_in] == 0xFFFFFFFFu) c.lambda_inc[e_in] = (uint32_t)t.inc.size();
                 (c.ci[e_in] == i ? c.inc_i : c.inc_j)[e_in] = (uint32_t)t.inc.size();
                 t.inc.push_back(make_uint2((other[k] + c.vtx_off) | (pidx[e_in] << 28), rb));
+                if (wide) t.inc_comp.push_back(c.comp[e_in]);
             }
         }
         for (uint32_t e = 0; e < c.e; ++e) {
@@ -461,17 +485,16 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
             con_in[c.con_off + e] = make_uint4(c.ci[e] + c.vtx_off, c.cj[e] + c.vtx_off, rb, cb);
         }
     });
-    for (uint32_t ci_ = 0; ci_ < C; ++ci_)
-        if (!ct[ci_].palette_ok)
-            return fail(ctx, XPBD_ERR_UNSUPPORTED, "more than 16 distinct compliance values in one cloth");
     // cloth k's incidences start at the total of the cloths before it; each cloth copies and rebases its own slice
     std::vector<size_t> inc_base(C + 1, 0);
     for (uint32_t ci_ = 0; ci_ < C; ++ci_) inc_base[ci_ + 1] = inc_base[ci_] + ct[ci_].inc.size();
     inc.resize(inc_base[C]);
+    std::vector<float> inc_comp(wide ? inc_base[C] : 0);
     parallel_for(C, [&](uint32_t ci_) {
         ClothHost& c = ctx->cloths[ci_];
         ClothTables& t = ct[ci_];
         const uint32_t base = (uint32_t)inc_base[ci_];
+        if (wide) std::copy(t.inc_comp.begin(), t.inc_comp.end(), inc_comp.begin() + base);
         for (uint32_t i = 0; i < c.n; ++i) row_off[c.vtx_off + i] = base + t.row_off[i];
         for (uint32_t e = 0; e < c.e; ++e) {
             if (c.lambda_inc[e] != 0xFFFFFFFFu) c.lambda_inc[e] += base;
@@ -553,6 +576,8 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     ALLOC(roff_d, uint32_t, N + 1);
     ALLOC(inc_d, uint2, inc.size());
     ALLOC(lam_inc, float, inc.size());
+    float* inc_comp_d = nullptr;
+    if (wide) ALLOC(inc_comp_d, float, inc.size());
     ALLOC(tiles_d, XpbdTile, tiles.size());
     uint16_t* rcloth_d;
     ALLOC(rcloth_d, uint16_t, N);
@@ -625,6 +650,10 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     H2D(rest, hrest.data(), N * sizeof(float4));
     H2D(roff_d, row_off.data(), (N + 1) * sizeof(uint32_t));
     if (!inc.empty()) H2D(inc_d, inc.data(), inc.size() * sizeof(uint2));
+    if (wide && !inc.empty()) {
+        H2D(inc_comp_d, inc_comp.data(), inc.size() * sizeof(float));
+        CK(cudaStreamSynchronize(st), "commit sync");
+    }
     CK(cudaMemsetAsync(lam_inc, 0, std::max<size_t>(inc.size(), 1) * sizeof(float), st), "memset");
     H2D(tiles_d, tiles.data(), tiles.size() * sizeof(XpbdTile));
     {
@@ -681,6 +710,7 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     W.tiles = tiles_d;
     W.row_cloth = rcloth_d;
     W.palette_comp = pal_d;
+    W.inc_comp = inc_comp_d;
     W.con = con_d;
     W.con_lambda = lam_con;
     W.color_off = color_d;
@@ -793,6 +823,7 @@ static int ensure_patches(xpbd_ctx* ctx, bool* usable) {
     *usable = ctx->patches_ok;
     if (ctx->patches_ok || ctx->patches_tried) return XPBD_OK;
     ctx->patches_tried = true;
+    if (ctx->wide_palette) return XPBD_OK;  // patch records name a 4-bit palette entry
     const uint32_t C = (uint32_t)ctx->cloths.size();
     std::vector<PatchArrays> per(C);
     std::vector<std::vector<uint32_t>> slot(C);
@@ -931,6 +962,177 @@ static bool patches_usable(xpbd_ctx* ctx) {
     return usable;
 }
 
+// Tables of the cloth-resident Jacobi kernel, built on its first selection. Usable when every cloth fits a cluster
+// of at most 8 CTAs (XPBD_CLOTH_RANK_MAX particles per CTA) and its color batches are particle-disjoint (then each
+// particle's neighbour-table row is ordered by color, which the kernel's summation order relies on); otherwise the
+// schedule keeps the thread-per-particle kernel and the reason is left in last_error.
+static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
+    *usable = ctx->cloth_ok;
+    if (ctx->cloth_tried) return XPBD_OK;
+    ctx->cloth_tried = true;
+    const uint32_t C = (uint32_t)ctx->cloths.size();
+    std::vector<int> cls(C, -1);
+    std::vector<uint32_t> q(C, 0), ncol(C, 0);
+    std::vector<std::vector<uint32_t>> seg(C);
+    std::vector<std::vector<uint2>> rec(C);
+    std::vector<std::vector<float>> comp(C);
+    std::atomic<int> bad{0};  // 1: a cloth too large, 2: batches share a particle
+    parallel_for(C, [&](uint32_t k) {
+        const ClothHost& c = ctx->cloths[k];
+        int id = -1;
+        for (int t = 0; t < kClothClasses; ++t)
+            if ((uint64_t)kClothClass[t].cl * kClothClass[t].rank_cap >= c.n) {
+                id = t;
+                break;
+            }
+        if (id < 0) {
+            bad = 1;
+            return;
+        }
+        const uint32_t cl = kClothClass[id].cl;
+        const uint32_t qq = std::max<uint32_t>(1, (c.n + cl - 1) / cl);
+        const uint32_t nb = (uint32_t)c.batch_off.size() - 1;
+        std::vector<uint32_t> stamp(c.n, 0xFFFFFFFFu);
+        for (uint32_t b = 0; b < nb; ++b)
+            for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
+                const uint32_t e = c.perm[t], i = c.ci[e], j = c.cj[e];
+                if (stamp[i] == b || (j != i && stamp[j] == b)) {
+                    bad = 2;
+                    return;
+                }
+                stamp[i] = b;
+                stamp[j] = b;
+            }
+        // records of constraints with an unpinned endpoint, grouped by (batch, rank owning endpoint i)
+        std::vector<uint32_t>& sg = seg[k];
+        sg.assign((size_t)nb * cl + 1, 0);
+        for (uint32_t b = 0; b < nb; ++b)
+            for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
+                const uint32_t e = c.perm[t];
+                if (c.w[c.ci[e]] <= 0.f && c.w[c.cj[e]] <= 0.f) continue;
+                ++sg[(size_t)b * cl + c.ci[e] / qq + 1];
+            }
+        for (size_t x = 1; x < sg.size(); ++x) sg[x] += sg[x - 1];
+        std::vector<uint32_t> cur(sg.begin(), sg.end() - 1);
+        rec[k].resize(sg.back());
+        comp[k].resize(sg.back());
+        auto ep = [qq](uint32_t p) { return ((p / qq) << XPBD_CLOTH_EP_BITS) | (p % qq); };
+        for (uint32_t b = 0; b < nb; ++b)
+            for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
+                const uint32_t e = c.perm[t];
+                if (c.w[c.ci[e]] <= 0.f && c.w[c.cj[e]] <= 0.f) continue;
+                const uint32_t at = cur[(size_t)b * cl + c.ci[e] / qq]++;
+                uint32_t rb;
+                memcpy(&rb, &c.rest[e], 4);
+                rec[k][at] = make_uint2(ep(c.ci[e]) | (ep(c.cj[e]) << 16), rb);
+                comp[k][at] = c.comp[e];
+            }
+        cls[k] = id;
+        q[k] = qq;
+        ncol[k] = nb;
+    });
+    if (bad) {
+        ctx->last_error = bad == 1 ? "cloth-resident Jacobi: a cloth exceeds 8 CTAs of shared memory"
+                                   : "cloth-resident Jacobi: a color batch shares a particle";
+        return XPBD_OK;
+    }
+    // concatenate in cloth order
+    std::vector<XpbdClothDesc> desc(C);
+    std::vector<size_t> rbase(C + 1, 0), sbase(C + 1, 0);
+    for (uint32_t k = 0; k < C; ++k) {
+        rbase[k + 1] = rbase[k] + rec[k].size();
+        sbase[k + 1] = sbase[k] + seg[k].size();
+    }
+    if (rbase[C] >= 0xFFFFFFFFull || sbase[C] >= 0xFFFFFFFFull) {
+        ctx->last_error = "cloth-resident Jacobi: more than 2^32 records";
+        return XPBD_OK;
+    }
+    std::vector<uint2> all_rec(rbase[C]);
+    std::vector<float> all_comp(rbase[C]);
+    std::vector<uint32_t> all_seg(sbase[C]);
+    parallel_for(C, [&](uint32_t k) {
+        const ClothHost& c = ctx->cloths[k];
+        std::copy(rec[k].begin(), rec[k].end(), all_rec.begin() + rbase[k]);
+        std::copy(comp[k].begin(), comp[k].end(), all_comp.begin() + rbase[k]);
+        for (size_t x = 0; x < seg[k].size(); ++x) all_seg[sbase[k] + x] = (uint32_t)(seg[k][x] + rbase[k]);
+        desc[k] = XpbdClothDesc{c.vtx_off, c.n, q[k], ncol[k], (uint32_t)sbase[k], kClothClass[cls[k]].cl, {0, 0}};
+    });
+    // one launch per class, largest cloths first
+    std::vector<uint32_t> order;
+    uint32_t count[kClothClasses] = {0}, first[kClothClasses] = {0}, cap[kClothClasses] = {0};
+    for (int t = 0; t < kClothClasses; ++t) {
+        first[t] = (uint32_t)order.size();
+        std::vector<uint32_t> mine;
+        for (uint32_t k = 0; k < C; ++k)
+            if (cls[k] == t) mine.push_back(k);
+        std::stable_sort(mine.begin(), mine.end(),
+                         [&](uint32_t a, uint32_t b) { return ctx->cloths[a].n > ctx->cloths[b].n; });
+        for (uint32_t k : mine) cap[t] = std::max(cap[t], q[k]);
+        count[t] = (uint32_t)mine.size();
+        order.insert(order.end(), mine.begin(), mine.end());
+    }
+    cudaError_t err = cudaSuccess;
+    XpbdClothDesc* d_desc = dev_alloc<XpbdClothDesc>(ctx, C, &err);
+    uint32_t* d_seg = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, all_seg.size(), &err) : nullptr;
+    uint2* d_rec = err == cudaSuccess ? dev_alloc<uint2>(ctx, all_rec.size(), &err) : nullptr;
+    float* d_comp = err == cudaSuccess ? dev_alloc<float>(ctx, all_comp.size(), &err) : nullptr;
+    uint32_t* d_order = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, order.size(), &err) : nullptr;
+    if (err != cudaSuccess) return cuda_fail(ctx, err, "cloth-resident tables");
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(d_desc, desc.data(), C * sizeof(XpbdClothDesc), cudaMemcpyHostToDevice, st), "upload");
+    CK(cudaMemcpyAsync(d_seg, all_seg.data(), all_seg.size() * 4, cudaMemcpyHostToDevice, st), "upload");
+    if (!all_rec.empty()) {
+        CK(cudaMemcpyAsync(d_rec, all_rec.data(), all_rec.size() * sizeof(uint2), cudaMemcpyHostToDevice, st),
+           "upload");
+        CK(cudaMemcpyAsync(d_comp, all_comp.data(), all_comp.size() * 4, cudaMemcpyHostToDevice, st), "upload");
+    }
+    CK(cudaMemcpyAsync(d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st), "upload");
+    CK(cudaStreamSynchronize(st), "upload sync");
+    CK(cloth_kernel_prepare(), "cloth kernel attributes");
+    for (int t = 0; t < kClothClasses; ++t) {
+        ctx->cloth_tab[t] = ClothSolveTable{d_desc, d_seg, d_rec, d_comp, d_order + first[t], count[t], cap[t]};
+        if (!ctx->cls_stream[t]) CK(cudaStreamCreateWithFlags(&ctx->cls_stream[t], cudaStreamNonBlocking), "stream");
+        if (!ctx->ev_join[t]) CK(cudaEventCreateWithFlags(&ctx->ev_join[t], cudaEventDisableTiming), "event");
+    }
+    if (!ctx->ev_fork) CK(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming), "event");
+    ctx->cloth_ok = true;
+    *usable = true;
+    return XPBD_OK;
+}
+
+static bool cloth_kernel_usable(xpbd_ctx* ctx) {
+    bool usable = false;
+    if (ensure_cloth_tables(ctx, &usable) != XPBD_OK) return false;
+    return usable;
+}
+
+// Launches the frame of the cloth-resident kernel: the class launches fork off the context stream onto their own
+// streams (largest class on the context stream itself) and join back.
+static cudaError_t launch_cloth_frame(xpbd_ctx* ctx, uint32_t substeps, cudaStream_t st, uint64_t* launches) {
+    cudaError_t e = cudaEventRecord(ctx->ev_fork, st);
+    if (e != cudaSuccess) return e;
+    bool on_main = false;
+    for (int t = kClothClasses - 1; t >= 0; --t) {
+        const ClothSolveTable& T = ctx->cloth_tab[t];
+        if (T.count == 0) continue;
+        cudaStream_t s = on_main ? ctx->cls_stream[t] : st;
+        if (on_main) {
+            e = cudaStreamWaitEvent(s, ctx->ev_fork, 0);
+            if (e != cudaSuccess) return e;
+        }
+        e = launch_cloth_jacobi(t, ctx->W, T, substeps, s);
+        *launches += 1;
+        if (e != cudaSuccess) return e;
+        if (on_main) {
+            e = cudaEventRecord(ctx->ev_join[t], s);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ctx->ev_join[t], 0);
+            if (e != cudaSuccess) return e;
+        }
+        on_main = true;
+    }
+    return cudaSuccess;
+}
+
 static void choose_schedule(xpbd_ctx* ctx) {
     uint32_t block = ctx->opts.block_threads ? ctx->opts.block_threads : 256;
     if (block != 128 && block != 256 && block != 512 && block != 1024) block = 256;
@@ -945,6 +1147,27 @@ static void choose_schedule(xpbd_ctx* ctx) {
         ctx->stats.block_threads = cblock;
         ctx->stats.solver_kernel = 3;
         ctx->stats.cluster_ctas = ctx->cl;
+        return;
+    }
+    const bool plain_jacobi = ctx->opts.solver == XPBD_SOLVER_JACOBI && !(ctx->opts.tolerance > 0.f) &&
+                              !ctx->opts.warm_start;
+    const bool cloth_eligible = plain_jacobi && ctx->opts.lambda_mode == XPBD_LAMBDA_RESET_PER_ITERATION &&
+                                ctx->opts.collision == XPBD_COLLISION_NONE;
+    if (cloth_eligible && (ctx->opts.jacobi_kernel == 0 || ctx->opts.jacobi_kernel == 4) &&
+        cloth_kernel_usable(ctx)) {
+        ctx->kernel = 7;
+        uint32_t blocks = 0, maxcl = 1;
+        for (int t = 0; t < kClothClasses; ++t) {
+            blocks += ctx->cloth_tab[t].count * kClothClass[t].cl;
+            if (ctx->cloth_tab[t].count) maxcl = std::max(maxcl, kClothClass[t].cl);
+        }
+        ctx->block = 1024;
+        ctx->grid = blocks;
+        ctx->coop = false;
+        ctx->stats.grid_blocks = blocks;
+        ctx->stats.block_threads = 1024;
+        ctx->stats.solver_kernel = 7;
+        ctx->stats.cluster_ctas = maxcl;
         return;
     }
     if (ctx->opts.solver == XPBD_SOLVER_JACOBI && (ctx->opts.tolerance > 0.f || ctx->opts.warm_start))
@@ -1058,6 +1281,7 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
         }
         return cudaSuccess;
     }
+    if (ctx->kernel == 7) return launch_cloth_frame(ctx, S, st, launches);  // no collision (choose_schedule)
     if (!coll) {
         e = launch_substeps(ctx, kEndFinalize, S, 0, 0, st);
         *launches += 1;
@@ -1557,6 +1781,10 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
             for (int bps = 1; bps <= maxb; bps *= 2) cands.push_back({blk, (uint32_t)bps, 1, jk});
         }
     }
+    if (base.solver == XPBD_SOLVER_JACOBI && !(base.tolerance > 0.f || base.warm_start) &&
+        base.lambda_mode == XPBD_LAMBDA_RESET_PER_ITERATION && base.collision == XPBD_COLLISION_NONE &&
+        cloth_kernel_usable(ctx))
+        cands.push_back({0, 0, 1, 4});  // cloth-resident kernel (its launch shapes are fixed per cloth size)
     if (base.solver == XPBD_SOLVER_GAUSS_SEIDEL && base.cluster_ctas != 1)
         for (uint32_t cl : {16u, 8u})
             for (uint32_t blk : {512u, 1024u}) cands.push_back({blk, 0, cl, 0});

@@ -1,0 +1,236 @@
+// Cloth-resident Jacobi for sm_100a: a whole frame of the reference's Jacobi substeps per cloth, the cloth held in
+// shared memory, each constraint solved once per pass.
+//
+// Reference: predict (xpbd_cpu.rs:38-65), jacobi_edges_pass + jacobi_gather_particle (xpbd_cpu.rs:139-226, WGSL
+// jacobi_edges / jacobi_gather, cloth_sim_jacobi.wgsl:143-218) with λ cleared before every pass (xpbd_cpu.rs:267),
+// post_velocity (xpbd_cpu.rs:393-409).
+//
+// Layout. A cloth is solved by one CTA, or by a thread-block cluster of up to 8 CTAs whose distributed shared
+// memory holds it: rank r owns a contiguous range of the cloth's particles and keeps, per particle, its position
+// (float4, w = inverse mass) and its correction sum (float4, w = incidence count). Positions and velocities leave
+// shared memory only at substep boundaries (x, v in global memory). The constraint records stream from global memory
+// (8 bytes + the compliance per constraint and pass), grouped by (color, rank).
+//
+// Order of the sums. The reference gathers each particle's corrections in its neighbour-table row, which lists the
+// particle's constraints in increasing batch-sorted index (the cursor scatter of mesh_prep.rs:588-635). The batches
+// are greedy colors, so a particle meets at most one constraint per color and its row is sorted by color. Solving the
+// colors one after another — every constraint of color c solved once, its two terms added to its two endpoints'
+// sums, a CTA / cluster barrier between colors — therefore adds each particle's terms in exactly the row's order,
+// bit for bit, without atomics and without solving a constraint twice. A constraint's Δλ and |d| are the same from
+// either endpoint and n̂ changes sign exactly, so the j endpoint's term is the negated i term (x − t == x + (−t)).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "xpbd_cluster.h"
+#include "xpbd_device.h"
+#include "xpbd_fpdiv.h"
+#include "xpbd_internal.h"
+#include "xpbd_kernels.h"
+
+namespace xpbd {
+
+// cl, threads per CTA, particles per rank: the first class whose cl · rank_cap holds a cloth takes it. The single-CTA
+// classes fit four, two and one CTA per SM in its 228 KB of shared memory.
+const ClothClass kClothClass[kClothClasses] = {
+    {1, 256, 1760}, {1, 512, 3520}, {1, 1024, XPBD_CLOTH_RANK_MAX},
+    {2, 1024, XPBD_CLOTH_RANK_MAX}, {4, 1024, XPBD_CLOTH_RANK_MAX}, {8, 1024, XPBD_CLOTH_RANK_MAX}};
+
+size_t cloth_kernel_smem_bytes(uint32_t cap) { return 2 * (size_t)cap * sizeof(float4); }
+
+template <int CL>
+__device__ __forceinline__ void cloth_sync() {
+    if (CL == 1)
+        __syncthreads();
+    else
+        cluster_sync();
+}
+
+// Shared-memory address of endpoint `ep` ((rank << 13) | local) in the array starting at `base` of every CTA.
+template <int CL>
+__device__ __forceinline__ float4 ld_ep(uint32_t base, uint32_t ep, uint32_t rank) {
+    const uint32_t a = base + (ep & ((1u << XPBD_CLOTH_EP_BITS) - 1u)) * 16u;
+    if (CL == 1) return ld_local(a);
+    const uint32_t r = ep >> XPBD_CLOTH_EP_BITS;
+    return r == rank ? ld_local(a) : ld_dsmem(map_rank(a, r));
+}
+template <int CL>
+__device__ __forceinline__ void add_ep(uint32_t base, uint32_t ep, uint32_t rank, float tx, float ty, float tz,
+                                       bool negate) {
+    const uint32_t a = base + (ep & ((1u << XPBD_CLOTH_EP_BITS) - 1u)) * 16u;
+    const uint32_t r = CL == 1 ? 0u : ep >> XPBD_CLOTH_EP_BITS;
+    const bool local = CL == 1 || r == rank;
+    const uint32_t ra = local ? a : map_rank(a, r);
+    float4 s = local ? ld_local(a) : ld_dsmem(ra);
+    if (negate) {
+        s.x = __fsub_rn(s.x, tx);
+        s.y = __fsub_rn(s.y, ty);
+        s.z = __fsub_rn(s.z, tz);
+    } else {
+        s.x = __fadd_rn(s.x, tx);
+        s.y = __fadd_rn(s.y, ty);
+        s.z = __fadd_rn(s.z, tz);
+    }
+    if (local)
+        st_local(a, s);
+    else
+        st_dsmem(ra, s);
+}
+
+// One constraint of the current color: the reference's Δλ (λ = 0), then (n̂·w_i)·Δλ into i's sum and the negated
+// (n̂·w_j)·Δλ into j's. Nothing is added for a pinned endpoint (its row is empty), for |d| < 1e-8 or w sum < 1e-8
+// (the reference skips the constraint / has Δλ = 0: its term is zero, which leaves a sum started at +0 unchanged).
+template <int CL>
+__device__ __forceinline__ void solve_record(uint2 r, float comp, uint32_t pos_base, uint32_t acc_base,
+                                             uint32_t rank, float inv_dt_sq) {
+    const uint32_t ei = r.x & 0xFFFFu, ej = r.x >> 16;
+    const float4 pi = ld_ep<CL>(pos_base, ei, rank);
+    const float4 pj = ld_ep<CL>(pos_base, ej, rank);
+    const F3 gv = sub3(f3(pi), f3(pj));
+    const float len = len3(gv);
+    const float alpha_t = __fmul_rn(comp, inv_dt_sq);
+    const float wsum = __fadd_rn(__fadd_rn(pi.w, pj.w), alpha_t);
+    if (len < 1e-8f || wsum < 1e-8f) return;
+    const float C = __fsub_rn(len, __uint_as_float(r.y));
+    const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
+    F3 n;
+    if (!fpdiv3_by_length_fast(gv.x, gv.y, gv.z, len, n.x, n.y, n.z)) fpdiv3(gv.x, gv.y, gv.z, len, n.x, n.y, n.z);
+    if (pi.w > 0.0f)
+        add_ep<CL>(acc_base, ei, rank, __fmul_rn(__fmul_rn(n.x, pi.w), dlam), __fmul_rn(__fmul_rn(n.y, pi.w), dlam),
+                   __fmul_rn(__fmul_rn(n.z, pi.w), dlam), false);
+    if (pj.w > 0.0f)
+        add_ep<CL>(acc_base, ej, rank, __fmul_rn(__fmul_rn(n.x, pj.w), dlam), __fmul_rn(__fmul_rn(n.y, pj.w), dlam),
+                   __fmul_rn(__fmul_rn(n.z, pj.w), dlam), true);
+}
+
+// A frame (`substeps` substeps) of one cloth per cluster: T.order[blockIdx.x / CL].
+template <int CL, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) jacobi_cloth_kernel(XpbdWorld W, ClothSolveTable T,
+                                                                         uint32_t substeps) {
+    extern __shared__ float4 s_mem[];
+    float4* s_pos = s_mem;
+    float4* s_acc = s_mem + T.cap;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t rank = CL > 1 ? cluster_rank() : 0u;
+    const XpbdClothDesc D = T.cloths[T.order[blockIdx.x / CL]];
+    const XpbdDevParams P = *W.params;
+    const uint32_t p0 = rank * D.q;
+    const uint32_t np = p0 < D.n ? min(D.q, D.n - p0) : 0u;
+    const uint32_t g0 = D.vtx_off + p0;
+    const uint32_t pos_base = smem_u32(s_pos), acc_base = smem_u32(s_acc);
+    const uint32_t I = P.iterations;
+    const uint32_t* seg = T.seg + D.seg_base + rank;
+    for (uint32_t p = tid; p < np; p += BLOCK)  // incidence count of the particle's row (degree averaging)
+        s_acc[p] = make_float4(0.0f, 0.0f, 0.0f, (float)(W.row_off[g0 + p + 1] - W.row_off[g0 + p]));
+    for (uint32_t s = 0; s < substeps; ++s) {
+        for (uint32_t p = tid; p < np; p += BLOCK) {  // predict (pinned particles keep their position)
+            const uint32_t g = g0 + p;
+            const float4 x4 = W.x[g];
+            if (x4.w <= 0.0f) {
+                s_pos[p] = x4;
+                continue;
+            }
+            F3 vel = f3(W.v[g]);
+            const F3 pos = predict_w(W, g, f3(x4), vel, P);
+            s_pos[p] = make_float4(pos.x, pos.y, pos.z, x4.w);
+        }
+        cloth_sync<CL>();
+        for (uint32_t it = 0; it < I; ++it) {
+            for (uint32_t c = 0; c < D.colors; ++c) {
+                const uint32_t k0 = __ldg(seg + c * CL), k1 = __ldg(seg + c * CL + 1);
+                for (uint32_t k = k0 + tid; k < k1; k += BLOCK)
+                    solve_record<CL>(__ldg(T.rec + k), __ldg(T.comp + k), pos_base, acc_base, rank, P.inv_dt_sq);
+                cloth_sync<CL>();
+            }
+            // the pass's update of the owned particles (jacobi_gather_particle's tail), then at the end of the
+            // substep the velocity update
+            const bool last = it + 1 == I;
+            for (uint32_t p = tid; p < np; p += BLOCK) {
+                const float4 ps = s_pos[p];
+                if (ps.w <= 0.0f) continue;
+                const float4 a = s_acc[p];
+                F3 delta = {__fmul_rn(P.omega, a.x), __fmul_rn(P.omega, a.y), __fmul_rn(P.omega, a.z)};
+                if (P.relaxation == 1u && a.w > 0.0f) delta = div3(delta, a.w);
+                delta = clamp_correction(delta);
+                F3 xn = add3(f3(ps), delta);
+                s_acc[p] = make_float4(0.0f, 0.0f, 0.0f, a.w);
+                if (last) {
+                    const uint32_t g = g0 + p;
+                    F3 vel;
+                    xn = finalize_particle(xn, f3(W.x[g]), vel, P, W.status);
+                    W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+                    W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+                } else {
+                    s_pos[p] = make_float4(xn.x, xn.y, xn.z, ps.w);
+                }
+            }
+            if (!last) cloth_sync<CL>();
+        }
+        if (I == 0) {  // no passes: the predicted positions are the substep's result (xpbd_cpu.rs:302-309)
+            for (uint32_t p = tid; p < np; p += BLOCK) {
+                const float4 ps = s_pos[p];
+                if (ps.w <= 0.0f) continue;
+                const uint32_t g = g0 + p;
+                F3 vel;
+                const F3 xn = finalize_particle(f3(ps), f3(W.x[g]), vel, P, W.status);
+                W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+                W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+            }
+        }
+        // the next substep's predict touches only this CTA's own particles; its barrier precedes any peer read
+    }
+    if (CL > 1) cluster_sync();  // no CTA leaves while a peer may still address its shared memory
+}
+
+template <int CL, int BLOCK>
+static const void* cloth_fn() {
+    return (const void*)&jacobi_cloth_kernel<CL, BLOCK>;
+}
+static const void* cloth_fn_of(int cls) {
+    switch (cls) {
+        case 0: return cloth_fn<1, 256>();
+        case 1: return cloth_fn<1, 512>();
+        case 2: return cloth_fn<1, 1024>();
+        case 3: return cloth_fn<2, 1024>();
+        case 4: return cloth_fn<4, 1024>();
+        case 5: return cloth_fn<8, 1024>();
+        default: return nullptr;
+    }
+}
+
+cudaError_t cloth_kernel_prepare() {
+    for (int c = 0; c < kClothClasses; ++c) {
+        const int bytes = (int)cloth_kernel_smem_bytes(kClothClass[c].rank_cap);
+        cudaError_t e = cudaFuncSetAttribute(cloth_fn_of(c), cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+        if (kClothClass[c].cl > 1) {
+            e = cudaFuncSetAttribute(cloth_fn_of(c), cudaFuncAttributeNonPortableClusterSizeAllowed, 0);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTable& T, uint32_t substeps,
+                               cudaStream_t st) {
+    if (cls < 0 || cls >= kClothClasses || T.count == 0) return cudaSuccess;
+    const ClothClass& K = kClothClass[cls];
+    if (T.cap > K.rank_cap) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(T.count * K.cl, 1, 1);
+    cfg.blockDim = dim3(K.block, 1, 1);
+    cfg.dynamicSmemBytes = cloth_kernel_smem_bytes(T.cap);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = K.cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = K.cl > 1 ? 1 : 0;
+    XpbdWorld w = W;
+    ClothSolveTable t = T;
+    void* args[] = {&w, &t, &substeps};
+    return cudaLaunchKernelExC(&cfg, cloth_fn_of(cls), args);
+}
+
+}  // namespace xpbd

@@ -107,6 +107,23 @@ struct XpbdPatch {
 #define XPBD_PATCH_MAX_LOCAL (1u << XPBD_PATCH_LOCAL_BITS)
 #define XPBD_PATCH_MAX_CON 32767u
 
+// Cloth-resident Jacobi (jacobi_cloth_kernel): one CTA, or a cluster of `cl` CTAs, holds a whole cloth in shared
+// memory for a frame. Rank r of the cluster owns the cloth-local particles [r·q, min(n, (r+1)·q)). A constraint
+// endpoint is addressed as (rank << 13) | local index. Records are grouped by (color, rank): seg[seg_base + c·cl + r]
+// is the first record of color c processed by rank r (the last entry closes the cloth's range).
+struct XpbdClothDesc {
+    uint32_t vtx_off;   // first particle of the cloth in the packed batch
+    uint32_t n;         // particles
+    uint32_t q;         // particles per rank (<= XPBD_CLOTH_RANK_MAX)
+    uint32_t colors;    // color batches
+    uint32_t seg_base;  // first entry of the cloth in seg[]
+    uint32_t cl;        // CTAs of the cluster that solves the cloth
+    uint32_t pad[2];
+};
+#define XPBD_CLOTH_EP_BITS 13
+#define XPBD_CLOTH_RANK_MAX 7168u     // particles per CTA: 2 x 16 B of shared memory each (224 KB)
+#define XPBD_CLOTH_MAX_CL 8u
+
 struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     uint32_t n, e, n_inc, n_tiles, n_colors, n_cloths;
     float4* x;
@@ -119,6 +136,7 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     const XpbdTile* tiles;
     const uint16_t* row_cloth;      // per particle: cloth index (palette row)
     const float* palette_comp;
+    const float* inc_comp;          // per incidence compliance when a cloth has more than 16 values (else null)
     const uint4* con;
     float* con_lambda;
     const uint32_t* color_off;

@@ -38,6 +38,28 @@ cudaError_t launch_mlp_adam(float* master, float* m1, float* m2, const float* gr
                             float beta1, float beta2, float eps, float bc1, float bc2, XpbdMlp* mlp, cudaStream_t st);
 cudaError_t launch_mlp_publish(const float* master, XpbdMlp* mlp, cudaStream_t st);
 
+// ---- cloth-resident Jacobi (cloth_jacobi.cu)
+struct ClothSolveTable {
+    const XpbdClothDesc* cloths;  // per cloth of the batch
+    const uint32_t* seg;          // (color, rank) segment starts into rec / comp
+    const uint2* rec;             // {endpoint i | endpoint j << 16, rest bits}
+    const float* comp;            // compliance per record
+    const uint32_t* order;        // cloth ids of one launch (one per cluster), largest first
+    uint32_t count;               // cloths in the launch
+    uint32_t cap;                 // shared-memory slots per rank in this launch (>= every cloth's q)
+};
+// Launch shapes of the cloth-resident kernel: CTAs per cluster and threads per CTA; a cloth of n particles takes
+// the first class whose capacity (cl x per-rank slots) holds it.
+struct ClothClass {
+    uint32_t cl, block, rank_cap;
+};
+constexpr int kClothClasses = 6;
+extern const ClothClass kClothClass[kClothClasses];
+size_t cloth_kernel_smem_bytes(uint32_t cap);
+cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTable& T, uint32_t substeps,
+                               cudaStream_t st);
+cudaError_t cloth_kernel_prepare();  // opt-in shared-memory sizes (host, once)
+
 // ---- cluster Gauss–Seidel (cluster_gs.cu)
 struct ClusterTable {
     const uint4* rec;    // constraint records grouped by (color, owning rank)

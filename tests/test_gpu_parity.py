@@ -365,7 +365,8 @@ def test_gauss_seidel_execution_paths_bit_exact(cluster):
     assert max_abs(plug2.positions(), o2.state()[0]) == 0.0
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 3], ids=["warp_tiles", "spatial_patches", "thread_rows"])
+@pytest.mark.parametrize("kernel", [1, 2, 3, 4], ids=["warp_tiles", "spatial_patches", "thread_rows",
+                                                     "cloth_resident"])
 @pytest.mark.parametrize("lam", [P.LAMBDA_RESET_PER_ITERATION, P.LAMBDA_PER_SUBSTEP], ids=["lambda_reset", "lambda_substep"])
 def test_jacobi_execution_paths_bit_exact(kernel, lam):
     """Every Jacobi execution — warp tiles over the neighbour table, shared-memory spatial patches that solve each
@@ -377,8 +378,10 @@ def test_jacobi_execution_paths_bit_exact(kernel, lam):
                jacobi_kernel=kernel)
     plug = gpu_sim(specs, prm, cfg)
     plug.step(frames=6)
-    # the requested execution ran: kernel ids 0 warp tiles, 2 spatial patches, 5 thread per particle
-    assert plug.stats()["solver_kernel"] == {1: 0, 2: 2, 3: 5}[kernel]
+    # the requested execution ran: kernel ids 0 warp tiles, 2 spatial patches, 5 thread per particle, 7 cloth-resident
+    # (λ cleared per pass only; with λ kept over the substep the thread-per-particle kernel runs instead)
+    want = {1: 0, 2: 2, 3: 5, 4: 7 if lam == P.LAMBDA_RESET_PER_ITERATION else 5}[kernel]
+    assert plug.stats()["solver_kernel"] == want
     for k, sp in enumerate(specs):
         o = oracle_sim(sp, prm, cfg)
         o.substeps(60)
@@ -430,3 +433,26 @@ def test_cluster_gs_coordinates_outside_fast_division_range_bit_exact(where):
     o = oracle_sim(sp, prm, cfg)
     o.substeps(20)
     assert max_abs(plug.positions(), o.state()[0]) == 0.0
+
+
+@pytest.mark.parametrize("solver,kernel,lam", [
+    (P.SOLVER_JACOBI, 3, P.LAMBDA_RESET_PER_ITERATION), (P.SOLVER_JACOBI, 1, P.LAMBDA_RESET_PER_ITERATION),
+    (P.SOLVER_JACOBI, 4, P.LAMBDA_RESET_PER_ITERATION), (P.SOLVER_JACOBI, 3, P.LAMBDA_PER_SUBSTEP),
+    (P.SOLVER_GAUSS_SEIDEL, 0, P.LAMBDA_RESET_PER_ITERATION)],
+    ids=["rows", "warp_tiles", "cloth_resident", "rows_lambda_substep", "gauss_seidel"])
+def test_any_number_of_compliance_values_bit_exact(solver, kernel, lam):
+    """A cloth whose every constraint has its own compliance (the reference packs an f32 compliance per constraint,
+    cloth_jacobi.rs:95-111): more than the 16 values a cloth's palette names, so the incidences carry their own."""
+    rng = np.random.default_rng(31)
+    specs = [wl.make_sheet(36, 1.0, 1.0, "corners", seed=32), wl.make_sheet(20, 1.0, 1.0, "top_edge", seed=33)]
+    specs[0].compliance = (10.0 ** rng.uniform(-9, -3, specs[0].num_constraints)).astype(np.float32)
+    assert len(np.unique(specs[0].compliance)) > 16
+    prm = params_for(10, 10, 1.0)
+    cfg = _cfg(solver=solver, relaxation=P.RELAX_AVERAGE if solver == P.SOLVER_JACOBI else P.RELAX_OMEGA,
+               lambda_mode=lam, solve_substeps=10, jacobi_kernel=kernel)
+    plug = gpu_sim(specs, prm, cfg)
+    plug.step(frames=3)
+    for k, sp in enumerate(specs):
+        o = oracle_sim(sp, prm, cfg)
+        o.substeps(30)
+        assert max_abs(plug.positions(k), o.state()[0]) == 0.0, k
