@@ -37,7 +37,7 @@ EXPORTED = [
     "xpbd_converge_history", "xpbd_converge_cloth_iterations", "xpbd_selftest_division",
     "xpbd_mlp_minibatch_gradients", "xpbd_mlp_apply_gradients", "xpbd_set_triangles", "xpbd_read_normals",
     "xpbd_mesh_grid_hanging", "xpbd_mesh_from_obj", "xpbd_mesh_from_triangles", "xpbd_mesh_sizes", "xpbd_mesh_get",
-    "xpbd_mesh_free", "xpbd_set_cloth_grab", "xpbd_color_constraints_device_scratch_bytes",
+    "xpbd_mesh_free", "xpbd_set_cloth_grab", "xpbd_set_cloth_wind", "xpbd_color_constraints_device_scratch_bytes",
     "xpbd_color_constraints_device", "xpbd_neighbor_table_device_scratch_bytes", "xpbd_neighbor_table_device",
 ]
 MLP_PARAMS = 4865
@@ -162,6 +162,7 @@ def load():
         "xpbd_mesh_get": (I, [P, P, P, P, P, P, P, P, P]),
         "xpbd_mesh_free": (None, [P]),
         "xpbd_set_cloth_grab": (I, [P, U, C.c_int32, P, C.c_float]),
+        "xpbd_set_cloth_wind": (I, [P, U, P, C.c_float]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -106,6 +106,7 @@ struct xpbd_ctx {
     uint64_t adam_step = 0;
     float norm[XPBD_MLP_NORM] = {0};
     std::vector<XpbdGrab> grabs;  // per cloth (host copy)
+    std::vector<XpbdWind> winds;  // per cloth (host copy)
     float forced_timeout_ms = 0.f;
     // cloth-resident Jacobi (kernel id 7): per launch class the cloths it solves; side streams run the classes
     // concurrently (fork / join events on the context stream)
@@ -115,6 +116,10 @@ struct xpbd_ctx {
     cudaStream_t cls_stream[kClothClasses] = {};
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_join[kClothClasses] = {};
+    // single-cluster small batch (kernel id 8)
+    bool small_ok = false, small_tried = false;
+    SmallBatch small{};
+    uint32_t small_cl = 0, small_block = 0;
 };
 
 // ------------------------------------------------------------------------------------------------- helpers
@@ -610,6 +615,11 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     uint32_t* grab_count_d;
     ALLOC(grabs_d, XpbdGrab, C);
     ALLOC(grab_count_d, uint32_t, 1);
+    XpbdWind* winds_d;
+    uint32_t* wind_count_d;
+    ALLOC(winds_d, XpbdWind, C);
+    ALLOC(wind_count_d, uint32_t, 1);
+    ctx->winds.assign(C, XpbdWind{{0.f, 0.f, 0.f}, 0.f});
     ctx->grabs.assign(C, XpbdGrab{-1, {0.f, 0.f, 0.f}, 0.f, {0u, 0u, 0u}});
     // render triangles: packed global vertex indices and the vertex → triangle table for the vertex normals
     std::vector<uint4> tri_all;
@@ -730,6 +740,11 @@ extern "C" int xpbd_commit(xpbd_ctx* ctx) {
     W.grab_count = grab_count_d;
     H2D(grabs_d, ctx->grabs.data(), C * sizeof(XpbdGrab));
     CK(cudaMemsetAsync(grab_count_d, 0, sizeof(uint32_t), st), "memset");
+    W.winds = winds_d;
+    W.wind_count = wind_count_d;
+    H2D(winds_d, ctx->winds.data(), C * sizeof(XpbdWind));
+    CK(cudaMemsetAsync(wind_count_d, 0, sizeof(uint32_t), st), "memset");
+    CK(cudaStreamSynchronize(st), "commit sync");
     CK(cudaMemsetAsync(div_exact_d, 0xFF, 4 * sizeof(unsigned), st), "memset");  // exact until the first check
     W.n_tris = T;
     W.tris = tris_d;
@@ -1100,6 +1115,84 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
     return XPBD_OK;
 }
 
+// Tables of the single-cluster small-batch kernel: the rows of the neighbour table split over the cluster's ranks
+// (records {self, other endpoint, rest, compliance}), built on its first selection from the device tables.
+constexpr uint32_t kSmallBatchMaxParticles = 16 * 512;
+static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
+    *usable = ctx->small_ok;
+    if (ctx->small_tried) return XPBD_OK;
+    ctx->small_tried = true;
+    const uint32_t N = ctx->W.n, C = (uint32_t)ctx->cloths.size();
+    if (N == 0 || N > kSmallBatchMaxParticles) return XPBD_OK;
+    std::vector<uint32_t> roff(N + 1);
+    std::vector<uint2> inc(ctx->W.n_inc);
+    std::vector<float> pal((size_t)C * XPBD_PALETTE), icomp(ctx->wide_palette ? ctx->W.n_inc : 0);
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(roff.data(), ctx->W.row_off, (N + 1) * 4, cudaMemcpyDeviceToHost, st), "download");
+    if (!inc.empty())
+        CK(cudaMemcpyAsync(inc.data(), ctx->W.inc, inc.size() * 8, cudaMemcpyDeviceToHost, st), "download");
+    CK(cudaMemcpyAsync(pal.data(), ctx->W.palette_comp, pal.size() * 4, cudaMemcpyDeviceToHost, st), "download");
+    if (!icomp.empty())
+        CK(cudaMemcpyAsync(icomp.data(), ctx->W.inc_comp, icomp.size() * 4, cudaMemcpyDeviceToHost, st), "download");
+    CK(cudaStreamSynchronize(st), "download sync");
+    std::vector<uint32_t> cloth_of(N);
+    for (uint32_t k = 0; k < C; ++k)
+        for (uint32_t i = 0; i < ctx->cloths[k].n; ++i) cloth_of[ctx->cloths[k].vtx_off + i] = k;
+    for (uint32_t cl : {16u, 8u}) {
+        const uint32_t q = (N + cl - 1) / cl;
+        if (q > 1024 || q >= (1u << XPBD_CLOTH_EP_BITS)) continue;
+        std::vector<uint4> rec;
+        std::vector<uint32_t> lroff((size_t)cl * (q + 1), 0), rbase(cl, 0);
+        uint32_t m_max = 0;
+        for (uint32_t r = 0; r < cl; ++r) {
+            rbase[r] = (uint32_t)rec.size();
+            const uint32_t p0 = r * q, p1 = std::min(N, p0 + q);
+            for (uint32_t p = p0; p < p1; ++p) {
+                lroff[(size_t)r * (q + 1) + (p - p0)] = (uint32_t)rec.size() - rbase[r];
+                for (uint32_t k = roff[p]; k < roff[p + 1]; ++k) {
+                    const uint32_t o = inc[k].x & XPBD_OTHER_MASK;
+                    const float comp = ctx->wide_palette ? icomp[k]
+                                                         : pal[(size_t)cloth_of[p] * XPBD_PALETTE + (inc[k].x >> 28)];
+                    uint32_t cb;
+                    memcpy(&cb, &comp, 4);
+                    rec.push_back(make_uint4(p - p0, ((o / q) << XPBD_CLOTH_EP_BITS) | (o % q), inc[k].y, cb));
+                }
+            }
+            const uint32_t m = (uint32_t)rec.size() - rbase[r];
+            for (uint32_t p = (p1 > p0 ? p1 - p0 : 0); p <= q; ++p) lroff[(size_t)r * (q + 1) + p] = m;
+            m_max = std::max(m_max, m);
+        }
+        const uint32_t block = std::min<uint32_t>(1024, std::max<uint32_t>(32, (std::max(m_max, q) + 31) / 32 * 32));
+        if (m_max > 4096 || !small_batch_supported(cl, block, q, m_max)) {
+            cudaGetLastError();
+            continue;
+        }
+        cudaError_t err = cudaSuccess;
+        uint4* d_rec = dev_alloc<uint4>(ctx, std::max<size_t>(1, rec.size()), &err);
+        uint32_t* d_roff = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, lroff.size(), &err) : nullptr;
+        uint32_t* d_rbase = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, cl, &err) : nullptr;
+        if (err != cudaSuccess) return cuda_fail(ctx, err, "small-batch tables");
+        if (!rec.empty())
+            CK(cudaMemcpyAsync(d_rec, rec.data(), rec.size() * 16, cudaMemcpyHostToDevice, st), "upload");
+        CK(cudaMemcpyAsync(d_roff, lroff.data(), lroff.size() * 4, cudaMemcpyHostToDevice, st), "upload");
+        CK(cudaMemcpyAsync(d_rbase, rbase.data(), cl * 4, cudaMemcpyHostToDevice, st), "upload");
+        CK(cudaStreamSynchronize(st), "upload sync");
+        ctx->small = SmallBatch{d_rec, d_roff, d_rbase, q, m_max};
+        ctx->small_cl = cl;
+        ctx->small_block = block;
+        ctx->small_ok = true;
+        *usable = true;
+        return XPBD_OK;
+    }
+    return XPBD_OK;
+}
+
+static bool small_batch_usable(xpbd_ctx* ctx) {
+    bool usable = false;
+    if (ensure_small_batch(ctx, &usable) != XPBD_OK) return false;
+    return usable;
+}
+
 static bool cloth_kernel_usable(xpbd_ctx* ctx) {
     bool usable = false;
     if (ensure_cloth_tables(ctx, &usable) != XPBD_OK) return false;
@@ -1153,6 +1246,18 @@ static void choose_schedule(xpbd_ctx* ctx) {
                               !ctx->opts.warm_start;
     const bool cloth_eligible = plain_jacobi && ctx->opts.lambda_mode == XPBD_LAMBDA_RESET_PER_ITERATION &&
                                 ctx->opts.collision == XPBD_COLLISION_NONE;
+    const bool small_default = ctx->opts.jacobi_kernel == 0 && ctx->W.n <= 4096;
+    if (cloth_eligible && (small_default || ctx->opts.jacobi_kernel == 5) && small_batch_usable(ctx)) {
+        ctx->kernel = 8;
+        ctx->block = ctx->small_block;
+        ctx->grid = ctx->small_cl;
+        ctx->coop = false;
+        ctx->stats.grid_blocks = ctx->small_cl;
+        ctx->stats.block_threads = ctx->small_block;
+        ctx->stats.solver_kernel = 8;
+        ctx->stats.cluster_ctas = ctx->small_cl;
+        return;
+    }
     if (cloth_eligible && (ctx->opts.jacobi_kernel == 0 || ctx->opts.jacobi_kernel == 4) &&
         cloth_kernel_usable(ctx)) {
         ctx->kernel = 7;
@@ -1282,6 +1387,10 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
         return cudaSuccess;
     }
     if (ctx->kernel == 7) return launch_cloth_frame(ctx, S, st, launches);  // no collision (choose_schedule)
+    if (ctx->kernel == 8) {
+        *launches += 1;
+        return launch_small_batch(ctx->small_cl, ctx->small_block, ctx->W, ctx->small, S, st);
+    }
     if (!coll) {
         e = launch_substeps(ctx, kEndFinalize, S, 0, 0, st);
         *launches += 1;
@@ -1609,6 +1718,31 @@ extern "C" int xpbd_set_cloth_grab(xpbd_ctx* ctx, uint32_t cloth_id, int32_t ver
     return XPBD_OK;
 }
 
+extern "C" int xpbd_set_cloth_wind(xpbd_ctx* ctx, uint32_t cloth_id, const float* velocity, float drag) {
+    if (!ctx || (drag != 0.f && !velocity)) return XPBD_ERR_INVALID_ARGUMENT;
+    if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
+    if (cloth_id >= ctx->cloths.size()) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "bad cloth id");
+    if (!(drag >= 0.f) || !std::isfinite(drag)) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "wind drag must be >= 0");
+    XpbdWind w{{0.f, 0.f, 0.f}, 0.f};
+    if (drag > 0.f) {
+        w.vel[0] = velocity[0];
+        w.vel[1] = velocity[1];
+        w.vel[2] = velocity[2];
+        w.drag = drag;
+    }
+    ctx->winds[cloth_id] = w;
+    uint32_t active = 0;
+    for (const XpbdWind& h : ctx->winds) active += h.drag > 0.f ? 1u : 0u;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    // ordered with the frames on the context's stream; the host copies are staged before the call returns
+    CK(cudaMemcpyAsync(const_cast<XpbdWind*>(ctx->W.winds) + cloth_id, &ctx->winds[cloth_id], sizeof(XpbdWind),
+                       cudaMemcpyHostToDevice, ctx->stream), "wind");
+    CK(cudaMemcpyAsync(const_cast<uint32_t*>(ctx->W.wind_count), &active, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                       ctx->stream), "wind");
+    CK(cudaStreamSynchronize(ctx->stream), "wind");
+    return XPBD_OK;
+}
+
 extern "C" int xpbd_read_normals(xpbd_ctx* ctx, uint32_t cloth_id, float* out_xyz) {
     if (!ctx || !out_xyz) return XPBD_ERR_INVALID_ARGUMENT;
     if (!ctx->committed) return fail(ctx, XPBD_ERR_STATE, "not committed");
@@ -1785,6 +1919,10 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
         base.lambda_mode == XPBD_LAMBDA_RESET_PER_ITERATION && base.collision == XPBD_COLLISION_NONE &&
         cloth_kernel_usable(ctx))
         cands.push_back({0, 0, 1, 4});  // cloth-resident kernel (its launch shapes are fixed per cloth size)
+    if (base.solver == XPBD_SOLVER_JACOBI && !(base.tolerance > 0.f || base.warm_start) &&
+        base.lambda_mode == XPBD_LAMBDA_RESET_PER_ITERATION && base.collision == XPBD_COLLISION_NONE &&
+        small_batch_usable(ctx))
+        cands.push_back({0, 0, 1, 5});  // the whole batch in one cluster
     if (base.solver == XPBD_SOLVER_GAUSS_SEIDEL && base.cluster_ctas != 1)
         for (uint32_t cl : {16u, 8u})
             for (uint32_t blk : {512u, 1024u}) cands.push_back({blk, 0, cl, 0});

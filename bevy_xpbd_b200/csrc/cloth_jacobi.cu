@@ -102,6 +102,24 @@ __device__ __forceinline__ void solve_record(uint2 r, float comp, uint32_t pos_b
                    __fmul_rn(__fmul_rn(n.z, pj.w), dlam), true);
 }
 
+// A thread's first two records of a color (k and k + BLOCK), loaded ahead of use.
+struct Pref {
+    uint2 r0, r1;
+    float c0, c1;
+};
+__device__ __forceinline__ Pref pref_load(const ClothSolveTable& T, uint32_t k, uint32_t k1, uint32_t block) {
+    Pref p = {make_uint2(0u, 0u), make_uint2(0u, 0u), 0.0f, 0.0f};
+    if (k < k1) {
+        p.r0 = __ldg(T.rec + k);
+        p.c0 = __ldg(T.comp + k);
+    }
+    if (k + block < k1) {
+        p.r1 = __ldg(T.rec + k + block);
+        p.c1 = __ldg(T.comp + k + block);
+    }
+    return p;
+}
+
 // A frame (`substeps` substeps) of one cloth per cluster: T.order[blockIdx.x / CL].
 template <int CL, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) jacobi_cloth_kernel(XpbdWorld W, ClothSolveTable T,
@@ -134,10 +152,21 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) jacobi_cloth_kernel(XpbdW
             s_pos[p] = make_float4(pos.x, pos.y, pos.z, x4.w);
         }
         cloth_sync<CL>();
+        // The records of a thread's first two rounds of each color are loaded while the previous color is solved
+        // (records do not change between passes: after the last color, color 0's are loaded again).
+        uint32_t pk0 = __ldg(seg), pk1 = __ldg(seg + 1);
+        Pref pf = pref_load(T, pk0 + tid, pk1, BLOCK);
         for (uint32_t it = 0; it < I; ++it) {
             for (uint32_t c = 0; c < D.colors; ++c) {
-                const uint32_t k0 = __ldg(seg + c * CL), k1 = __ldg(seg + c * CL + 1);
-                for (uint32_t k = k0 + tid; k < k1; k += BLOCK)
+                const uint32_t k0 = pk0, k1 = pk1;
+                const Pref cur = pf;
+                const uint32_t cn = c + 1 < D.colors ? c + 1 : 0u;
+                pk0 = __ldg(seg + cn * CL);
+                pk1 = __ldg(seg + cn * CL + 1);
+                pf = pref_load(T, pk0 + tid, pk1, BLOCK);
+                if (k0 + tid < k1) solve_record<CL>(cur.r0, cur.c0, pos_base, acc_base, rank, P.inv_dt_sq);
+                if (k0 + tid + BLOCK < k1) solve_record<CL>(cur.r1, cur.c1, pos_base, acc_base, rank, P.inv_dt_sq);
+                for (uint32_t k = k0 + tid + 2 * BLOCK; k < k1; k += BLOCK)
                     solve_record<CL>(__ldg(T.rec + k), __ldg(T.comp + k), pos_base, acc_base, rank, P.inv_dt_sq);
                 cloth_sync<CL>();
             }
@@ -231,6 +260,178 @@ cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTab
     ClothSolveTable t = T;
     void* args[] = {&w, &t, &substeps};
     return cudaLaunchKernelExC(&cfg, cloth_fn_of(cls), args);
+}
+
+// ---------------------------------------------------------------------------------------------- one small batch
+// Latency path for a single small cloth (or a few): the whole batch spread over one cluster of CL CTAs, thread per
+// incidence, one cluster barrier per pass. Rank r owns particles [r·q, (r+1)·q) and their neighbour-table rows; its
+// shared memory holds the two Jacobi position buffers of those particles (the reference's jac_a / jac_b ping-pong),
+// the rows' incidence records and one correction term per incidence. A pass: every thread evaluates one incidence —
+// the reference's Δλ recomputed from the row's endpoint, times n̂·w_self (jacobi_edges + jacobi_gather,
+// xpbd_cpu.rs:139-226) — reading the other endpoint from its owner's shared memory; then each particle sums its row's
+// terms in table order and writes its new position into the other buffer; a cluster barrier ends the pass. The
+// constraint is evaluated from both ends (as the thread-per-particle kernel does), which costs instructions but
+// keeps the pass to one barrier: for a small cloth the pass is latency-bound, not issue-bound.
+size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max) {
+    return 2 * (size_t)q * 16 + (size_t)m_max * 32 + ((size_t)(q + 1) * 4 + 15) / 16 * 16;
+}
+
+template <int CL>
+__global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W, SmallBatch B, uint32_t substeps) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t q = B.q;
+    float4* s_pos0 = reinterpret_cast<float4*>(smem);
+    uint4* s_rec = reinterpret_cast<uint4*>(smem + 2 * (size_t)q * 16);
+    float4* s_term = reinterpret_cast<float4*>(smem + 2 * (size_t)q * 16 + (size_t)B.m_max * 16);
+    uint32_t* s_roff = reinterpret_cast<uint32_t*>(smem + 2 * (size_t)q * 16 + (size_t)B.m_max * 32);
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t rank = cluster_rank();
+    const uint32_t p0 = rank * q;
+    const uint32_t np = p0 < W.n ? min(q, W.n - p0) : 0u;
+    const XpbdDevParams P = *W.params;
+    const uint32_t m = B.roff[rank * (q + 1) + np];
+    for (uint32_t k = tid; k <= np; k += nthr) s_roff[k] = B.roff[rank * (q + 1) + k];
+    for (uint32_t k = tid; k < m; k += nthr) s_rec[k] = B.rec[B.rbase[rank] + k];
+    const uint32_t pos_base = smem_u32(s_pos0);
+    uint32_t b = 0;  // buffer the next predict writes: never the one a peer may still be reading
+    const uint32_t I = P.iterations;
+    __syncthreads();
+    for (uint32_t s = 0; s < substeps; ++s) {
+        for (uint32_t p = tid; p < np; p += nthr) {
+            const uint32_t g = p0 + p;
+            const float4 x4 = W.x[g];
+            float4 out = x4;
+            if (x4.w > 0.0f) {
+                F3 vel = f3(W.v[g]);
+                const F3 pos = predict_w(W, g, f3(x4), vel, P);
+                out = make_float4(pos.x, pos.y, pos.z, x4.w);
+            }
+            if (x4.w > 0.0f)
+                s_pos0[b * q + p] = out;
+            else if (s == 0)  // pinned: the same in both buffers, for the whole frame
+                s_pos0[p] = s_pos0[q + p] = x4;
+        }
+        cluster_sync();
+        for (uint32_t it = 0; it < I; ++it) {
+            const uint32_t src = pos_base + b * q * 16u;
+            for (uint32_t k = tid; k < m; k += nthr) {
+                const uint4 r = s_rec[k];
+                const float4 ps = ld_local(src + r.x * 16u);
+                const uint32_t ro = r.y >> XPBD_CLOTH_EP_BITS;
+                const uint32_t ao = src + (r.y & ((1u << XPBD_CLOTH_EP_BITS) - 1u)) * 16u;
+                const float4 po = ro == rank ? ld_local(ao) : ld_dsmem(map_rank(ao, ro));
+                const F3 gv = sub3(f3(ps), f3(po));
+                const float len = len3(gv);
+                const float alpha_t = __fmul_rn(__uint_as_float(r.w), P.inv_dt_sq);
+                const float wsum = __fadd_rn(__fadd_rn(ps.w, po.w), alpha_t);
+                float4 t = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (!(len < 1e-8f) && !(wsum < 1e-8f)) {
+                    F3 n;
+                    if (!fpdiv3_by_length_fast(gv.x, gv.y, gv.z, len, n.x, n.y, n.z))
+                        fpdiv3(gv.x, gv.y, gv.z, len, n.x, n.y, n.z);
+                    const float C = __fsub_rn(len, __uint_as_float(r.z));
+                    const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
+                    t = make_float4(__fmul_rn(__fmul_rn(n.x, ps.w), dlam), __fmul_rn(__fmul_rn(n.y, ps.w), dlam),
+                                    __fmul_rn(__fmul_rn(n.z, ps.w), dlam), 0.0f);
+                }
+                s_term[k] = t;
+            }
+            __syncthreads();
+            const bool last = it + 1 == I;
+            for (uint32_t p = tid; p < np; p += nthr) {
+                const float4 ps = s_pos0[b * q + p];
+                if (ps.w <= 0.0f) continue;
+                const uint32_t rs = s_roff[p], re = s_roff[p + 1];
+                float ax = 0.0f, ay = 0.0f, az = 0.0f;
+                for (uint32_t k = rs; k < re; ++k) {
+                    const float4 t = s_term[k];
+                    ax = __fadd_rn(ax, t.x);
+                    ay = __fadd_rn(ay, t.y);
+                    az = __fadd_rn(az, t.z);
+                }
+                F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
+                if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
+                delta = clamp_correction(delta);
+                F3 xn = add3(f3(ps), delta);
+                if (last) {
+                    const uint32_t g = p0 + p;
+                    F3 vel;
+                    xn = finalize_particle(xn, f3(W.x[g]), vel, P, W.status);
+                    W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+                    W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+                }
+                s_pos0[(b ^ 1u) * q + p] = make_float4(xn.x, xn.y, xn.z, ps.w);
+            }
+            b ^= 1u;
+            if (!last) cluster_sync();
+        }
+        if (I == 0) {
+            for (uint32_t p = tid; p < np; p += nthr) {
+                const float4 ps = s_pos0[b * q + p];
+                if (ps.w <= 0.0f) continue;
+                const uint32_t g = p0 + p;
+                F3 vel;
+                const F3 xn = finalize_particle(f3(ps), f3(W.x[g]), vel, P, W.status);
+                W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
+                W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+            }
+        }
+        // the last pass read buffer b ^ 1 (peers may still be reading it) and wrote b: the next predict writes b
+        __syncthreads();
+    }
+    cluster_sync();
+}
+
+static const void* small_fn(uint32_t cl) {
+    if (cl == 8) return (const void*)&jacobi_small_batch_kernel<8>;
+    if (cl == 16) return (const void*)&jacobi_small_batch_kernel<16>;
+    return nullptr;
+}
+
+static cudaLaunchConfig_t small_cfg(uint32_t cl, uint32_t block, size_t smem, cudaStream_t st,
+                                    cudaLaunchAttribute* attr) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl, 1, 1);
+    cfg.blockDim = dim3(block, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+bool small_batch_supported(uint32_t cl, uint32_t block, uint32_t q, uint32_t m_max) {
+    const void* fn = small_fn(cl);
+    if (!fn || block > 1024 || q > block) return false;
+    const size_t smem = small_batch_smem_bytes(q, m_max);
+    if (smem > 220 * 1024) return false;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+    if (cl > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+        return false;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = small_cfg(cl, block, smem, nullptr, attr);
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return clusters >= 1;
+}
+
+cudaError_t launch_small_batch(uint32_t cl, uint32_t block, const XpbdWorld& W, const SmallBatch& B,
+                               uint32_t substeps, cudaStream_t st) {
+    const void* fn = small_fn(cl);
+    if (!fn) return cudaErrorInvalidValue;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = small_cfg(cl, block, small_batch_smem_bytes(B.q, B.m_max), st, attr);
+    XpbdWorld w = W;
+    SmallBatch b = B;
+    void* args[] = {&w, &b, &substeps};
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 }  // namespace xpbd

@@ -51,8 +51,12 @@ __device__ __forceinline__ V3 vclamp(V3 dx) {
 }
 __device__ __forceinline__ bool vfinite(V3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
 
-__device__ __forceinline__ V3 predict(uint32_t i, V3 sim, V3& vel, const XpbdDevParams& P) {
+__device__ __forceinline__ V3 predict(uint32_t i, V3 sim, V3& vel, const XpbdDevParams& P, const XpbdWorld& W) {
     V3 v = vadd(vel, vmul(V3{P.gravity[0], P.gravity[1], P.gravity[2]}, P.dt));
+    if (*W.wind_count != 0u) {  // per-cloth wind (extension): v += (wind − v) · (drag · dt)
+        const XpbdWind wd = W.winds[W.row_cloth[i]];
+        if (wd.drag > 0.0f) v = vadd(v, vmul(vsub(V3{wd.vel[0], wd.vel[1], wd.vel[2]}, v), __fmul_rn(wd.drag, P.dt)));
+    }
     const float v2 = __fadd_rn(__fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)), __fmul_rn(v.z, v.z));
     if (v2 >= 144.0f) {
         const float speed = __fsqrt_rn(v2);
@@ -222,7 +226,7 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
                 W.v[i] = make_float4(vel.x, vel.y, vel.z, 0.0f);
                 xo = xn;
             }
-            V3 p = predict(i, xo, vel, P);
+            V3 p = predict(i, xo, vel, P, W);
             if (*W.grab_count != 0u) {  // per-cloth grab (extension), the reference's pull on the grabbed vertex
                 const XpbdGrab g = W.grabs[W.row_cloth[i]];
                 if (g.idx == (int32_t)i) {

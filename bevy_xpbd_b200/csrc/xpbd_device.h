@@ -58,9 +58,12 @@ __device__ __forceinline__ F3 clamp_correction(F3 dx) {
 }
 
 // predict_particle, xpbd_cpu.rs:38-65 (callers handle inv_mass <= 0)
-__device__ __forceinline__ F3 predict_particle(uint32_t i, F3 sim, F3& vel, const XpbdDevParams& P) {
+// `wind` (extension, may be null): after gravity, v += (wind − v) · (drag · dt).
+__device__ __forceinline__ F3 predict_particle(uint32_t i, F3 sim, F3& vel, const XpbdDevParams& P,
+                                               const XpbdWind* wind = nullptr) {
     F3 g = {P.gravity[0], P.gravity[1], P.gravity[2]};
     F3 v = add3(vel, mul3(g, P.dt));
+    if (wind) v = add3(v, mul3(sub3(F3{wind->vel[0], wind->vel[1], wind->vel[2]}, v), __fmul_rn(wind->drag, P.dt)));
     const float v2 = dot3(v, v);
     if (v2 >= 144.0f) {  // below 12² the reference's speed = sqrt(v2) cannot exceed 12: skip the root
         const float speed = __fsqrt_rn(v2);
@@ -90,7 +93,13 @@ __device__ __forceinline__ F3 apply_cloth_grab(const XpbdWorld& W, uint32_t i, F
     return add3(pos, pull);
 }
 __device__ __forceinline__ F3 predict_w(const XpbdWorld& W, uint32_t i, F3 sim, F3& vel, const XpbdDevParams& P) {
-    return apply_cloth_grab(W, i, predict_particle(i, sim, vel, P));
+    XpbdWind wind;
+    const XpbdWind* wp = nullptr;
+    if (*W.wind_count != 0u) {
+        wind = W.winds[W.row_cloth[i]];
+        if (wind.drag > 0.0f) wp = &wind;
+    }
+    return apply_cloth_grab(W, i, predict_particle(i, sim, vel, P, wp));
 }
 
 // xpbd_substep_post_velocity, xpbd_cpu.rs:393-409, for an unpinned particle: ground plane (extension), then

@@ -74,6 +74,13 @@ struct XpbdGrab {
     uint32_t pad[3];
 };
 
+// Wind on a cloth (extension, off by default): after gravity, every unpinned particle's predicted velocity relaxes
+// toward the wind velocity, v += (wind - v) · (drag · dt).
+struct XpbdWind {
+    float vel[3];
+    float drag;  // 1/s; 0 = no wind
+};
+
 struct XpbdGridSync {
     unsigned int count;
     unsigned int gen;
@@ -159,6 +166,8 @@ struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     unsigned* cloth_iters;          // per cloth: update passes of the current substep
     const XpbdGrab* grabs;          // per cloth
     const uint32_t* grab_count;     // number of cloths with an active grab (device word)
+    const XpbdWind* winds;          // per cloth
+    const uint32_t* wind_count;     // number of cloths with wind (device word)
     unsigned* div_exact;            // 3 slots: pass p of the row kernel takes the exact division when slot p % 3 != 0
     // render triangles (vertex normals)
     uint32_t n_tris;

@@ -59,6 +59,18 @@ size_t cloth_kernel_smem_bytes(uint32_t cap);
 cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTable& T, uint32_t substeps,
                                cudaStream_t st);
 cudaError_t cloth_kernel_prepare();  // opt-in shared-memory sizes (host, once)
+// A whole small batch in one cluster of cl (8 or 16) CTAs, thread per incidence (cloth_jacobi.cu).
+struct SmallBatch {
+    const uint4* rec;       // per incidence, rank-major: {self local, other endpoint (rank << 13 | local), rest, comp}
+    const uint32_t* roff;   // per rank: q + 1 local row starts into the rank's incidences
+    const uint32_t* rbase;  // per rank: first incidence of the rank in rec
+    uint32_t q;             // particles per rank
+    uint32_t m_max;         // largest incidence count of a rank
+};
+size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max);
+bool small_batch_supported(uint32_t cl, uint32_t block, uint32_t q, uint32_t m_max);
+cudaError_t launch_small_batch(uint32_t cl, uint32_t block, const XpbdWorld& W, const SmallBatch& B,
+                               uint32_t substeps, cudaStream_t st);
 
 // ---- cluster Gauss–Seidel (cluster_gs.cu)
 struct ClusterTable {

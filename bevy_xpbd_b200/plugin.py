@@ -245,6 +245,11 @@ class ClothComputePlugin:
         self._check(self._L.xpbd_set_cloth_grab(self._h, cloth, -1 if vertex is None else int(vertex), _ptr(t),
                                                 C.c_float(stiffness)))
 
+    def set_cloth_wind(self, cloth: int, velocity=(0.0, 0.0, 0.0), drag: float = 0.0):
+        """Wind on a cloth (extension): after gravity, v += (velocity - v) * (drag * dt); drag 0 turns it off."""
+        w = np.ascontiguousarray(velocity, np.float32)
+        self._check(self._L.xpbd_set_cloth_wind(self._h, cloth, _ptr(w), C.c_float(drag)))
+
     def set_triangles(self, cloth: int, tri_indices):
         """Render triangles (local vertex indices, 3 per triangle) of a cloth, for `normals`."""
         t = _u32(tri_indices).reshape(-1)

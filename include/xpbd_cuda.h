@@ -177,6 +177,10 @@ int xpbd_commit(xpbd_ctx* ctx);
  * each prediction the cloth's local vertex `vertex` moves by stiffness·(target − x), at most 0.065 per substep
  * (xpbd_cpu.rs:56-63). vertex < 0 releases it. Takes effect from the next frame; no graph recapture. */
 int xpbd_set_cloth_grab(xpbd_ctx* ctx, uint32_t cloth_id, int32_t vertex, const float* target_xyz, float stiffness);
+/* Wind on one cloth (an extension; the reference has no wind): after gravity, the predicted velocity of every unpinned
+ * particle of the cloth relaxes toward `velocity` (3 floats, m/s): v += (velocity - v) * (drag * dt). drag = 0 turns
+ * it off (velocity may then be NULL). Takes effect from the next frame; no graph recapture. */
+int xpbd_set_cloth_wind(xpbd_ctx* ctx, uint32_t cloth_id, const float* velocity, float drag);
 /* Render triangles of a cloth (3 local vertex indices each; before xpbd_commit), for xpbd_read_normals. */
 int xpbd_set_triangles(xpbd_ctx* ctx, uint32_t cloth_id, uint32_t num_tris, const uint32_t* tri_indices);
 /* Vertex normals of the current positions, accumulate_normals + finalize_normals (cloth_sim_jacobi.wgsl:492-547):

@@ -36,7 +36,7 @@ class OracleParams(C.Structure):
         ("solver", C.c_uint32), ("relaxation", C.c_uint32), ("lambda_mode", C.c_uint32),
         ("collision", C.c_uint32), ("thickness", C.c_float), ("coll_scale", C.c_float),
         ("hash_cell", C.c_float), ("ground_enabled", C.c_uint32), ("ground_y", C.c_float), ("damp", C.c_float),
-        ("tolerance", C.c_float), ("warm_start", C.c_uint32),
+        ("tolerance", C.c_float), ("warm_start", C.c_uint32), ("wind", C.c_float * 3), ("wind_drag", C.c_float),
     ]
 
 
@@ -161,7 +161,7 @@ def build_csr(n: int, ci, cj):
 def make_params(p: dict) -> OracleParams:
     o = OracleParams()
     for k, v in p.items():
-        if k in ("gravity", "grab_target"):
+        if k in ("gravity", "grab_target", "wind"):
             getattr(o, k)[:] = [float(x) for x in v]
         elif hasattr(o, k):
             setattr(o, k, v)

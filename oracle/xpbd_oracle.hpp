@@ -520,6 +520,8 @@ struct Params {  // XpbdCpuTimeStepParams, xpbd_cpu.rs:11-26, plus the extension
     float damp;            // exp(-k·dt) evaluated once on the host (xpbd_cpu.rs:402)
     float tolerance;       // extension: stop when the pre-update residual max|C+α̃λ|/rest <= tolerance (0 = off)
     uint32_t warm_start;   // extension: 1 = start from the given λ0 (warm_lambda) when it lowers the residual
+    float wind[3];         // extension: wind velocity; after gravity v += (wind - v) * (wind_drag * dt)
+    float wind_drag;       // 0 = no wind
 };
 
 template <typename T>
@@ -557,6 +559,10 @@ struct Sim {
         V g = {(T)p.gravity[0], (T)p.gravity[1], (T)p.gravity[2]};
         T dt = (T)p.dt;
         v = v + g * dt;
+        if (p.wind_drag > 0.0f) {  // extension: wind (no reference counterpart)
+            V wv = {(T)p.wind[0], (T)p.wind[1], (T)p.wind[2]};
+            v = v + (wv - v) * (T)(p.wind_drag * p.dt);
+        }
         T speed = length(v);
         T max_v = (T)PREDICT_MAX_SPEED;
         if (speed > max_v && speed > (T)0) v = v * (max_v / speed);

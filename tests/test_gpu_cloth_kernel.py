@@ -133,3 +133,40 @@ def test_cloth_kernel_refuses_batches_that_share_a_particle():
     o.set_params(oracle_params(prm, cfg))
     o.substeps(10)
     assert max_abs(plug.positions(), o.state()[0]) == 0.0
+
+
+SMALL = 8  # kernel id of the single-cluster small-batch kernel
+
+
+@pytest.mark.parametrize("relax", [P.RELAX_AVERAGE, P.RELAX_OMEGA], ids=["average", "omega"])
+def test_small_batch_kernel_bit_exact(relax):
+    """A few small cloths in one cluster (thread per incidence, one cluster barrier per pass) against the oracle."""
+    specs = [wl.make_sheet(s, 1.0, 1.0, "corners" if k % 2 else "top_edge", seed=60 + k)
+             for k, s in enumerate([32, 17, 9, 40])]
+    prm = params_for(10, 10, 1.0 if relax == P.RELAX_AVERAGE else 0.32, drag=0.3)
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=relax, solve_substeps=10, jacobi_kernel=5)
+    plug = gpu_sim(specs, prm, cfg)
+    assert plug.stats()["solver_kernel"] == SMALL
+    plug.step(frames=3)
+    for k, sp in enumerate(specs):
+        o = oracle_sim(sp, prm, cfg)
+        o.substeps(30)
+        xo, vo = o.state()
+        assert max_abs(plug.positions(k), xo) == 0.0, k
+        assert max_abs(plug.velocities(k), vo) == 0.0, k
+
+
+@pytest.mark.parametrize("iters", [0, 1, 3], ids=["no_pass", "one_pass", "three_passes"])
+def test_small_batch_kernel_odd_pass_counts_and_grab(iters):
+    """Odd pass counts alternate the two position buffers across substeps; a context grab pulls one vertex."""
+    sp = wl.make_sheet(32, 1.0, 1.0, "corners", seed=64)
+    prm = params_for(10, iters, 1.0)
+    prm.grab_idx, prm.grab_active, prm.grab_target, prm.grab_stiffness = 700, True, (0.2, 0.7, 0.1), 0.28
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
+    plug = gpu_sim(sp, prm, cfg)
+    assert plug.stats()["solver_kernel"] == SMALL  # the default for a 1,024-particle sheet
+    plug.step(frames=2)
+    plug.substep(3)
+    o = oracle_sim(sp, prm, cfg)
+    o.substeps(23)
+    assert max_abs(plug.positions(), o.state()[0]) == 0.0

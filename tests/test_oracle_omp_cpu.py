@@ -51,3 +51,22 @@ def test_openmp_oracle_equals_serial_oracle(name, make, kw, substeps, drag):
     assert np.array_equal(xa, xb) and np.array_equal(va, vb)
     if kw.get("collision"):
         assert np.array_equal(a.collision_pairs(), b.collision_pairs())
+
+
+def test_oracle_wind_changes_only_the_windy_run():
+    """The wind extension of the oracle's predict: off (drag 0) leaves the reference result, on moves the sheet."""
+    from tests.helpers import oracle_params
+    sp = wl.make_sheet(12, 1.0, 1.0, "top_edge", seed=3)
+    prm = params_for(10, 10, 1.0)
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
+    a = oracle_sim(sp, prm, cfg)
+    b = oracle_sim(sp, prm, cfg)
+    c = oracle_sim(sp, prm, cfg)
+    d = oracle_params(prm, cfg)
+    b.set_params(dict(d, wind=(4.0, 0.0, 0.0), wind_drag=0.0))
+    c.set_params(dict(d, wind=(4.0, 0.0, 0.0), wind_drag=1.0))
+    for s in (a, b, c):
+        s.substeps(20)
+    assert np.array_equal(a.state()[0], b.state()[0])
+    assert np.abs(a.state()[0] - c.state()[0]).max() > 1e-4
+    assert c.state()[0][:, 0].mean() > a.state()[0][:, 0].mean()
