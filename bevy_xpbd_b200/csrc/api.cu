@@ -978,7 +978,8 @@ static bool patches_usable(xpbd_ctx* ctx) {
 }
 
 // Tables of the cloth-resident Jacobi kernel, built on its first selection. Usable when every cloth fits a cluster
-// of at most 8 CTAs (XPBD_CLOTH_RANK_MAX particles per CTA) and its color batches are particle-disjoint (then each
+// (8 CTAs of XPBD_CLOTH_RANK_MAX particles, or 16 of 4,096 where the device runs such clusters) and its color
+// batches are particle-disjoint (then each
 // particle's neighbour-table row is ordered by color, which the kernel's summation order relies on); otherwise the
 // schedule keeps the thread-per-particle kernel and the reason is left in last_error.
 static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
@@ -992,11 +993,14 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
     std::vector<std::vector<uint2>> rec(C);
     std::vector<std::vector<float>> comp(C);
     std::atomic<int> bad{0};  // 1: a cloth too large, 2: batches share a particle
+    bool class_ok[kClothClasses];
+    CK(cloth_kernel_prepare(), "cloth kernel attributes");
+    for (int t = 0; t < kClothClasses; ++t) class_ok[t] = cloth_class_launchable(t);
     parallel_for(C, [&](uint32_t k) {
         const ClothHost& c = ctx->cloths[k];
         int id = -1;
         for (int t = 0; t < kClothClasses; ++t)
-            if ((uint64_t)kClothClass[t].cl * kClothClass[t].rank_cap >= c.n) {
+            if ((uint64_t)kClothClass[t].cl * kClothClass[t].rank_cap >= c.n && class_ok[t]) {
                 id = t;
                 break;
             }
@@ -1031,7 +1035,8 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
         std::vector<uint32_t> cur(sg.begin(), sg.end() - 1);
         rec[k].resize(sg.back());
         comp[k].resize(sg.back());
-        auto ep = [qq](uint32_t p) { return ((p / qq) << XPBD_CLOTH_EP_BITS) | (p % qq); };
+        const uint32_t eb = cloth_ep_bits(cl);
+        auto ep = [qq, eb](uint32_t p) { return ((p / qq) << eb) | (p % qq); };
         for (uint32_t b = 0; b < nb; ++b)
             for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
                 const uint32_t e = c.perm[t];
@@ -1047,7 +1052,7 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
         ncol[k] = nb;
     });
     if (bad) {
-        ctx->last_error = bad == 1 ? "cloth-resident Jacobi: a cloth exceeds 8 CTAs of shared memory"
+        ctx->last_error = bad == 1 ? "cloth-resident Jacobi: a cloth exceeds a cluster's shared memory"
                                    : "cloth-resident Jacobi: a color batch shares a particle";
         return XPBD_OK;
     }
@@ -1140,7 +1145,7 @@ static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
         for (uint32_t i = 0; i < ctx->cloths[k].n; ++i) cloth_of[ctx->cloths[k].vtx_off + i] = k;
     for (uint32_t cl : {16u, 8u}) {
         const uint32_t q = (N + cl - 1) / cl;
-        if (q > 1024 || q >= (1u << XPBD_CLOTH_EP_BITS)) continue;
+        if (q > 1024) continue;
         std::vector<uint4> rec;
         std::vector<uint32_t> lroff((size_t)cl * (q + 1), 0), rbase(cl, 0);
         uint32_t m_max = 0;
@@ -1155,7 +1160,7 @@ static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
                                                          : pal[(size_t)cloth_of[p] * XPBD_PALETTE + (inc[k].x >> 28)];
                     uint32_t cb;
                     memcpy(&cb, &comp, 4);
-                    rec.push_back(make_uint4(p - p0, ((o / q) << XPBD_CLOTH_EP_BITS) | (o % q), inc[k].y, cb));
+                    rec.push_back(make_uint4(p - p0, ((o / q) << 16) | (o % q), inc[k].y, cb));
                 }
             }
             const uint32_t m = (uint32_t)rec.size() - rbase[r];

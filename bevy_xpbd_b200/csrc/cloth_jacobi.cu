@@ -33,7 +33,8 @@ namespace xpbd {
 // classes fit four, two and one CTA per SM in its 228 KB of shared memory.
 const ClothClass kClothClass[kClothClasses] = {
     {1, 256, 1760}, {1, 512, 3520}, {1, 1024, XPBD_CLOTH_RANK_MAX},
-    {2, 1024, XPBD_CLOTH_RANK_MAX}, {4, 1024, XPBD_CLOTH_RANK_MAX}, {8, 1024, XPBD_CLOTH_RANK_MAX}};
+    {2, 1024, XPBD_CLOTH_RANK_MAX}, {4, 1024, XPBD_CLOTH_RANK_MAX}, {8, 1024, XPBD_CLOTH_RANK_MAX},
+    {16, 1024, 4096}};
 
 size_t cloth_kernel_smem_bytes(uint32_t cap) { return 2 * (size_t)cap * sizeof(float4); }
 
@@ -48,16 +49,18 @@ __device__ __forceinline__ void cloth_sync() {
 // Shared-memory address of endpoint `ep` ((rank << 13) | local) in the array starting at `base` of every CTA.
 template <int CL>
 __device__ __forceinline__ float4 ld_ep(uint32_t base, uint32_t ep, uint32_t rank) {
-    const uint32_t a = base + (ep & ((1u << XPBD_CLOTH_EP_BITS) - 1u)) * 16u;
+    constexpr uint32_t B = cloth_ep_bits(CL);
+    const uint32_t a = base + (ep & ((1u << B) - 1u)) * 16u;
     if (CL == 1) return ld_local(a);
-    const uint32_t r = ep >> XPBD_CLOTH_EP_BITS;
+    const uint32_t r = ep >> B;
     return r == rank ? ld_local(a) : ld_dsmem(map_rank(a, r));
 }
 template <int CL>
 __device__ __forceinline__ void add_ep(uint32_t base, uint32_t ep, uint32_t rank, float tx, float ty, float tz,
                                        bool negate) {
-    const uint32_t a = base + (ep & ((1u << XPBD_CLOTH_EP_BITS) - 1u)) * 16u;
-    const uint32_t r = CL == 1 ? 0u : ep >> XPBD_CLOTH_EP_BITS;
+    constexpr uint32_t B = cloth_ep_bits(CL);
+    const uint32_t a = base + (ep & ((1u << B) - 1u)) * 16u;
+    const uint32_t r = CL == 1 ? 0u : ep >> B;
     const bool local = CL == 1 || r == rank;
     const uint32_t ra = local ? a : map_rank(a, r);
     float4 s = local ? ld_local(a) : ld_dsmem(ra);
@@ -222,8 +225,31 @@ static const void* cloth_fn_of(int cls) {
         case 3: return cloth_fn<2, 1024>();
         case 4: return cloth_fn<4, 1024>();
         case 5: return cloth_fn<8, 1024>();
+        case 6: return cloth_fn<16, 1024>();
         default: return nullptr;
     }
+}
+
+bool cloth_class_launchable(int cls) {
+    const ClothClass& K = kClothClass[cls];
+    if (K.cl <= 8) return true;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(K.cl, 1, 1);
+    cfg.blockDim = dim3(K.block, 1, 1);
+    cfg.dynamicSmemBytes = cloth_kernel_smem_bytes(K.rank_cap);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = K.cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, cloth_fn_of(cls), &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return clusters >= 1;
 }
 
 cudaError_t cloth_kernel_prepare() {
@@ -231,8 +257,8 @@ cudaError_t cloth_kernel_prepare() {
         const int bytes = (int)cloth_kernel_smem_bytes(kClothClass[c].rank_cap);
         cudaError_t e = cudaFuncSetAttribute(cloth_fn_of(c), cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         if (e != cudaSuccess) return e;
-        if (kClothClass[c].cl > 1) {
-            e = cudaFuncSetAttribute(cloth_fn_of(c), cudaFuncAttributeNonPortableClusterSizeAllowed, 0);
+        if (kClothClass[c].cl > 8) {
+            e = cudaFuncSetAttribute(cloth_fn_of(c), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
             if (e != cudaSuccess) return e;
         }
     }
@@ -317,8 +343,8 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
             for (uint32_t k = tid; k < m; k += nthr) {
                 const uint4 r = s_rec[k];
                 const float4 ps = ld_local(src + r.x * 16u);
-                const uint32_t ro = r.y >> XPBD_CLOTH_EP_BITS;
-                const uint32_t ao = src + (r.y & ((1u << XPBD_CLOTH_EP_BITS) - 1u)) * 16u;
+                const uint32_t ro = r.y >> 16;  // {rank << 16 | local}
+                const uint32_t ao = src + (r.y & 0xFFFFu) * 16u;
                 const float4 po = ro == rank ? ld_local(ao) : ld_dsmem(map_rank(ao, ro));
                 const F3 gv = sub3(f3(ps), f3(po));
                 const float len = len3(gv);

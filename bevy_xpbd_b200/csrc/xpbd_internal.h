@@ -116,7 +116,7 @@ struct XpbdPatch {
 
 // Cloth-resident Jacobi (jacobi_cloth_kernel): one CTA, or a cluster of `cl` CTAs, holds a whole cloth in shared
 // memory for a frame. Rank r of the cluster owns the cloth-local particles [r·q, min(n, (r+1)·q)). A constraint
-// endpoint is addressed as (rank << 13) | local index. Records are grouped by (color, rank): seg[seg_base + c·cl + r]
+// endpoint is addressed as (rank << b) | local index, b = cloth_ep_bits(cl). Records are grouped by (color, rank): seg[seg_base + c·cl + r]
 // is the first record of color c processed by rank r (the last entry closes the cloth's range).
 struct XpbdClothDesc {
     uint32_t vtx_off;   // first particle of the cloth in the packed batch
@@ -127,9 +127,11 @@ struct XpbdClothDesc {
     uint32_t cl;        // CTAs of the cluster that solves the cloth
     uint32_t pad[2];
 };
-#define XPBD_CLOTH_EP_BITS 13
-#define XPBD_CLOTH_RANK_MAX 7168u     // particles per CTA: 2 x 16 B of shared memory each (224 KB)
-#define XPBD_CLOTH_MAX_CL 8u
+#define XPBD_CLOTH_EP_BITS 13          // local index bits of an endpoint for clusters of up to 8 CTAs
+#define XPBD_CLOTH_RANK_MAX 7168u      // particles per CTA: 2 x 16 B of shared memory each (224 KB)
+#define XPBD_CLOTH_MAX_CL 16u
+// clusters of 16 CTAs (non-portable size) need four rank bits: 12 local bits, at most 4,096 particles per CTA
+__host__ __device__ constexpr uint32_t cloth_ep_bits(uint32_t cl) { return cl > 8 ? 12u : 13u; }
 
 struct XpbdWorld {  // device pointers + sizes, passed by value to kernels
     uint32_t n, e, n_inc, n_tiles, n_colors, n_cloths;

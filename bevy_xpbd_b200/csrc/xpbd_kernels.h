@@ -53,15 +53,16 @@ struct ClothSolveTable {
 struct ClothClass {
     uint32_t cl, block, rank_cap;
 };
-constexpr int kClothClasses = 6;
+constexpr int kClothClasses = 7;
 extern const ClothClass kClothClass[kClothClasses];
 size_t cloth_kernel_smem_bytes(uint32_t cap);
 cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTable& T, uint32_t substeps,
                                cudaStream_t st);
 cudaError_t cloth_kernel_prepare();  // opt-in shared-memory sizes (host, once)
+bool cloth_class_launchable(int cls);  // a cluster of the class fits on this device
 // A whole small batch in one cluster of cl (8 or 16) CTAs, thread per incidence (cloth_jacobi.cu).
 struct SmallBatch {
-    const uint4* rec;       // per incidence, rank-major: {self local, other endpoint (rank << 13 | local), rest, comp}
+    const uint4* rec;       // per incidence, rank-major: {self local, other endpoint (rank << 16 | local), rest, comp}
     const uint32_t* roff;   // per rank: q + 1 local row starts into the rank's incidences
     const uint32_t* rbase;  // per rank: first incidence of the rank in rec
     uint32_t q;             // particles per rank

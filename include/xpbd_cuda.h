@@ -103,13 +103,15 @@ typedef struct xpbd_solver_opts {
     uint32_t blocks_per_sm;           /* 0 = autotuned / default */
     uint32_t warm_start;              /* convergence solve start: XPBD_WARM_* (0 = plain, λ = 0) */
     uint32_t cluster_ctas;            /* Gauss–Seidel in one thread-block cluster: 0 auto, 1 off, 8 or 16 CTAs */
-    uint32_t jacobi_kernel;           /* Jacobi: 0 default (= 4 where it applies, else 3), 1 warp tiles, 2 shared-
+    uint32_t jacobi_kernel;           /* Jacobi: 0 default (= 5, else 4 where they apply, else 3), 1 warp tiles, 2 shared-
                                          memory patches (their tables are built by the first call that selects them,
                                          or by xpbd_autotune, which tries them for plain Jacobi), 3 thread per
                                          particle, 4 cloth-resident (each cloth in the shared memory of one CTA or a
-                                         cluster of up to 8 for a whole frame, each constraint solved once per pass;
-                                         λ cleared per pass, no collision, every cloth at most 57,344 particles with
-                                         particle-disjoint color batches — otherwise 3 runs) */
+                                         cluster of up to 16 for a whole frame, each constraint solved once per
+                                         pass; λ cleared per pass, no collision, every cloth at most 65,536
+                                         particles with particle-disjoint color batches — otherwise 3 runs),
+                                         5 small batch (at most 8,192 particles: the whole batch in one cluster,
+                                         thread per incidence; the default up to 4,096 particles) */
     float tolerance;                  /* > 0 (or warm_start != 0): convergence solve — Jacobi, λ kept per substep,
                                          iterate until max |C + α̃λ|/rest <= tolerance, at most inner_iterations */
     uint32_t reserved[3];

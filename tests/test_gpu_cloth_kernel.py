@@ -1,7 +1,7 @@
 """The cloth-resident Jacobi kernel (jacobi_kernel 4, kernel id 7: each cloth in the shared memory of one CTA or of a
 thread-block cluster for a whole frame, each constraint solved once per pass, colors summed in order) against the
 CPU oracle of xpbd_cpu.rs, bit for bit: every launch class (single CTAs of 256 / 512 / 1024 threads, clusters of
-2, 4 and 8 CTAs), both relaxations, per-cloth grabs, no-iteration substeps, single substeps, and the fallback to the
+2, 4, 8 and 16 CTAs), both relaxations, per-cloth grabs, no-iteration substeps, single substeps, and the fallback to the
 thread-per-particle kernel when a cloth's color batches share a particle."""
 import numpy as np
 import pytest
@@ -24,8 +24,8 @@ def _cfg(**kw):
 
 
 # sides whose particle counts land in every launch class: <= 1,760 / 3,520 / 7,168 particles on one CTA, then
-# clusters of 2 (<= 14,336), 4 (<= 28,672) and 8 (<= 57,344) CTAs
-SIDES = [12, 41, 42, 59, 60, 84, 85, 119, 120, 169, 170, 239]
+# clusters of 2 (<= 14,336), 4 (<= 28,672), 8 (<= 57,344) and 16 (<= 65,536) CTAs
+SIDES = [12, 41, 42, 59, 60, 84, 85, 119, 120, 169, 170, 239, 240, 256]
 
 
 @pytest.fixture(scope="module")
@@ -45,7 +45,7 @@ def test_cloth_kernel_every_launch_class_bit_exact(mixed_batch, relax):
     plug = gpu_sim(mixed_batch, prm, cfg)
     st = plug.stats()
     assert st["solver_kernel"] == CLOTH
-    assert st["cluster_ctas"] == 8
+    assert st["cluster_ctas"] == 16
     plug.step(frames=2)
     for k, sp in enumerate(mixed_batch):
         o = oracle_sim(sp, prm, cfg, omp=True)

@@ -211,8 +211,12 @@ def test_learned_warm_start_bit_exact_against_oracle_with_same_lambda0():
 
 
 def test_learned_warm_start_reduces_iterations(record_property):
-    """Train on one batch of config-3 cloths (varied stiffness), then run a different batch plain and learned from the
-    same initial state: the learned start needs fewer update passes per cloth-substep to reach the tolerance."""
+    """Train on one batch of config-3 cloths (varied stiffness), then run a different batch plain, previous-λ and learned
+    from the same initial state. The learned start needs fewer update passes per cloth-substep than the plain start.
+    Against the previous substep's λ — the method the network extends (it is one of its inputs, and the network
+    predicts the change over it) — the gain is recorded (passes_gain_over_previous) and the learned start, its predicted
+    change shrunk by 0.15 toward the previous multiplier, must not take more passes than previous-λ plus 5 %: on these
+    cloths the network adds little to what that input carries."""
     cap = 1024
     prm = params_for(10, cap, 1.0, drag=0.01)
     cfg = _cfg(solve_substeps=10)
@@ -226,7 +230,7 @@ def test_learned_warm_start_reduces_iterations(record_property):
                              plug.mlp_train(500, batch=4096, lr=3e-4, seed=12)])
     assert np.all(np.isfinite(losses))
     assert losses[-200:].mean() < losses[:20].mean()      # per-batch losses are heavy-tailed: compare means
-    params, norm = plug.mlp_params()
+    params, norm = P.mlp_scale_change(*plug.mlp_params(), 0.15)  # the change shrunk as the bench chooses it
     runs = {}
     for name, warm in (("plain", P.WARM_NONE), ("previous", P.WARM_PREVIOUS), ("learned", P.WARM_LEARNED)):
         q = gpu_sim(test, prm, cfg)
@@ -237,7 +241,10 @@ def test_learned_warm_start_reduces_iterations(record_property):
         st = q.stats()
         runs[name] = st["converge_iterations"] / st["converge_substeps"]
         record_property(f"passes_per_cloth_substep_{name}", runs[name])
+    record_property("passes_gain_over_previous", runs["previous"] / runs["learned"])
+    record_property("passes_gain_over_plain", runs["plain"] / runs["learned"])
     assert runs["learned"] < runs["plain"]
+    assert runs["learned"] <= 1.05 * runs["previous"]
 
 
 def test_data_parallel_training_step_matches_oracle():
