@@ -329,7 +329,7 @@ def roofline(w: dict, mean_ms: float, kernel: str, peaks: dict) -> dict:
 
 def fixed_schedule(args) -> bool:
     return (args.no_autotune or args.jacobi_kernel is not None or args.block is not None or args.bps is not None
-            or args.cluster is not None)
+            or args.cluster is not None or args.gs_strips is not None)
 
 
 def apply_schedule(w: dict, plug, args):
@@ -345,6 +345,8 @@ def apply_schedule(w: dict, plug, args):
         cfg.blocks_per_sm = args.bps
     if args.cluster is not None:
         cfg.cluster_ctas = args.cluster
+    if args.gs_strips is not None:
+        cfg.gs_strips = args.gs_strips
     plug.set_params(w["params"], cfg)
     return cfg
 
@@ -362,7 +364,7 @@ def run_gpu_workload(name: str, args, rank: int, world: int, device: int, peaks:
     cloth_steps = w["total_cloths"] * steps
     kernel = {0: "jacobi_persistent_kernel", 1: "gs_persistent_kernel", 2: "jacobi_patch_kernel",
               3: "gs_cluster_kernel", 5: "jacobi_row_kernel", 6: "jacobi_converge_kernel",
-              7: "jacobi_cloth_kernel"}[st["solver_kernel"]]
+              7: "jacobi_cloth_kernel", 8: "jacobi_small_batch_kernel", 9: "gs_strip_kernel"}[st["solver_kernel"]]
     res = {
         "value": round(cloth_steps / (total_ms * 1e-3), 2),
         "ms_per_step": round(mean_ms, 4),
@@ -730,6 +732,7 @@ def main():
     ap.add_argument("--block", type=int, default=None)
     ap.add_argument("--bps", type=int, default=None)
     ap.add_argument("--cluster", type=int, default=None, help="Gauss-Seidel cluster size (0 = grid kernel)")
+    ap.add_argument("--gs-strips", type=int, default=None, help="Gauss-Seidel over this many clusters (strips)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

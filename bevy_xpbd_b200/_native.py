@@ -63,7 +63,8 @@ class SolverOpts(C.Structure):
         ("ring_depth", C.c_uint32), ("ground_enabled", C.c_uint32), ("ground_y", C.c_float),
         ("use_graphs", C.c_uint32), ("barrier_timeout_ms", C.c_float), ("block_threads", C.c_uint32),
         ("blocks_per_sm", C.c_uint32), ("warm_start", C.c_uint32), ("cluster_ctas", C.c_uint32),
-        ("jacobi_kernel", C.c_uint32), ("tolerance", C.c_float), ("reserved", C.c_uint32 * 3),
+        ("jacobi_kernel", C.c_uint32), ("tolerance", C.c_float), ("gs_strips", C.c_uint32),
+        ("reserved", C.c_uint32 * 2),
     ]
 
 

@@ -116,6 +116,9 @@ struct xpbd_ctx {
     cudaStream_t cls_stream[kClothClasses] = {};
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_join[kClothClasses] = {};
+    // Gauss–Seidel strips (kernel id 9)
+    StripTable strip{};
+    uint32_t strip_cl = 0, strip_s = 0, strip_block = 0;
     // single-cluster small batch (kernel id 8)
     bool small_ok = false, small_tried = false;
     SmallBatch small{};
@@ -952,6 +955,109 @@ static int ensure_patches(xpbd_ctx* ctx, bool* usable) {
     return XPBD_OK;
 }
 
+// Gauss–Seidel strips: the packed particles split over `strips` clusters of `cl` CTAs (consecutive ranges); the
+// particles joined by a constraint to another strip are kept in global memory slots. Built (or rebuilt for another
+// shape) when selected; false if the shape does not fit (the schedule then uses the single-cluster or grid kernel).
+static bool build_strip_table(xpbd_ctx* ctx, uint32_t cl, uint32_t strips) {
+    if (ctx->strip_cl == cl && ctx->strip_s == strips) return true;
+    const uint32_t N = ctx->W.n, ncta = cl * strips, ncol = ctx->W.n_colors;
+    if (N == 0 || ncol == 0) return false;
+    const uint32_t q = (N + ncta - 1) / ncta;
+    if (q > 4096 || q * (ncta - 1) >= N) return false;  // every CTA owns particles
+    const uint32_t block = std::min<uint32_t>(512, std::max<uint32_t>(128, (q + 127) / 128 * 128));
+    if (!strip_gs_supported(cl, strips, block, q)) {
+        cudaGetLastError();
+        return false;
+    }
+    const std::vector<uint4>& con = ctx->con_host;
+    auto cta = [q](uint32_t p) { return p / q; };
+    auto strip = [q, cl](uint32_t p) { return p / q / cl; };
+    std::vector<uint32_t> slot(N, 0xFFFFFFFFu);
+    std::vector<uint8_t> bnd(N, 0);
+    for (const uint4& r : con)
+        if (strip(r.x) != strip(r.y)) slot[r.x] = slot[r.y] = 0u;
+    uint32_t ns = 0;
+    for (uint32_t p = 0; p < N; ++p)
+        if (slot[p] == 0u) slot[p] = ns++;
+    const auto shared = [&](uint32_t p) { return slot[p] != 0xFFFFFFFFu; };
+    for (const uint4& r : con)
+        if (cta(r.x) != cta(r.y)) bnd[r.x] = bnd[r.y] = 1;
+    auto kind = [&](const uint4& r) -> uint32_t {
+        if (shared(r.x) || shared(r.y)) return 0;
+        if (cta(r.x) != cta(r.y) || bnd[r.x] || bnd[r.y]) return 1;
+        return 2;
+    };
+    auto code = [&](uint32_t p) {
+        return shared(p) ? (0x80000000u | slot[p]) : (((cta(p) % cl) << 16) | (p - cta(p) * q));
+    };
+    std::vector<uint32_t> off((size_t)ncol * ncta * 3 + 1, 0);
+    for (uint32_t c = 0; c < ncol; ++c)
+        for (uint32_t e = ctx->color_off_host[c]; e < ctx->color_off_host[c + 1]; ++e)
+            ++off[((size_t)c * ncta + cta(con[e].x)) * 3 + kind(con[e]) + 1];
+    for (size_t k = 1; k < off.size(); ++k) off[k] += off[k - 1];
+    std::vector<uint32_t> cur(off.begin(), off.end() - 1);
+    std::vector<uint4> rec(con.size());
+    // CTAs touching each shared particle: its owner and the solvers of its constraints
+    std::vector<std::vector<uint32_t>> touch(ns);
+    for (uint32_t p = 0; p < N; ++p)
+        if (shared(p)) touch[slot[p]].push_back(cta(p));
+    for (uint32_t c = 0; c < ncol; ++c)
+        for (uint32_t e = ctx->color_off_host[c]; e < ctx->color_off_host[c + 1]; ++e) {
+            const uint4 r = con[e];
+            rec[cur[((size_t)c * ncta + cta(r.x)) * 3 + kind(r)]++] = make_uint4(code(r.x), code(r.y), r.z, r.w);
+            if (shared(r.x)) touch[slot[r.x]].push_back(cta(r.x));
+            if (shared(r.y)) touch[slot[r.y]].push_back(cta(r.x));
+        }
+    std::vector<std::vector<uint32_t>> dep(ncta);
+    for (auto& t : touch) {
+        std::sort(t.begin(), t.end());
+        t.erase(std::unique(t.begin(), t.end()), t.end());
+        for (uint32_t a : t)
+            for (uint32_t b : t)
+                if (a / cl != b / cl) dep[a].push_back(b);
+    }
+    std::vector<uint32_t> deps, dep_off(ncta + 1, 0);
+    for (uint32_t a = 0; a < ncta; ++a) {
+        std::sort(dep[a].begin(), dep[a].end());
+        dep[a].erase(std::unique(dep[a].begin(), dep[a].end()), dep[a].end());
+        deps.insert(deps.end(), dep[a].begin(), dep[a].end());
+        dep_off[a + 1] = (uint32_t)deps.size();
+    }
+    cudaError_t err = cudaSuccess;
+    uint4* d_rec = dev_alloc<uint4>(ctx, std::max<size_t>(1, rec.size()), &err);
+    uint32_t* d_off = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, off.size(), &err) : nullptr;
+    uint32_t* d_slot = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, N, &err) : nullptr;
+    float4* d_gx = err == cudaSuccess ? dev_alloc<float4>(ctx, std::max<uint32_t>(1, ns), &err) : nullptr;
+    unsigned* d_flags = err == cudaSuccess ? dev_alloc<unsigned>(ctx, ncta, &err) : nullptr;
+    uint32_t* d_deps = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, std::max<size_t>(1, deps.size()), &err) : nullptr;
+    uint32_t* d_dep_off = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, dep_off.size(), &err) : nullptr;
+    if (err != cudaSuccess) return false;
+    if (cudaMemcpy(d_rec, rec.data(), rec.size() * 16, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_slot, slot.data(), (size_t)N * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(d_flags, 0, ncta * 4) != cudaSuccess ||
+        (!deps.empty() && cudaMemcpy(d_deps, deps.data(), deps.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) ||
+        cudaMemcpy(d_dep_off, dep_off.data(), dep_off.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    ctx->strip = StripTable{d_rec, d_off, d_slot, d_gx, d_flags, d_deps, d_dep_off, q, ncta, ncol};
+    ctx->strip_cl = cl;
+    ctx->strip_s = strips;
+    ctx->strip_block = block;
+    return true;
+}
+
+// Strips for Gauss–Seidel (λ cleared per iteration, no collision): `want` strips, or none when 0 / 1.
+static bool pick_strips(xpbd_ctx* ctx, uint32_t want) {
+    if (ctx->opts.solver != XPBD_SOLVER_GAUSS_SEIDEL || ctx->opts.lambda_mode != XPBD_LAMBDA_RESET_PER_ITERATION ||
+        ctx->opts.collision != XPBD_COLLISION_NONE || want < 2)
+        return false;
+    for (uint32_t cl : {16u, 8u}) {
+        if (ctx->opts.cluster_ctas > 1 && ctx->opts.cluster_ctas != cl) continue;
+        if (build_strip_table(ctx, cl, want)) return true;
+    }
+    return false;
+}
+
 // Cluster path: Gauss–Seidel, λ cleared per iteration, every particle fits in the cluster's shared memory.
 static uint32_t pick_cluster(xpbd_ctx* ctx, uint32_t want, uint32_t block) {
     if (ctx->opts.solver != XPBD_SOLVER_GAUSS_SEIDEL || ctx->opts.lambda_mode != XPBD_LAMBDA_RESET_PER_ITERATION)
@@ -1235,6 +1341,18 @@ static void choose_schedule(xpbd_ctx* ctx) {
     uint32_t block = ctx->opts.block_threads ? ctx->opts.block_threads : 256;
     if (block != 128 && block != 256 && block != 512 && block != 1024) block = 256;
     const uint32_t cblock = ctx->opts.block_threads ? block : 1024;
+    if (pick_strips(ctx, ctx->opts.gs_strips)) {
+        ctx->kernel = 9;
+        ctx->cl = 0;
+        ctx->block = ctx->strip_block;
+        ctx->grid = ctx->strip.ncta;
+        ctx->coop = false;
+        ctx->stats.grid_blocks = ctx->strip.ncta;
+        ctx->stats.block_threads = ctx->strip_block;
+        ctx->stats.solver_kernel = 9;
+        ctx->stats.cluster_ctas = ctx->strip_cl;
+        return;
+    }
     ctx->cl = pick_cluster(ctx, ctx->opts.cluster_ctas, cblock);
     if (ctx->cl) {
         ctx->kernel = 1;
@@ -1396,6 +1514,10 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
         *launches += 1;
         return launch_small_batch(ctx->small_cl, ctx->small_block, ctx->W, ctx->small, S, st);
     }
+    if (ctx->kernel == 9) {  // no collision (pick_strips)
+        *launches += 1;
+        return launch_strip_gs(ctx->strip_cl, ctx->strip_block, ctx->W, ctx->strip, S, st);
+    }
     if (!coll) {
         e = launch_substeps(ctx, kEndFinalize, S, 0, 0, st);
         *launches += 1;
@@ -1434,10 +1556,10 @@ static cudaError_t enqueue_frame(xpbd_ctx* ctx, cudaStream_t st, uint64_t* launc
 static std::string schedule_key(xpbd_ctx* ctx) {
     const xpbd_solver_opts& o = ctx->opts;
     char buf[256];
-    snprintf(buf, sizeof(buf), "%u/%u/%u/%u/%u/%u/%u/%u/%d/%p/%u/%u/%u/%u/%u", o.solver, o.substeps, o.collision,
-             o.collision_every_n_substeps, ctx->tsp.inner_iterations, ctx->block, ctx->grid, (int)ctx->coop,
-             (int)(o.coll_scale > 1e-12f), (void*)ctx->stream, o.hash_table_bits, o.ring_depth, ctx->cl, ctx->kernel,
-             o.warm_start);
+    snprintf(buf, sizeof(buf), "%u/%u/%u/%u/%u/%u/%u/%u/%d/%p/%u/%u/%u/%u/%u/%u/%u", o.solver, o.substeps,
+             o.collision, o.collision_every_n_substeps, ctx->tsp.inner_iterations, ctx->block, ctx->grid,
+             (int)ctx->coop, (int)(o.coll_scale > 1e-12f), (void*)ctx->stream, o.hash_table_bits, o.ring_depth,
+             ctx->cl, ctx->kernel, o.warm_start, ctx->strip_cl, ctx->strip_s);
     return buf;
 }
 
@@ -1584,6 +1706,8 @@ static int read_status(xpbd_ctx* ctx) {
     // clear the status and the barrier state so the context stays usable
     CK(cudaMemsetAsync(ctx->W.status, 0, 4 * sizeof(int), ctx->stream), "memset");
     CK(cudaMemsetAsync(ctx->W.sync, 0, sizeof(XpbdGridSync), ctx->stream), "memset");
+    if (ctx->strip.flags)  // a strip launch that gave up leaves its step flags uneven: start them over
+        CK(cudaMemsetAsync(ctx->strip.flags, 0, ctx->strip.ncta * sizeof(unsigned), ctx->stream), "memset");
     CK(cudaStreamSynchronize(ctx->stream), "stream sync");
     if (h[0] & XPBD_DEV_BARRIER_TIMEOUT) return fail(ctx, XPBD_ERR_BARRIER_TIMEOUT, "grid barrier wait timed out");
     if (h[0] & XPBD_DEV_NONFINITE) return fail(ctx, XPBD_ERR_DEVICE_NONFINITE, "non-finite position or velocity");

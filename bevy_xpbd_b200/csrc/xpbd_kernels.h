@@ -73,6 +73,22 @@ bool small_batch_supported(uint32_t cl, uint32_t block, uint32_t q, uint32_t m_m
 cudaError_t launch_small_batch(uint32_t cl, uint32_t block, const XpbdWorld& W, const SmallBatch& B,
                                uint32_t substeps, cudaStream_t st);
 
+// ---- Gauss–Seidel over several clusters (strip_gs.cu)
+struct StripTable {
+    const uint4* rec;        // {code i, code j, rest, comp} grouped by (color, CTA, kind 0/1/2)
+    const uint32_t* off;     // 3 · ncolors · ncta + 1 group starts
+    const uint32_t* slot;    // per particle: its global slot when shared between strips, else 0xFFFFFFFF
+    float4* gx;              // shared particles' positions during a frame
+    unsigned* flags;         // per CTA: steps completed (monotonic across launches)
+    const uint32_t* deps;    // CTAs of other strips sharing particles with a CTA, dep_off[cta] .. dep_off[cta + 1]
+    const uint32_t* dep_off;
+    uint32_t q, ncta, ncolors;
+};
+size_t strip_gs_smem_bytes(uint32_t q);
+bool strip_gs_supported(uint32_t cl, uint32_t strips, uint32_t block, uint32_t q);
+cudaError_t launch_strip_gs(uint32_t cl, uint32_t block, const XpbdWorld& W, const StripTable& T, uint32_t substeps,
+                            cudaStream_t st);
+
 // ---- cluster Gauss–Seidel (cluster_gs.cu)
 struct ClusterTable {
     const uint4* rec;    // constraint records grouped by (color, owning rank)

@@ -123,6 +123,7 @@ class ClothSimConfig:
     cluster_ctas: int = 0
     jacobi_kernel: int = 0
     tolerance: float = 0.0
+    gs_strips: int = 0
 
     def to_c(self) -> N.SolverOpts:
         o = N.SolverOpts()
@@ -137,6 +138,7 @@ class ClothSimConfig:
         o.cluster_ctas = self.cluster_ctas
         o.jacobi_kernel = self.jacobi_kernel
         o.tolerance = self.tolerance
+        o.gs_strips = self.gs_strips
         return o
 
 
@@ -441,6 +443,7 @@ class ClothComputePlugin:
         self.config.block_threads, self.config.blocks_per_sm = o.block_threads, o.blocks_per_sm
         self.config.cluster_ctas = o.cluster_ctas
         self.config.jacobi_kernel = o.jacobi_kernel
+        self.config.gs_strips = o.gs_strips
         return self.config
 
     # ---- collision introspection

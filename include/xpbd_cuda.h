@@ -114,7 +114,10 @@ typedef struct xpbd_solver_opts {
                                          thread per incidence; the default up to 4,096 particles) */
     float tolerance;                  /* > 0 (or warm_start != 0): convergence solve — Jacobi, λ kept per substep,
                                          iterate until max |C + α̃λ|/rest <= tolerance, at most inner_iterations */
-    uint32_t reserved[3];
+    uint32_t gs_strips;               /* Gauss–Seidel over several clusters: 0 auto, 1 off, S >= 2 strips of
+                                         cluster_ctas (16, or 8) CTAs each, particles shared between strips in
+                                         global memory and ordered by per-CTA step flags (bounded waits) */
+    uint32_t reserved[2];
 } xpbd_solver_opts;
 
 /* One cloth: the arrays of ClothMeshData / ClothSimConfig (mesh_prep.rs:103-131, cloth_compute.rs:140-179). All
