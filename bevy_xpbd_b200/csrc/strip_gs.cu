@@ -133,6 +133,21 @@ __device__ __forceinline__ void strip_solve(const uint4 r, uint32_t xs_base, con
 
 }  // namespace
 
+// Record ranges of one (color, CTA) group by kind, and this thread's first record of each kind.
+struct Group {
+    uint32_t k[4];
+    uint4 r[3];
+};
+__device__ __forceinline__ Group load_group(const StripTable& T, uint32_t c, uint32_t cta, uint32_t tid) {
+    Group g;
+    const uint32_t* off = T.off + ((size_t)c * T.ncta + cta) * 3;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) g.k[q] = __ldg(off + q);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) g.r[q] = g.k[q] + tid < g.k[q + 1] ? __ldg(T.rec + g.k[q] + tid) : make_uint4(0, 0, 0, 0);
+    return g;
+}
+
 // Waits until every dependency of this CTA has completed step `target` (flag - target >= 0, wrapping); false when
 // the bounded wait gave up or another CTA reported an error.
 __device__ __forceinline__ bool strip_wait(const XpbdWorld& W, const StripTable& T, uint32_t cta, unsigned target,
@@ -227,19 +242,30 @@ __global__ void __launch_bounds__(512, 1) gs_strip_kernel(XpbdWorld W, StripTabl
         if (has_deps) strip_publish(T, cta, base + step + 1);
         ++step;
         cluster_sync();
+        // A thread's first record of each kind is loaded one color ahead (the records repeat every pass).
+        Group g = load_group(T, 0, cta, tid);
         for (uint32_t it = 0; it < I; ++it) {
             for (uint32_t c = 0; c < ncol; ++c, ++step) {
-                const uint32_t* off = T.off + ((size_t)c * T.ncta + cta) * 3;
-                const uint32_t k0 = off[0], k1 = off[1], k2 = off[2], k3 = off[3];
+                const Group cur = g;
+                g = load_group(T, c + 1 < ncol ? c + 1 : 0u, cta, tid);
                 if (has_deps) ok = ok && strip_wait(W, T, cta, base + step, tmo);
-                if (ok)
-                    for (uint32_t k = k0 + tid; k < k1; k += nthr) strip_solve<0>(T.rec[k], xs_base, s_rank_base, T, P);
+                if (ok) {
+                    if (cur.k[0] + tid < cur.k[1]) strip_solve<0>(cur.r[0], xs_base, s_rank_base, T, P);
+                    for (uint32_t k = cur.k[0] + tid + nthr; k < cur.k[1]; k += nthr)
+                        strip_solve<0>(T.rec[k], xs_base, s_rank_base, T, P);
+                }
                 if (has_deps) strip_publish(T, cta, base + step + 1);
-                if (ok)
-                    for (uint32_t k = k1 + tid; k < k2; k += nthr) strip_solve<1>(T.rec[k], xs_base, s_rank_base, T, P);
+                if (ok) {
+                    if (cur.k[1] + tid < cur.k[2]) strip_solve<1>(cur.r[1], xs_base, s_rank_base, T, P);
+                    for (uint32_t k = cur.k[1] + tid + nthr; k < cur.k[2]; k += nthr)
+                        strip_solve<1>(T.rec[k], xs_base, s_rank_base, T, P);
+                }
                 cluster_arrive();
-                if (ok)
-                    for (uint32_t k = k2 + tid; k < k3; k += nthr) strip_solve<2>(T.rec[k], xs_base, s_rank_base, T, P);
+                if (ok) {
+                    if (cur.k[2] + tid < cur.k[3]) strip_solve<2>(cur.r[2], xs_base, s_rank_base, T, P);
+                    for (uint32_t k = cur.k[2] + tid + nthr; k < cur.k[3]; k += nthr)
+                        strip_solve<2>(T.rec[k], xs_base, s_rank_base, T, P);
+                }
                 __syncthreads();
                 cluster_wait();
             }
