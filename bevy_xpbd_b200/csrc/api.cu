@@ -2575,6 +2575,30 @@ extern "C" int xpbd_debug_force_barrier_timeout(xpbd_ctx* ctx, float timeout_ms)
     if (!(timeout_ms > 0.f) || timeout_ms > 10000.f)
         return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "timeout must be in (0, 10000] ms");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (ctx->kernel == 7 || ctx->kernel == 8)
+        return fail(ctx, XPBD_ERR_UNSUPPORTED, "this schedule has no wait across thread-block clusters to force");
+    if (ctx->kernel == 9) {
+        // strips: one CTA that waits for others starts from a step count its dependencies never reach
+        std::vector<uint32_t> dep_off(ctx->strip.ncta + 1);
+        CK(cudaMemcpy(dep_off.data(), ctx->strip.dep_off, dep_off.size() * 4, cudaMemcpyDeviceToHost), "download");
+        uint32_t victim = 0xFFFFFFFFu;
+        for (uint32_t c = 0; c < ctx->strip.ncta && victim == 0xFFFFFFFFu; ++c)
+            if (dep_off[c + 1] > dep_off[c]) victim = c;
+        if (victim == 0xFFFFFFFFu) return fail(ctx, XPBD_ERR_UNSUPPORTED, "no strip shares particles");
+        const unsigned far = 0x40000000u;
+        CK(cudaMemcpyAsync(ctx->strip.flags + victim, &far, 4, cudaMemcpyHostToDevice, ctx->stream), "flags");
+        ctx->forced_timeout_ms = timeout_ms;
+        fill_dev_params(ctx);
+        CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream), "p");
+        cudaError_t e = launch_strip_gs(ctx->strip_cl, ctx->strip_block, ctx->W, ctx->strip, 1, ctx->stream);
+        ctx->forced_timeout_ms = 0.f;
+        fill_dev_params(ctx);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "forced launch");
+        r = read_status(ctx);  // expected XPBD_ERR_BARRIER_TIMEOUT; also starts the step flags over
+        CK(cudaMemcpyAsync(ctx->dparams, &ctx->hp, sizeof(XpbdDevParams), cudaMemcpyHostToDevice, ctx->stream), "p");
+        CK(cudaStreamSynchronize(ctx->stream), "sync");
+        return r;
+    }
     // one extra expected block: the barrier can never complete and must time out
     XpbdGridSync gs = {0u, 0u, 1u, 0u};
     ctx->forced_timeout_ms = timeout_ms;

@@ -92,7 +92,7 @@ def test_cloth_kernel_context_grab_against_oracle():
     sp = wl.make_sheet(48, 1.0, 1.0, "top_edge", seed=24)
     prm = params_for(10, 10, 1.0, drag=0.5)
     prm.grab_idx, prm.grab_active, prm.grab_target, prm.grab_stiffness = 1500, True, (0.1, 0.8, 0.2), 0.28
-    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10, jacobi_kernel=4)
     plug = gpu_sim(sp, prm, cfg)
     assert plug.stats()["solver_kernel"] == CLOTH
     plug.step(frames=3)
@@ -104,7 +104,7 @@ def test_cloth_kernel_context_grab_against_oracle():
 def test_cloth_kernel_zero_iterations_bit_exact():
     sp = wl.make_sheet(30, 1.0, 1.0, "corners", seed=25)
     prm = params_for(10, 0, 1.0)
-    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10, jacobi_kernel=4)
     plug = gpu_sim(sp, prm, cfg)
     assert plug.stats()["solver_kernel"] == CLOTH
     plug.step(frames=2)
@@ -123,7 +123,7 @@ def test_cloth_kernel_refuses_batches_that_share_a_particle():
                    order=P.ORDER_PRESORTED, batch_offsets=np.array([0, e // 2, e], np.uint32))
     plug.commit()
     prm = params_for(10, 10, 1.0)
-    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10, jacobi_kernel=4)
     plug.set_params(prm, cfg)
     assert plug.stats()["solver_kernel"] == ROWS
     plug.step(frames=1)

@@ -10,18 +10,23 @@ from tests.helpers import gpu_sim, params_for
 pytestmark = pytest.mark.gpu
 
 
-def _plug(solver=P.SOLVER_JACOBI):
-    sp = wl.make_sheet(24, 1.0, 1.0, "corners", seed=1)
+def _plug(solver=P.SOLVER_JACOBI, **kw):
+    sp = wl.make_sheet(kw.pop("side", 24), 1.0, 1.0, "corners", seed=1)
     cfg = P.ClothSimConfig(solver=solver, relaxation=P.RELAX_AVERAGE if solver == 0 else P.RELAX_OMEGA,
-                           solve_substeps=10)
+                           solve_substeps=10, **kw)
     return sp, gpu_sim(sp, params_for(10, 10, 1.0), cfg)
 
 
-@pytest.mark.parametrize("solver", [P.SOLVER_JACOBI, P.SOLVER_GAUSS_SEIDEL], ids=["jacobi", "gauss_seidel"])
-def test_grid_barrier_wait_times_out_and_context_recovers(solver):
-    """A launch whose first grid barrier expects one block more than exists: every wait ends after 20 ms with
-    XPBD_ERR_BARRIER_TIMEOUT, and the context keeps working afterwards."""
-    sp, plug = _plug(solver)
+@pytest.mark.parametrize("solver,kw", [(P.SOLVER_JACOBI, dict(jacobi_kernel=3)), (P.SOLVER_GAUSS_SEIDEL, {}),
+                                       (P.SOLVER_GAUSS_SEIDEL, dict(side=128, gs_strips=4, cluster_ctas=16))],
+                         ids=["jacobi_rows", "gauss_seidel", "gauss_seidel_strips"])
+def test_grid_barrier_wait_times_out_and_context_recovers(solver, kw):
+    """A launch whose wait can never complete — the grid barrier expects one block more than exists, or one strip CTA
+    starts from a step count its neighbours never reach: the wait ends after 20 ms with XPBD_ERR_BARRIER_TIMEOUT,
+    and the context keeps working afterwards."""
+    sp, plug = _plug(solver, **kw)
+    if kw.get("gs_strips"):
+        assert plug.stats()["solver_kernel"] == 9
     st = plug.debug_force_barrier_timeout(20.0)
     assert st == N.ERR_BARRIER_TIMEOUT, plug._L.xpbd_last_error(plug._h).decode()
     plug.reset()

