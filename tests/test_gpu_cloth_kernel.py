@@ -23,9 +23,9 @@ def _cfg(**kw):
     return c
 
 
-# sides whose particle counts land in every launch class: <= 1,760 / 3,520 / 7,168 particles on one CTA, then
-# clusters of 2 (<= 14,336), 4 (<= 28,672), 8 (<= 57,344) and 16 (<= 65,536) CTAs
-SIDES = [12, 41, 42, 59, 60, 84, 85, 119, 120, 169, 170, 239, 240, 256]
+# sides whose particle counts land in every launch class: <= 1,024 / 2,048 / 4,096 particles on one CTA, then
+# clusters of 2 (<= 8,192), 4 (<= 16,384), 8 (<= 32,768) and 16 (<= 65,536) CTAs
+SIDES = [12, 32, 33, 45, 46, 64, 65, 90, 91, 128, 129, 181, 182, 256]
 
 
 @pytest.fixture(scope="module")
