@@ -1098,6 +1098,7 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
     std::vector<std::vector<uint32_t>> seg(C);
     std::vector<std::vector<uint2>> rec(C);
     std::vector<std::vector<float>> comp(C);
+    std::vector<std::vector<uint32_t>> nbd(C);  // per (batch, rank): leading records touching boundary particles
     std::atomic<int> bad{0};  // 1: a cloth too large, 2: batches share a particle
     bool class_ok[kClothClasses];
     CK(cloth_kernel_prepare(), "cloth kernel attributes");
@@ -1128,9 +1129,16 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
                 stamp[i] = b;
                 stamp[j] = b;
             }
-        // records of constraints with an unpinned endpoint, grouped by (batch, rank owning endpoint i)
+        // records of constraints with an unpinned endpoint, grouped by (batch, rank owning endpoint i); within a
+        // group the records touching a particle that another rank's records also touch (in any batch) come first:
+        // the kernel solves them, signals the cluster barrier, and solves the rest while it completes
+        std::vector<uint8_t> bndp(c.n, 0);
+        if (cl > 1)
+            for (uint32_t e = 0; e < c.e; ++e)
+                if (c.ci[e] / qq != c.cj[e] / qq) bndp[c.ci[e]] = bndp[c.cj[e]] = 1;
         std::vector<uint32_t>& sg = seg[k];
         sg.assign((size_t)nb * cl + 1, 0);
+        nbd[k].assign((size_t)nb * cl, 0);
         for (uint32_t b = 0; b < nb; ++b)
             for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
                 const uint32_t e = c.perm[t];
@@ -1143,16 +1151,21 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
         comp[k].resize(sg.back());
         const uint32_t eb = cloth_ep_bits(cl);
         auto ep = [qq, eb](uint32_t p) { return ((p / qq) << eb) | (p % qq); };
-        for (uint32_t b = 0; b < nb; ++b)
-            for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
-                const uint32_t e = c.perm[t];
-                if (c.w[c.ci[e]] <= 0.f && c.w[c.cj[e]] <= 0.f) continue;
-                const uint32_t at = cur[(size_t)b * cl + c.ci[e] / qq]++;
-                uint32_t rb;
-                memcpy(&rb, &c.rest[e], 4);
-                rec[k][at] = make_uint2(ep(c.ci[e]) | (ep(c.cj[e]) << 16), rb);
-                comp[k][at] = c.comp[e];
-            }
+        for (int pass = 0; pass < 2; ++pass)  // boundary records, then the rest
+            for (uint32_t b = 0; b < nb; ++b)
+                for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
+                    const uint32_t e = c.perm[t];
+                    if (c.w[c.ci[e]] <= 0.f && c.w[c.cj[e]] <= 0.f) continue;
+                    const bool bd = bndp[c.ci[e]] || bndp[c.cj[e]];
+                    if (bd != (pass == 0)) continue;
+                    const size_t g = (size_t)b * cl + c.ci[e] / qq;
+                    const uint32_t at = cur[g]++;
+                    if (bd) ++nbd[k][g];
+                    uint32_t rb;
+                    memcpy(&rb, &c.rest[e], 4);
+                    rec[k][at] = make_uint2(ep(c.ci[e]) | (ep(c.cj[e]) << 16), rb);
+                    comp[k][at] = c.comp[e];
+                }
         cls[k] = id;
         q[k] = qq;
         ncol[k] = nb;
@@ -1175,12 +1188,13 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
     }
     std::vector<uint2> all_rec(rbase[C]);
     std::vector<float> all_comp(rbase[C]);
-    std::vector<uint32_t> all_seg(sbase[C]);
+    std::vector<uint32_t> all_seg(sbase[C]), all_bnd(sbase[C], 0);
     parallel_for(C, [&](uint32_t k) {
         const ClothHost& c = ctx->cloths[k];
         std::copy(rec[k].begin(), rec[k].end(), all_rec.begin() + rbase[k]);
         std::copy(comp[k].begin(), comp[k].end(), all_comp.begin() + rbase[k]);
         for (size_t x = 0; x < seg[k].size(); ++x) all_seg[sbase[k] + x] = (uint32_t)(seg[k][x] + rbase[k]);
+        for (size_t x = 0; x < nbd[k].size(); ++x) all_bnd[sbase[k] + x] = (uint32_t)(seg[k][x] + rbase[k] + nbd[k][x]);
         desc[k] = XpbdClothDesc{c.vtx_off, c.n, q[k], ncol[k], (uint32_t)sbase[k], kClothClass[cls[k]].cl, {0, 0}};
     });
     // one launch per class, largest cloths first
@@ -1203,6 +1217,7 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
     uint2* d_rec = err == cudaSuccess ? dev_alloc<uint2>(ctx, all_rec.size(), &err) : nullptr;
     float* d_comp = err == cudaSuccess ? dev_alloc<float>(ctx, all_comp.size(), &err) : nullptr;
     uint32_t* d_order = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, order.size(), &err) : nullptr;
+    uint32_t* d_bnd = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, all_bnd.size(), &err) : nullptr;
     if (err != cudaSuccess) return cuda_fail(ctx, err, "cloth-resident tables");
     cudaStream_t st = ctx->stream;
     CK(cudaMemcpyAsync(d_desc, desc.data(), C * sizeof(XpbdClothDesc), cudaMemcpyHostToDevice, st), "upload");
@@ -1213,10 +1228,11 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
         CK(cudaMemcpyAsync(d_comp, all_comp.data(), all_comp.size() * 4, cudaMemcpyHostToDevice, st), "upload");
     }
     CK(cudaMemcpyAsync(d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st), "upload");
+    CK(cudaMemcpyAsync(d_bnd, all_bnd.data(), all_bnd.size() * 4, cudaMemcpyHostToDevice, st), "upload");
     CK(cudaStreamSynchronize(st), "upload sync");
     CK(cloth_kernel_prepare(), "cloth kernel attributes");
     for (int t = 0; t < kClothClasses; ++t) {
-        ctx->cloth_tab[t] = ClothSolveTable{d_desc, d_seg, d_rec, d_comp, d_order + first[t], count[t], cap[t]};
+        ctx->cloth_tab[t] = ClothSolveTable{d_desc, d_seg, d_bnd, d_rec, d_comp, d_order + first[t], count[t], cap[t]};
         if (!ctx->cls_stream[t]) CK(cudaStreamCreateWithFlags(&ctx->cls_stream[t], cudaStreamNonBlocking), "stream");
         if (!ctx->ev_join[t]) CK(cudaEventCreateWithFlags(&ctx->ev_join[t], cudaEventDisableTiming), "event");
     }
@@ -2030,7 +2046,7 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
     float best = 1e30f;
     xpbd_solver_opts best_opts = base;
     struct Cand {
-        uint32_t block, bps, cl, jk;
+        uint32_t block, bps, cl, jk, strips;
     };
     std::vector<Cand> cands;
     const uint32_t blocks[] = {128, 256, 512, 1024};
@@ -2041,28 +2057,34 @@ extern "C" int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* o
         const uint32_t kid = base.solver == XPBD_SOLVER_JACOBI ? (jk == 2 ? 2u : (jk == 3 ? 5u : 0u)) : 1u;
         for (uint32_t blk : blocks) {
             int maxb = max_blocks_per_sm(kid, blk, ctx->W);
-            for (int bps = 1; bps <= maxb; bps *= 2) cands.push_back({blk, (uint32_t)bps, 1, jk});
+            for (int bps = 1; bps <= maxb; bps *= 2) cands.push_back({blk, (uint32_t)bps, 1, jk, 1});
         }
     }
     if (base.solver == XPBD_SOLVER_JACOBI && !(base.tolerance > 0.f || base.warm_start) &&
         base.lambda_mode == XPBD_LAMBDA_RESET_PER_ITERATION && base.collision == XPBD_COLLISION_NONE &&
         cloth_kernel_usable(ctx))
-        cands.push_back({0, 0, 1, 4});  // cloth-resident kernel (its launch shapes are fixed per cloth size)
+        cands.push_back({0, 0, 1, 4, 1});  // cloth-resident kernel (its launch shapes are fixed per cloth size)
     if (base.solver == XPBD_SOLVER_JACOBI && !(base.tolerance > 0.f || base.warm_start) &&
         base.lambda_mode == XPBD_LAMBDA_RESET_PER_ITERATION && base.collision == XPBD_COLLISION_NONE &&
         small_batch_usable(ctx))
-        cands.push_back({0, 0, 1, 5});  // the whole batch in one cluster
-    if (base.solver == XPBD_SOLVER_GAUSS_SEIDEL && base.cluster_ctas != 1)
+        cands.push_back({0, 0, 1, 5, 1});  // the whole batch in one cluster
+    if (base.solver == XPBD_SOLVER_GAUSS_SEIDEL && base.cluster_ctas != 1) {
         for (uint32_t cl : {16u, 8u})
-            for (uint32_t blk : {512u, 1024u}) cands.push_back({blk, 0, cl, 0});
+            for (uint32_t blk : {512u, 1024u}) cands.push_back({blk, 0, cl, 0, 1});
+        if (base.gs_strips != 1 && base.lambda_mode == XPBD_LAMBDA_RESET_PER_ITERATION &&
+            base.collision == XPBD_COLLISION_NONE && ctx->W.n >= 16384)
+            for (uint32_t strips : {2u, 4u, 8u}) cands.push_back({0, 0, 16, 0, strips});
+    }
     for (const Cand& cd : cands) {
         ctx->opts = base;
         ctx->opts.block_threads = cd.block;
         ctx->opts.blocks_per_sm = cd.bps;
         ctx->opts.cluster_ctas = cd.cl;
         ctx->opts.jacobi_kernel = cd.jk;
+        ctx->opts.gs_strips = cd.strips;
         choose_schedule(ctx);
-        if (cd.cl > 1 && ctx->cl != cd.cl) continue;  // cluster candidate not launchable here
+        if (cd.strips > 1 && ctx->kernel != 9) continue;             // strip shape not launchable here
+        if (cd.strips <= 1 && cd.cl > 1 && ctx->cl != cd.cl) continue;  // cluster candidate not launchable here
         r = run_frames(ctx, 1);  // warm-up / capture
         if (r != XPBD_OK) break;
         cudaEventRecord(a, st);

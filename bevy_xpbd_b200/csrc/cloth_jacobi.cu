@@ -235,6 +235,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) jacobi_cloth_kernel(XpbdW
     const uint32_t pos_base = smem_u32(s_pos), acc_base = smem_u32(s_acc);
     const uint32_t I = P.iterations;
     const uint32_t* seg = T.seg + D.seg_base + rank;
+    const uint32_t* bnd = T.bnd + D.seg_base + rank;
     for (uint32_t p = tid; p < np; p += BLOCK)  // incidence count of the particle's row (degree averaging)
         s_acc[p] = make_float4(0.0f, 0.0f, 0.0f, (float)(W.row_off[g0 + p + 1] - W.row_off[g0 + p]));
     for (uint32_t s = 0; s < substeps; ++s) {
@@ -257,20 +258,36 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) jacobi_cloth_kernel(XpbdW
         for (uint32_t it = 0; it < I; ++it) {
             for (uint32_t c = 0; c < D.colors; ++c) {
                 const uint32_t k0 = pk0, k1 = pk1;
+                // clusters: the segment's leading records touch particles of other ranks; the rest touch only
+                // particles no other rank ever touches and are solved while the cluster barrier completes
+                const uint32_t kb = CL > 1 ? __ldg(bnd + c * CL) : k1;
                 const Pref cur = pf;
                 const uint32_t cn = c + 1 < D.colors ? c + 1 : 0u;
                 pk0 = __ldg(seg + cn * CL);
                 pk1 = __ldg(seg + cn * CL + 1);
                 pf = pref_load(T, pk0 + tid, pk1, BLOCK);
-                if (k0 + tid < k1)
-                    solve_two<CL>(cur.r0, cur.c0, true, cur.r1, cur.c1, k0 + tid + BLOCK < k1, pos_base, acc_base,
-                                  rank, P.inv_dt_sq);
-                for (uint32_t k = k0 + tid + 2 * BLOCK; k < k1; k += 2 * BLOCK)
-                    solve_two<CL>(__ldg(T.rec + k), __ldg(T.comp + k), true,
-                                  k + BLOCK < k1 ? __ldg(T.rec + k + BLOCK) : make_uint2(0u, 0u),
-                                  k + BLOCK < k1 ? __ldg(T.comp + k + BLOCK) : 0.0f, k + BLOCK < k1, pos_base,
-                                  acc_base, rank, P.inv_dt_sq);
-                cloth_sync<CL>();
+                const uint32_t a0 = k0 + tid, a1 = a0 + BLOCK;
+                for (int part = 0; part < (CL > 1 ? 2 : 1); ++part) {
+                    const uint32_t lo = part == 0 ? k0 : kb, hi = part == 0 ? kb : k1;
+                    const bool h0 = a0 >= lo && a0 < hi, h1 = a1 >= lo && a1 < hi;
+                    if (h0 || h1)
+                        solve_two<CL>(cur.r0, cur.c0, h0, cur.r1, cur.c1, h1, pos_base, acc_base, rank, P.inv_dt_sq);
+                    for (uint32_t k = a0 + 2 * BLOCK; k < k1; k += 2 * BLOCK) {
+                        const bool g0 = k >= lo && k < hi, g1 = k + BLOCK >= lo && k + BLOCK < hi;
+                        if (!g0 && !g1) continue;
+                        solve_two<CL>(g0 ? __ldg(T.rec + k) : make_uint2(0u, 0u), g0 ? __ldg(T.comp + k) : 0.0f, g0,
+                                      g1 ? __ldg(T.rec + k + BLOCK) : make_uint2(0u, 0u),
+                                      g1 ? __ldg(T.comp + k + BLOCK) : 0.0f, g1, pos_base, acc_base, rank,
+                                      P.inv_dt_sq);
+                    }
+                    if (CL > 1 && part == 0) cluster_arrive();
+                }
+                if (CL > 1) {
+                    __syncthreads();  // this CTA's interior sums before anyone's next color
+                    cluster_wait();
+                } else {
+                    __syncthreads();
+                }
             }
             // the pass's update of the owned particles (jacobi_gather_particle's tail), then at the end of the
             // substep the velocity update
