@@ -1098,7 +1098,6 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
     std::vector<std::vector<uint32_t>> seg(C);
     std::vector<std::vector<uint2>> rec(C);
     std::vector<std::vector<float>> comp(C);
-    std::vector<std::vector<uint32_t>> nbd(C);  // per (batch, rank): leading records touching boundary particles
     std::atomic<int> bad{0};  // 1: a cloth too large, 2: batches share a particle
     bool class_ok[kClothClasses];
     CK(cloth_kernel_prepare(), "cloth kernel attributes");
@@ -1129,16 +1128,9 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
                 stamp[i] = b;
                 stamp[j] = b;
             }
-        // records of constraints with an unpinned endpoint, grouped by (batch, rank owning endpoint i); within a
-        // group the records touching a particle that another rank's records also touch (in any batch) come first:
-        // the kernel solves them, signals the cluster barrier, and solves the rest while it completes
-        std::vector<uint8_t> bndp(c.n, 0);
-        if (cl > 1)
-            for (uint32_t e = 0; e < c.e; ++e)
-                if (c.ci[e] / qq != c.cj[e] / qq) bndp[c.ci[e]] = bndp[c.cj[e]] = 1;
+        // records of constraints with an unpinned endpoint, grouped by (batch, rank owning endpoint i)
         std::vector<uint32_t>& sg = seg[k];
         sg.assign((size_t)nb * cl + 1, 0);
-        nbd[k].assign((size_t)nb * cl, 0);
         for (uint32_t b = 0; b < nb; ++b)
             for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
                 const uint32_t e = c.perm[t];
@@ -1151,21 +1143,16 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
         comp[k].resize(sg.back());
         const uint32_t eb = cloth_ep_bits(cl);
         auto ep = [qq, eb](uint32_t p) { return ((p / qq) << eb) | (p % qq); };
-        for (int pass = 0; pass < 2; ++pass)  // boundary records, then the rest
-            for (uint32_t b = 0; b < nb; ++b)
-                for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
-                    const uint32_t e = c.perm[t];
-                    if (c.w[c.ci[e]] <= 0.f && c.w[c.cj[e]] <= 0.f) continue;
-                    const bool bd = bndp[c.ci[e]] || bndp[c.cj[e]];
-                    if (bd != (pass == 0)) continue;
-                    const size_t g = (size_t)b * cl + c.ci[e] / qq;
-                    const uint32_t at = cur[g]++;
-                    if (bd) ++nbd[k][g];
-                    uint32_t rb;
-                    memcpy(&rb, &c.rest[e], 4);
-                    rec[k][at] = make_uint2(ep(c.ci[e]) | (ep(c.cj[e]) << 16), rb);
-                    comp[k][at] = c.comp[e];
-                }
+        for (uint32_t b = 0; b < nb; ++b)
+            for (uint32_t t = c.batch_off[b]; t < c.batch_off[b + 1]; ++t) {
+                const uint32_t e = c.perm[t];
+                if (c.w[c.ci[e]] <= 0.f && c.w[c.cj[e]] <= 0.f) continue;
+                const uint32_t at = cur[(size_t)b * cl + c.ci[e] / qq]++;
+                uint32_t rb;
+                memcpy(&rb, &c.rest[e], 4);
+                rec[k][at] = make_uint2(ep(c.ci[e]) | (ep(c.cj[e]) << 16), rb);
+                comp[k][at] = c.comp[e];
+            }
         cls[k] = id;
         q[k] = qq;
         ncol[k] = nb;
@@ -1188,13 +1175,12 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
     }
     std::vector<uint2> all_rec(rbase[C]);
     std::vector<float> all_comp(rbase[C]);
-    std::vector<uint32_t> all_seg(sbase[C]), all_bnd(sbase[C], 0);
+    std::vector<uint32_t> all_seg(sbase[C]);
     parallel_for(C, [&](uint32_t k) {
         const ClothHost& c = ctx->cloths[k];
         std::copy(rec[k].begin(), rec[k].end(), all_rec.begin() + rbase[k]);
         std::copy(comp[k].begin(), comp[k].end(), all_comp.begin() + rbase[k]);
         for (size_t x = 0; x < seg[k].size(); ++x) all_seg[sbase[k] + x] = (uint32_t)(seg[k][x] + rbase[k]);
-        for (size_t x = 0; x < nbd[k].size(); ++x) all_bnd[sbase[k] + x] = (uint32_t)(seg[k][x] + rbase[k] + nbd[k][x]);
         desc[k] = XpbdClothDesc{c.vtx_off, c.n, q[k], ncol[k], (uint32_t)sbase[k], kClothClass[cls[k]].cl, {0, 0}};
     });
     // one launch per class, largest cloths first
@@ -1217,7 +1203,6 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
     uint2* d_rec = err == cudaSuccess ? dev_alloc<uint2>(ctx, all_rec.size(), &err) : nullptr;
     float* d_comp = err == cudaSuccess ? dev_alloc<float>(ctx, all_comp.size(), &err) : nullptr;
     uint32_t* d_order = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, order.size(), &err) : nullptr;
-    uint32_t* d_bnd = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, all_bnd.size(), &err) : nullptr;
     if (err != cudaSuccess) return cuda_fail(ctx, err, "cloth-resident tables");
     cudaStream_t st = ctx->stream;
     CK(cudaMemcpyAsync(d_desc, desc.data(), C * sizeof(XpbdClothDesc), cudaMemcpyHostToDevice, st), "upload");
@@ -1228,11 +1213,10 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
         CK(cudaMemcpyAsync(d_comp, all_comp.data(), all_comp.size() * 4, cudaMemcpyHostToDevice, st), "upload");
     }
     CK(cudaMemcpyAsync(d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st), "upload");
-    CK(cudaMemcpyAsync(d_bnd, all_bnd.data(), all_bnd.size() * 4, cudaMemcpyHostToDevice, st), "upload");
     CK(cudaStreamSynchronize(st), "upload sync");
     CK(cloth_kernel_prepare(), "cloth kernel attributes");
     for (int t = 0; t < kClothClasses; ++t) {
-        ctx->cloth_tab[t] = ClothSolveTable{d_desc, d_seg, d_bnd, d_rec, d_comp, d_order + first[t], count[t], cap[t]};
+        ctx->cloth_tab[t] = ClothSolveTable{d_desc, d_seg, d_rec, d_comp, d_order + first[t], count[t], cap[t]};
         if (!ctx->cls_stream[t]) CK(cudaStreamCreateWithFlags(&ctx->cls_stream[t], cudaStreamNonBlocking), "stream");
         if (!ctx->ev_join[t]) CK(cudaEventCreateWithFlags(&ctx->ev_join[t], cudaEventDisableTiming), "event");
     }
@@ -1397,8 +1381,7 @@ static void choose_schedule(xpbd_ctx* ctx) {
         ctx->stats.cluster_ctas = ctx->small_cl;
         return;
     }
-    if (cloth_eligible && (ctx->opts.jacobi_kernel == 0 || ctx->opts.jacobi_kernel == 4) &&
-        cloth_kernel_usable(ctx)) {
+    if (cloth_eligible && ctx->opts.jacobi_kernel == 4 && cloth_kernel_usable(ctx)) {
         ctx->kernel = 7;
         uint32_t blocks = 0, maxcl = 1;
         for (int t = 0; t < kClothClasses; ++t) {

@@ -29,11 +29,11 @@
 
 namespace xpbd {
 
-// cl, threads per CTA, particles per rank: the first class whose cl · rank_cap holds a cloth takes it. A rank holds
-// at most four particles per thread: a color then gives a thread about two records (a cloth has about six
-// constraints per particle over about twelve colors), both loaded one color ahead and solved together.
+// cl, threads per CTA, particles per rank: the first class whose cl · rank_cap holds a cloth takes it. The single-CTA
+// classes fit four, two and one CTA per SM in its 228 KB of shared memory.
 const ClothClass kClothClass[kClothClasses] = {
-    {1, 256, 1024}, {1, 512, 2048}, {1, 1024, 4096}, {2, 1024, 4096}, {4, 1024, 4096}, {8, 1024, 4096},
+    {1, 256, 1760}, {1, 512, 3520}, {1, 1024, XPBD_CLOTH_RANK_MAX},
+    {2, 1024, XPBD_CLOTH_RANK_MAX}, {4, 1024, XPBD_CLOTH_RANK_MAX}, {8, 1024, XPBD_CLOTH_RANK_MAX},
     {16, 1024, 4096}};
 
 size_t cloth_kernel_smem_bytes(uint32_t cap) { return 2 * (size_t)cap * sizeof(float4); }
@@ -105,101 +105,6 @@ __device__ __forceinline__ void solve_record(uint2 r, float comp, uint32_t pos_b
                    __fmul_rn(__fmul_rn(n.z, pj.w), dlam), true);
 }
 
-// Two records of one color at once, in phases — the four endpoint positions, the two constraint solves, the four
-// correction-sum loads, then the adds and stores — so that the memory latencies of the two overlap. Within a color
-// the two records touch four different particles, so their loads and stores commute.
-struct EpAddr {
-    uint32_t a;  // local shared-memory address, or the mapped cluster address when remote
-    bool local;
-};
-template <int CL>
-__device__ __forceinline__ EpAddr ep_addr(uint32_t base, uint32_t ep, uint32_t rank) {
-    constexpr uint32_t B = cloth_ep_bits(CL);
-    const uint32_t a = base + (ep & ((1u << B) - 1u)) * 16u;
-    if (CL == 1) return {a, true};
-    const uint32_t r = ep >> B;
-    return r == rank ? EpAddr{a, true} : EpAddr{map_rank(a, r), false};
-}
-__device__ __forceinline__ float4 ld_addr(EpAddr e) { return e.local ? ld_local(e.a) : ld_dsmem(e.a); }
-__device__ __forceinline__ void st_addr(EpAddr e, float4 v) {
-    if (e.local)
-        st_local(e.a, v);
-    else
-        st_dsmem(e.a, v);
-}
-
-// The constraint of record r from its endpoints: whether it contributes (the reference skips |d| < 1e-8 and has
-// Δλ = 0 for a w sum < 1e-8), n̂ and Δλ.
-__device__ __forceinline__ bool record_terms(float4 pi, float4 pj, uint32_t rest_bits, float comp, float inv_dt_sq,
-                                             F3& n, float& dlam) {
-    const F3 gv = sub3(f3(pi), f3(pj));
-    const float len = len3(gv);
-    const float alpha_t = __fmul_rn(comp, inv_dt_sq);
-    const float wsum = __fadd_rn(__fadd_rn(pi.w, pj.w), alpha_t);
-    if (len < 1e-8f || wsum < 1e-8f) return false;
-    const float C = __fsub_rn(len, __uint_as_float(rest_bits));
-    dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
-    if (!fpdiv3_by_length_fast(gv.x, gv.y, gv.z, len, n.x, n.y, n.z)) fpdiv3(gv.x, gv.y, gv.z, len, n.x, n.y, n.z);
-    return true;
-}
-
-template <int CL>
-__device__ __forceinline__ void solve_two(uint2 rA, float cA, bool hA, uint2 rB, float cB, bool hB,
-                                          uint32_t pos_base, uint32_t acc_base, uint32_t rank, float inv_dt_sq) {
-    const EpAddr piA_a = ep_addr<CL>(pos_base, rA.x & 0xFFFFu, rank), pjA_a = ep_addr<CL>(pos_base, rA.x >> 16, rank);
-    const EpAddr piB_a = ep_addr<CL>(pos_base, rB.x & 0xFFFFu, rank), pjB_a = ep_addr<CL>(pos_base, rB.x >> 16, rank);
-    float4 piA = make_float4(0.f, 0.f, 0.f, 0.f), pjA = piA, piB = piA, pjB = piA;
-    if (hA) {
-        piA = ld_addr(piA_a);
-        pjA = ld_addr(pjA_a);
-    }
-    if (hB) {
-        piB = ld_addr(piB_a);
-        pjB = ld_addr(pjB_a);
-    }
-    F3 nA, nB;
-    float dA = 0.0f, dB = 0.0f;
-    const bool uA = hA && record_terms(piA, pjA, rA.y, cA, inv_dt_sq, nA, dA);
-    const bool uB = hB && record_terms(piB, pjB, rB.y, cB, inv_dt_sq, nB, dB);
-    const bool aiA = uA && piA.w > 0.0f, ajA = uA && pjA.w > 0.0f;
-    const bool aiB = uB && piB.w > 0.0f, ajB = uB && pjB.w > 0.0f;
-    // the sums sit at a fixed offset from the positions in every CTA's window (mapa maps a CTA's shared memory
-    // linearly), so their addresses follow from the position addresses
-    const uint32_t d = acc_base - pos_base;
-    const EpAddr siA = {piA_a.a + d, piA_a.local}, sjA = {pjA_a.a + d, pjA_a.local};
-    const EpAddr siB = {piB_a.a + d, piB_a.local}, sjB = {pjB_a.a + d, pjB_a.local};
-    float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0, s2 = s0, s3 = s0;
-    if (aiA) s0 = ld_addr(siA);
-    if (ajA) s1 = ld_addr(sjA);
-    if (aiB) s2 = ld_addr(siB);
-    if (ajB) s3 = ld_addr(sjB);
-    // (n̂·w_i)·Δλ added to i's sum, (n̂·w_j)·Δλ subtracted from j's (the j endpoint's term is its negation)
-    if (aiA) {
-        s0.x = __fadd_rn(s0.x, __fmul_rn(__fmul_rn(nA.x, piA.w), dA));
-        s0.y = __fadd_rn(s0.y, __fmul_rn(__fmul_rn(nA.y, piA.w), dA));
-        s0.z = __fadd_rn(s0.z, __fmul_rn(__fmul_rn(nA.z, piA.w), dA));
-        st_addr(siA, s0);
-    }
-    if (ajA) {
-        s1.x = __fsub_rn(s1.x, __fmul_rn(__fmul_rn(nA.x, pjA.w), dA));
-        s1.y = __fsub_rn(s1.y, __fmul_rn(__fmul_rn(nA.y, pjA.w), dA));
-        s1.z = __fsub_rn(s1.z, __fmul_rn(__fmul_rn(nA.z, pjA.w), dA));
-        st_addr(sjA, s1);
-    }
-    if (aiB) {
-        s2.x = __fadd_rn(s2.x, __fmul_rn(__fmul_rn(nB.x, piB.w), dB));
-        s2.y = __fadd_rn(s2.y, __fmul_rn(__fmul_rn(nB.y, piB.w), dB));
-        s2.z = __fadd_rn(s2.z, __fmul_rn(__fmul_rn(nB.z, piB.w), dB));
-        st_addr(siB, s2);
-    }
-    if (ajB) {
-        s3.x = __fsub_rn(s3.x, __fmul_rn(__fmul_rn(nB.x, pjB.w), dB));
-        s3.y = __fsub_rn(s3.y, __fmul_rn(__fmul_rn(nB.y, pjB.w), dB));
-        s3.z = __fsub_rn(s3.z, __fmul_rn(__fmul_rn(nB.z, pjB.w), dB));
-        st_addr(sjB, s3);
-    }
-}
-
 // A thread's first two records of a color (k and k + BLOCK), loaded ahead of use.
 struct Pref {
     uint2 r0, r1;
@@ -235,7 +140,6 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) jacobi_cloth_kernel(XpbdW
     const uint32_t pos_base = smem_u32(s_pos), acc_base = smem_u32(s_acc);
     const uint32_t I = P.iterations;
     const uint32_t* seg = T.seg + D.seg_base + rank;
-    const uint32_t* bnd = T.bnd + D.seg_base + rank;
     for (uint32_t p = tid; p < np; p += BLOCK)  // incidence count of the particle's row (degree averaging)
         s_acc[p] = make_float4(0.0f, 0.0f, 0.0f, (float)(W.row_off[g0 + p + 1] - W.row_off[g0 + p]));
     for (uint32_t s = 0; s < substeps; ++s) {
@@ -258,36 +162,16 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) jacobi_cloth_kernel(XpbdW
         for (uint32_t it = 0; it < I; ++it) {
             for (uint32_t c = 0; c < D.colors; ++c) {
                 const uint32_t k0 = pk0, k1 = pk1;
-                // clusters: the segment's leading records touch particles of other ranks; the rest touch only
-                // particles no other rank ever touches and are solved while the cluster barrier completes
-                const uint32_t kb = CL > 1 ? __ldg(bnd + c * CL) : k1;
                 const Pref cur = pf;
                 const uint32_t cn = c + 1 < D.colors ? c + 1 : 0u;
                 pk0 = __ldg(seg + cn * CL);
                 pk1 = __ldg(seg + cn * CL + 1);
                 pf = pref_load(T, pk0 + tid, pk1, BLOCK);
-                const uint32_t a0 = k0 + tid, a1 = a0 + BLOCK;
-                for (int part = 0; part < (CL > 1 ? 2 : 1); ++part) {
-                    const uint32_t lo = part == 0 ? k0 : kb, hi = part == 0 ? kb : k1;
-                    const bool h0 = a0 >= lo && a0 < hi, h1 = a1 >= lo && a1 < hi;
-                    if (h0 || h1)
-                        solve_two<CL>(cur.r0, cur.c0, h0, cur.r1, cur.c1, h1, pos_base, acc_base, rank, P.inv_dt_sq);
-                    for (uint32_t k = a0 + 2 * BLOCK; k < k1; k += 2 * BLOCK) {
-                        const bool g0 = k >= lo && k < hi, g1 = k + BLOCK >= lo && k + BLOCK < hi;
-                        if (!g0 && !g1) continue;
-                        solve_two<CL>(g0 ? __ldg(T.rec + k) : make_uint2(0u, 0u), g0 ? __ldg(T.comp + k) : 0.0f, g0,
-                                      g1 ? __ldg(T.rec + k + BLOCK) : make_uint2(0u, 0u),
-                                      g1 ? __ldg(T.comp + k + BLOCK) : 0.0f, g1, pos_base, acc_base, rank,
-                                      P.inv_dt_sq);
-                    }
-                    if (CL > 1 && part == 0) cluster_arrive();
-                }
-                if (CL > 1) {
-                    __syncthreads();  // this CTA's interior sums before anyone's next color
-                    cluster_wait();
-                } else {
-                    __syncthreads();
-                }
+                if (k0 + tid < k1) solve_record<CL>(cur.r0, cur.c0, pos_base, acc_base, rank, P.inv_dt_sq);
+                if (k0 + tid + BLOCK < k1) solve_record<CL>(cur.r1, cur.c1, pos_base, acc_base, rank, P.inv_dt_sq);
+                for (uint32_t k = k0 + tid + 2 * BLOCK; k < k1; k += BLOCK)
+                    solve_record<CL>(__ldg(T.rec + k), __ldg(T.comp + k), pos_base, acc_base, rank, P.inv_dt_sq);
+                cloth_sync<CL>();
             }
             // the pass's update of the owned particles (jacobi_gather_particle's tail), then at the end of the
             // substep the velocity update

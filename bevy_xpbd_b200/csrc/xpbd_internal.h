@@ -128,7 +128,7 @@ struct XpbdClothDesc {
     uint32_t pad[2];
 };
 #define XPBD_CLOTH_EP_BITS 13          // local index bits of an endpoint for clusters of up to 8 CTAs
-#define XPBD_CLOTH_RANK_MAX 4096u      // particles per CTA: 2 x 16 B of shared memory each (128 KB)
+#define XPBD_CLOTH_RANK_MAX 7168u      // particles per CTA: 2 x 16 B of shared memory each (224 KB)
 #define XPBD_CLOTH_MAX_CL 16u
 // clusters of 16 CTAs (non-portable size) need four rank bits: 12 local bits, at most 4,096 particles per CTA
 __host__ __device__ constexpr uint32_t cloth_ep_bits(uint32_t cl) { return cl > 8 ? 12u : 13u; }

@@ -42,7 +42,6 @@ cudaError_t launch_mlp_publish(const float* master, XpbdMlp* mlp, cudaStream_t s
 struct ClothSolveTable {
     const XpbdClothDesc* cloths;  // per cloth of the batch
     const uint32_t* seg;          // (color, rank) segment starts into rec / comp
-    const uint32_t* bnd;          // per segment: end of its leading records that touch another rank's particles
     const uint2* rec;             // {endpoint i | endpoint j << 16, rest bits}
     const float* comp;            // compliance per record
     const uint32_t* order;        // cloth ids of one launch (one per cluster), largest first

@@ -23,9 +23,9 @@ def _cfg(**kw):
     return c
 
 
-# sides whose particle counts land in every launch class: <= 1,024 / 2,048 / 4,096 particles on one CTA, then
-# clusters of 2 (<= 8,192), 4 (<= 16,384), 8 (<= 32,768) and 16 (<= 65,536) CTAs
-SIDES = [12, 32, 33, 45, 46, 64, 65, 90, 91, 128, 129, 181, 182, 256]
+# sides whose particle counts land in every launch class: <= 1,760 / 3,520 / 7,168 particles on one CTA, then
+# clusters of 2 (<= 14,336), 4 (<= 28,672), 8 (<= 57,344) and 16 (<= 65,536) CTAs
+SIDES = [12, 41, 42, 59, 60, 84, 85, 119, 120, 169, 170, 239, 240, 256]
 
 
 @pytest.fixture(scope="module")
@@ -55,10 +55,11 @@ def test_cloth_kernel_every_launch_class_bit_exact(mixed_batch, relax):
         assert max_abs(plug.velocities(k), vo) == 0.0, (k, sp.side)
 
 
-def test_cloth_kernel_is_the_default_for_plain_jacobi_and_matches_rows():
+def test_cloth_kernel_matches_the_thread_per_particle_kernel():
     specs = wl.config3_batch(seed=21, count=12, side_lo=16, side_hi=100)
     prm = params_for(10, 10, 1.0)
-    a = gpu_sim(specs, prm, _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10))
+    a = gpu_sim(specs, prm, _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10,
+                                 jacobi_kernel=4))
     b = gpu_sim(specs, prm, _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10,
                                  jacobi_kernel=3))
     assert a.stats()["solver_kernel"] == CLOTH and b.stats()["solver_kernel"] == ROWS
@@ -72,7 +73,7 @@ def test_cloth_kernel_grabs_drag_gravity_and_substep_api_bit_exact():
     sp = wl.make_sheet(70, 1.0, 1.0, "corners", seed=23)
     prm = params_for(10, 10, 1.0, drag=1.25, gravity=(0.3, -9.81, -0.2))
     prm.grab_idx, prm.grab_active, prm.grab_target, prm.grab_stiffness = 2000, True, (0.1, 0.8, 0.2), 0.28
-    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10)
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10, jacobi_kernel=4)
     plug = gpu_sim(sp, prm, cfg)
     assert plug.stats()["solver_kernel"] == CLOTH
     plug.set_cloth_grab(0, 3000, (-0.2, 0.9, 0.1), 0.45)

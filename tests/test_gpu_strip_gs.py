@@ -20,9 +20,9 @@ def _cfg(**kw):
     return c
 
 
-@pytest.mark.parametrize("side,strips,cluster,frames", [(256, 8, 16, 6), (96, 4, 8, 6), (256, 4, 16, 3),
+@pytest.mark.parametrize("side,strips,cluster,frames", [(256, 8, 8, 6), (96, 4, 8, 6), (256, 4, 16, 3),
                                                         (130, 2, 16, 5)],
-                         ids=["256_8x16", "96_4x8", "256_4x16", "130_2x16"])
+                         ids=["256_8x8", "96_4x8", "256_4x16", "130_2x16"])
 def test_strip_gauss_seidel_bit_exact(side, strips, cluster, frames):
     sp = wl.make_sheet(side, 2.0, 1.0, "top_edge", seed=80 + side)
     prm = params_for(10, 10, 1.0, drag=0.01)
