@@ -437,7 +437,8 @@ def run_warm_leg(args, device: int) -> dict:
         tr.set_cloth_wind(k, (speed * np.cos(ang), 0.0, speed * np.sin(ang)), 1.0)
     frames, every = 2000, 20
     e_total = sum(sp.num_constraints for sp in train)
-    stride = max(1, int(np.ceil(e_total * (frames // every) / ((1 << 21) - e_total))))
+    # every stride-th constraint of each collected substep, so that the 100 collections fill the 2^21-sample store
+    stride = max(1, int(np.ceil(e_total * (frames // every) / (1 << 21))))
     tr.set_params(plain_prm, plain_cfg)
     samples = 0
     for f in range(frames):
