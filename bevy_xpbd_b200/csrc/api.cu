@@ -1230,9 +1230,14 @@ static int ensure_cloth_tables(xpbd_ctx* ctx, bool* usable) {
 // (records {self, other endpoint, rest, compliance}), built on its first selection from the device tables.
 constexpr uint32_t kSmallBatchMaxParticles = 16 * 512;
 static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
-    *usable = ctx->small_ok;
-    if (ctx->small_tried) return XPBD_OK;
+    const uint32_t want = ctx->opts.cluster_ctas > 1 ? ctx->opts.cluster_ctas : 0u;
+    if (ctx->small_tried && (want == 0 || want == ctx->small_cl || !ctx->small_ok)) {
+        *usable = ctx->small_ok && (want == 0 || want == ctx->small_cl);
+        return XPBD_OK;
+    }
+    *usable = false;
     ctx->small_tried = true;
+    ctx->small_ok = false;
     const uint32_t N = ctx->W.n, C = (uint32_t)ctx->cloths.size();
     if (N == 0 || N > kSmallBatchMaxParticles) return XPBD_OK;
     std::vector<uint32_t> roff(N + 1);
@@ -1250,6 +1255,7 @@ static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
     for (uint32_t k = 0; k < C; ++k)
         for (uint32_t i = 0; i < ctx->cloths[k].n; ++i) cloth_of[ctx->cloths[k].vtx_off + i] = k;
     for (uint32_t cl : {16u, 8u}) {
+        if (ctx->opts.cluster_ctas > 1 && ctx->opts.cluster_ctas != cl) continue;  // a requested cluster size
         const uint32_t q = (N + cl - 1) / cl;
         if (q > 1024) continue;
         std::vector<uint4> rec;
