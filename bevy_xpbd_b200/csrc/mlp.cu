@@ -1,9 +1,11 @@
 // Learned λ warm start: a 9→64→64→1 MLP (SiLU) predicting each constraint's initial Lagrange multiplier from local
 // features. Inference, training (forward, backward) and the Adam update are hand-written kernels; every matrix
-// product runs on the tensor cores as BF16 tiles with FP32 accumulation (mma.sync.m16n8k16), one warp per tile of
-// 16 constraints: layer 1 = [16 x 16(9 padded)] x [16 x 64], layer 2 = [16 x 64] x [64 x 64] (the layer-1 accumulator
-// registers are repacked as layer-2 A fragments), layer 3 a 64-wide dot product. Weight gradients are the same tiles
-// with the batch as the reduction dimension. No reference counterpart: the reference has no learned component.
+// product runs on the tensor cores as BF16 tiles with FP32 accumulation. Inference uses the sm_100a tcgen05 path:
+// 128-constraint tiles, tcgen05.mma issued by one thread on shared-memory operands, accumulators in tensor memory
+// read back with tcgen05.ld. Training uses warp-level mma.sync.m16n8k16 tiles of 16 constraints (its backward keeps
+// the forward's accumulators in registers): layer 1 = [16 x 16(9 padded)] x [16 x 64], layer 2 = [16 x 64] x
+// [64 x 64] (the layer-1 accumulator registers are repacked as layer-2 A fragments), layer 3 a 64-wide dot product;
+// weight gradients are the same tiles with the batch as the reduction dimension. No reference counterpart: the reference has no learned component.
 //
 // Features of constraint e = (i, j) at the predicted positions of the substep, before any iteration:
 //   f0 strain (|xi-xj| - rest)/rest      f1 previous-substep λ · (wi + wj + α̃)/rest
@@ -13,11 +15,13 @@
 // strain units; the network predicts its change over the previous substep, t - f1, standardised — so a network that
 // outputs the mean change reproduces the previous-λ warm start, and the learning spends its capacity on the update.
 #include <cuda_bf16.h>
+#include <mutex>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "xpbd_internal.h"
 #include "xpbd_kernels.h"
+#include "xpbd_tcgen05.h"
 
 namespace xpbd {
 
@@ -181,80 +185,188 @@ __device__ __forceinline__ void store_row(const SmemMlp& S, const float f[9], __
 }
 }  // namespace
 
+// ---- inference on the tcgen05 tensor cores: 128 constraints per tile, one thread per row.
+// Layer 1 (M=128, N=64, K=16) and layer 2 (M=128, N=64, K=64, four K steps) are tcgen05.mma instructions issued by
+// one thread on BF16 operands in shared memory, accumulating in FP32 in tensor memory (columns 0-63 and 64-127);
+// each thread reads its row's accumulators back with tcgen05.ld, adds the bias, applies SiLU, and either stores the
+// BF16 activations as the next layer's A operand or forms the output dot product. The rounding points are those of
+// the training forward: BF16 inputs, weights and hidden activations, FP32 accumulation and output.
+struct TcSmem {
+    __nv_bfloat16 w1[64 * 16];   // B of layer 1, canonical K-major layout (see tc_index)
+    __nv_bfloat16 w2[64 * 64];   // B of layer 2
+    __nv_bfloat16 a1[128 * 16];  // A of layer 1: the tile's standardised features
+    __nv_bfloat16 a2[128 * 64];  // A of layer 2: the tile's BF16 hidden activations
+    float b1[64], b2[64], w3[64];
+    float fmean[XPBD_MLP_IN], fstd[XPBD_MLP_IN], b3, tmean, tstd;
+    uint64_t bar;
+    uint32_t tmem;
+};
+// Dynamic shared memory per CTA: padded so that at most three CTAs share an SM (3 × 128 of its 512 tensor-memory
+// columns), so the allocation never waits.
+constexpr size_t kTcSmemBytes = 72 * 1024;
+constexpr uint32_t kTcCols = 128;
+constexpr uint32_t kTcIdesc = tc_idesc_bf16(128, 64);
+
+// Element index of (row r, column k) of an R-row K-major BF16 matrix in the no-swizzle canonical layout: 8-element
+// K chunks are planes of R × 16 bytes (lbo = 16·R); inside a plane, 8-row groups of 128 bytes (sbo = 128).
+__device__ __forceinline__ uint32_t tc_index(uint32_t r, uint32_t k, uint32_t rows) {
+    return (((k >> 3) * (rows >> 3) + (r >> 3)) * 8u + (r & 7u)) * 8u + (k & 7u);
+}
+
+__device__ void tc_load_mlp(TcSmem& s, const XpbdMlp& m) {
+    const __nv_bfloat16* w1 = reinterpret_cast<const __nv_bfloat16*>(m.w1);
+    const __nv_bfloat16* w2 = reinterpret_cast<const __nv_bfloat16*>(m.w2);
+    for (uint32_t q = threadIdx.x; q < 64 * 16; q += blockDim.x) s.w1[tc_index(q >> 4, q & 15u, 64)] = w1[q];
+    for (uint32_t q = threadIdx.x; q < 64 * 64; q += blockDim.x) s.w2[tc_index(q >> 6, q & 63u, 64)] = w2[q];
+    for (uint32_t k = threadIdx.x; k < 64; k += blockDim.x) {
+        s.b1[k] = m.b1[k];
+        s.b2[k] = m.b2[k];
+        s.w3[k] = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(m.w3)[k]);
+    }
+    if (threadIdx.x < XPBD_MLP_IN) {
+        s.fmean[threadIdx.x] = m.fmean[threadIdx.x];
+        s.fstd[threadIdx.x] = m.fstd[threadIdx.x];
+    }
+    if (threadIdx.x == 0) {
+        s.b3 = m.b3;
+        s.tmean = m.tmean;
+        s.tstd = m.tstd;
+    }
+}
+
+// This thread's row of the layer-1 operand: standardised features, BF16, columns 9..15 zero.
+__device__ __forceinline__ void tc_store_features(TcSmem& s, uint32_t r, const float f[9]) {
+    __nv_bfloat16 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        v[k] = __float2bfloat16_rn(k < 5 ? (f[k] - s.fmean[k]) / s.fstd[k] : (k < 9 ? f[k] : 0.0f));
+    *reinterpret_cast<uint4*>(s.a1 + tc_index(r, 0, 128)) = *reinterpret_cast<const uint4*>(v);
+    *reinterpret_cast<uint4*>(s.a1 + tc_index(r, 8, 128)) = *reinterpret_cast<const uint4*>(v + 8);
+}
+// Forward of the tile whose layer-1 operand is staged (every thread called tc_store_features): returns this
+// thread's row output y (standardised). `phase` is the mbarrier parity of the next completion; false when a wait gave
+// up (the kernel then stops).
+__device__ __forceinline__ bool tc_tile_forward(TcSmem& s, uint32_t& phase, float& y) {
+    const uint32_t r = threadIdx.x, warp = r >> 5;
+    const uint32_t lane_base = s.tmem + ((32u * warp) << 16);
+    tc_fence_proxy();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (r == 0) {
+        tc_mma(s.tmem, tc_desc(tc_smem_addr(s.a1), 128 * 16, 128), tc_desc(tc_smem_addr(s.w1), 64 * 16, 128),
+               kTcIdesc, false);
+        tc_commit(&s.bar);
+    }
+    bool ok = tc_mbar_wait(&s.bar, phase);
+    phase ^= 1u;
+    tc_fence_after();
+    // layer-1 epilogue: bias, SiLU, BF16 → this row of the layer-2 operand
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float z[16];
+        tc_ld16(lane_base + 16u * c, z);
+        __nv_bfloat16 h[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) h[k] = __float2bfloat16_rn(silu(z[k] + s.b1[16 * c + k]));
+        *reinterpret_cast<uint4*>(s.a2 + tc_index(r, 16 * c, 128)) = *reinterpret_cast<const uint4*>(h);
+        *reinterpret_cast<uint4*>(s.a2 + tc_index(r, 16 * c + 8, 128)) = *reinterpret_cast<const uint4*>(h + 8);
+    }
+    tc_fence_proxy();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (r == 0) {
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q)  // K steps of 16: two 8-element chunk planes each
+            tc_mma(s.tmem + 64u, tc_desc(tc_smem_addr(s.a2) + q * 2u * 128u * 16u, 128 * 16, 128),
+                   tc_desc(tc_smem_addr(s.w2) + q * 2u * 64u * 16u, 64 * 16, 128), kTcIdesc, q > 0);
+        tc_commit(&s.bar);
+    }
+    ok = tc_mbar_wait(&s.bar, phase) && ok;
+    phase ^= 1u;
+    tc_fence_after();
+    float acc = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float z[16];
+        tc_ld16(lane_base + 64u + 16u * c, z);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc += bf16r(silu(z[k] + s.b2[16 * c + k])) * s.w3[16 * c + k];
+    }
+    y = acc + s.b3;
+    // every thread's reads of the accumulators and of the operands end before the next tile overwrites them; the
+    // verdict of the waits is made uniform so that every thread leaves the tile loop together
+    tc_fence_before();
+    return __syncthreads_and(ok) != 0;
+}
+
+__device__ __forceinline__ void tc_setup(TcSmem& s, const XpbdMlp& m) {
+    tc_load_mlp(s, m);
+    if (threadIdx.x == 0) tc_mbar_init(&s.bar, 1);
+    if (threadIdx.x < 32) tc_alloc(&s.tmem, kTcCols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+}
+__device__ __forceinline__ void tc_teardown(TcSmem& s) {
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x < 32) tc_dealloc(s.tmem, kTcCols);
+}
+
 // ---- inference: λ0 for every constraint, written to both incidences (warm_lam_inc)
 __global__ void __launch_bounds__(128) mlp_infer_kernel(XpbdWorld W, const XpbdMlp* __restrict__ mlp) {
-    __shared__ SmemMlp S;
-    __shared__ __align__(16) __nv_bfloat16 xs_all[4][16 * 16];
-    load_mlp(S, *mlp);
-    __syncthreads();
+    extern __shared__ __align__(1024) unsigned char tc_raw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>(tc_raw);
+    tc_setup(S, *mlp);
     const XpbdDevParams P = *W.params;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    __nv_bfloat16* xs = xs_all[warp];
-    const uint32_t tiles = (W.e + 15) / 16;
-    for (uint32_t tile = blockIdx.x * 4 + warp; tile < tiles; tile += gridDim.x * 4) {
-        const uint32_t e_row = tile * 16 + (lane & 15u);
-        float scale = 0.0f, prev = 0.0f;
-        if (lane < 16) {
-            float f[9];
-            if (e_row < W.e) {
-                raw_features(W, P, e_row, f, scale);
-            } else {
-                for (int k = 0; k < 9; ++k) f[k] = 0.0f;
-            }
-            prev = f[1];
-            store_row(S, f, xs + lane * 16);
+    uint32_t phase = 0;
+    const uint32_t tiles = (W.e + 127) / 128;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t e = tile * 128 + threadIdx.x;
+        float f[9], scale = 0.0f;
+        if (e < W.e) {
+            raw_features(W, P, e, f, scale);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) f[k] = 0.0f;
         }
-        __syncwarp();
-        TileFwd F;
-        tile_forward(S, xs, F);
-        const uint32_t g = lane >> 2;
-        const float sc_lo = __shfl_sync(kAll, scale, g), sc_hi = __shfl_sync(kAll, scale, g + 8);
-        const float pv_lo = __shfl_sync(kAll, prev, g), pv_hi = __shfl_sync(kAll, prev, g + 8);
-        if ((lane & 3u) == 0) {
-            const uint32_t e_lo = tile * 16 + g, e_hi = tile * 16 + g + 8;
-            if (e_lo < W.e) {
-                const float lam = (F.y_lo * S.tstd + S.tmean + pv_lo) * sc_lo;
-                const uint32_t a = W.inc_of_con[2 * e_lo], b = W.inc_of_con[2 * e_lo + 1];
-                if (a != 0xFFFFFFFFu) W.warm_lam_inc[a] = lam;
-                if (b != 0xFFFFFFFFu) W.warm_lam_inc[b] = lam;
-            }
-            if (e_hi < W.e) {
-                const float lam = (F.y_hi * S.tstd + S.tmean + pv_hi) * sc_hi;
-                const uint32_t a = W.inc_of_con[2 * e_hi], b = W.inc_of_con[2 * e_hi + 1];
-                if (a != 0xFFFFFFFFu) W.warm_lam_inc[a] = lam;
-                if (b != 0xFFFFFFFFu) W.warm_lam_inc[b] = lam;
-            }
+        tc_store_features(S, threadIdx.x, f);
+        float y;
+        if (!tc_tile_forward(S, phase, y)) {
+            if (threadIdx.x == 0) atomicOr(W.status, XPBD_DEV_BARRIER_TIMEOUT);
+            break;
         }
-        __syncwarp();
+        if (e < W.e) {
+            const float lam = (y * S.tstd + S.tmean + f[1]) * scale;
+            const uint32_t a = W.inc_of_con[2 * e], b = W.inc_of_con[2 * e + 1];
+            if (a != 0xFFFFFFFFu) W.warm_lam_inc[a] = lam;
+            if (b != 0xFFFFFFFFu) W.warm_lam_inc[b] = lam;
+        }
     }
+    tc_teardown(S);
 }
 
 // ---- inference on given raw features (tests): out[r] = standardised prediction y
 __global__ void __launch_bounds__(128) mlp_eval_kernel(const XpbdMlp* __restrict__ mlp, const float* __restrict__ feat,
                                                        uint32_t n, float* __restrict__ out) {
-    __shared__ SmemMlp S;
-    __shared__ __align__(16) __nv_bfloat16 xs_all[4][16 * 16];
-    load_mlp(S, *mlp);
-    __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    __nv_bfloat16* xs = xs_all[warp];
-    for (uint32_t tile = blockIdx.x * 4 + warp; tile < (n + 15) / 16; tile += gridDim.x * 4) {
-        if (lane < 16) {
-            float f[9];
-            const uint32_t r = tile * 16 + lane;
-            for (int k = 0; k < 9; ++k) f[k] = r < n ? feat[(size_t)r * 9 + k] : 0.0f;
-            store_row(S, f, xs + lane * 16);
-        }
-        __syncwarp();
-        TileFwd F;
-        tile_forward(S, xs, F);
-        const uint32_t g = lane >> 2;
-        if ((lane & 3u) == 0) {
-            if (tile * 16 + g < n) out[tile * 16 + g] = F.y_lo;
-            if (tile * 16 + g + 8 < n) out[tile * 16 + g + 8] = F.y_hi;
-        }
-        __syncwarp();
+    extern __shared__ __align__(1024) unsigned char tc_raw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>(tc_raw);
+    tc_setup(S, *mlp);
+    uint32_t phase = 0;
+    for (uint32_t tile = blockIdx.x; tile < (n + 127) / 128; tile += gridDim.x) {
+        const uint32_t r = tile * 128 + threadIdx.x;
+        float f[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) f[k] = r < n ? feat[(size_t)r * 9 + k] : 0.0f;
+        tc_store_features(S, threadIdx.x, f);
+        float y;
+        if (!tc_tile_forward(S, phase, y)) break;
+        if (r < n) out[r] = y;
     }
+    tc_teardown(S);
 }
 
 // ---- dataset collection: sampled constraints e = offset + m*stride
@@ -508,19 +620,36 @@ __global__ void mlp_publish_kernel(const float* __restrict__ master, XpbdMlp* __
 }
 
 // ---------------------------------------------------------------------------------------------- launchers
+static cudaError_t tc_prepare(const void* fn) {
+    static_assert(sizeof(TcSmem) <= kTcSmemBytes, "tensor-core MLP shared memory");
+    static std::once_flag once;
+    static cudaError_t result = cudaSuccess;
+    std::call_once(once, [] {
+        result = cudaFuncSetAttribute((const void*)mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTcSmemBytes);
+        if (result == cudaSuccess)
+            result = cudaFuncSetAttribute((const void*)mlp_eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kTcSmemBytes);
+    });
+    (void)fn;
+    return result;
+}
 cudaError_t launch_mlp_infer(const XpbdWorld& W, const XpbdMlp* mlp, int sms, cudaStream_t st) {
-    uint32_t tiles = (W.e + 15) / 16;
-    uint32_t grid = (tiles + 3) / 4;
-    if (grid > (uint32_t)sms * 8) grid = (uint32_t)sms * 8;
+    cudaError_t e = tc_prepare((const void*)mlp_infer_kernel);
+    if (e != cudaSuccess) return e;
+    uint32_t grid = (W.e + 127) / 128;
+    if (grid > (uint32_t)sms * 3) grid = (uint32_t)sms * 3;
     if (grid == 0) grid = 1;
-    mlp_infer_kernel<<<grid, 128, 0, st>>>(W, mlp);
+    mlp_infer_kernel<<<grid, 128, kTcSmemBytes, st>>>(W, mlp);
     return cudaGetLastError();
 }
 cudaError_t launch_mlp_eval(const XpbdMlp* mlp, const float* feat, uint32_t n, float* out, cudaStream_t st) {
-    uint32_t grid = ((n + 15) / 16 + 3) / 4;
+    cudaError_t e = tc_prepare((const void*)mlp_eval_kernel);
+    if (e != cudaSuccess) return e;
+    uint32_t grid = (n + 127) / 128;
     if (grid == 0) grid = 1;
-    if (grid > 1184) grid = 1184;
-    mlp_eval_kernel<<<grid, 128, 0, st>>>(mlp, feat, n, out);
+    if (grid > 444) grid = 444;
+    mlp_eval_kernel<<<grid, 128, kTcSmemBytes, st>>>(mlp, feat, n, out);
     return cudaGetLastError();
 }
 cudaError_t launch_mlp_collect_features(const XpbdWorld& W, uint32_t stride, uint32_t offset, float* feat,
