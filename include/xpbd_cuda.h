@@ -103,7 +103,7 @@ typedef struct xpbd_solver_opts {
     uint32_t blocks_per_sm;           /* 0 = autotuned / default */
     uint32_t warm_start;              /* convergence solve start: XPBD_WARM_* (0 = plain, λ = 0) */
     uint32_t cluster_ctas;            /* Gauss–Seidel in one thread-block cluster: 0 auto, 1 off, 8 or 16 CTAs */
-    uint32_t jacobi_kernel;           /* Jacobi: 0 default (= 5, else 4 where they apply, else 3), 1 warp tiles, 2 shared-
+    uint32_t jacobi_kernel;           /* Jacobi: 0 default (= 5 where it applies, else 3), 1 warp tiles, 2 shared-
                                          memory patches (their tables are built by the first call that selects them,
                                          or by xpbd_autotune, which tries them for plain Jacobi), 3 thread per
                                          particle, 4 cloth-resident (each cloth in the shared memory of one CTA or a
@@ -114,7 +114,8 @@ typedef struct xpbd_solver_opts {
                                          thread per incidence; the default up to 4,096 particles) */
     float tolerance;                  /* > 0 (or warm_start != 0): convergence solve — Jacobi, λ kept per substep,
                                          iterate until max |C + α̃λ|/rest <= tolerance, at most inner_iterations */
-    uint32_t gs_strips;               /* Gauss–Seidel over several clusters: 0 auto, 1 off, S >= 2 strips of
+    uint32_t gs_strips;               /* Gauss–Seidel over several clusters: 0 / 1 none (xpbd_autotune may pick
+                                         strips where they time faster), S >= 2 strips of
                                          cluster_ctas (16, or 8) CTAs each, particles shared between strips in
                                          global memory and ordered by per-CTA step flags (bounded waits) */
     uint32_t reserved[2];
@@ -238,8 +239,8 @@ int xpbd_color_constraints(uint32_t num_particles, uint32_t num_constraints, con
 /* ---- autotuning -------------------------------------------------------------------------------------------- */
 /* Times `frames` frames per candidate schedule on a snapshot of the state, restores the state and keeps the fastest.
  * Candidates: Jacobi execution (spatial patches — their tables built here if needed —, thread per particle, warp
- * tiles) × block size × resident blocks per SM; Gauss–Seidel: grid kernel × block × blocks per SM, and clusters of 16
- * or 8 CTAs. Writes the chosen block_threads / blocks_per_sm / cluster_ctas / jacobi_kernel to opts_out. */
+ * tiles) × block size × resident blocks per SM, plus the cloth-resident and small-batch kernels where they apply;
+ * Gauss–Seidel: grid kernel × block × blocks per SM, clusters of 16 or 8 CTAs, and 2 / 4 / 8 strips of 16 CTAs. Writes the chosen block_threads / blocks_per_sm / cluster_ctas / jacobi_kernel / gs_strips to opts_out. */
 int xpbd_autotune(xpbd_ctx* ctx, uint32_t frames, xpbd_solver_opts* opts_out);
 
 /* ---- collision pipeline introspection (bit-exact parity tests) ---------------------------------------------- */
