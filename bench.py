@@ -40,7 +40,7 @@ import numpy as np  # noqa: E402
 METRIC = "cloth-steps/s at 256² & batched; iters to 1e-4 strain residual, learned vs plain"
 UNIT = "cloth-steps/s"
 L2_BYTES = 126 * 1024 * 1024
-DEV_PARAMS_BYTES = 120  # sizeof(XpbdDevParams): the per-call parameter block uploaded by xpbd_set_params
+DEV_PARAMS_BYTES = 128  # sizeof(XpbdDevParams): the per-call parameter block uploaded by xpbd_set_params
 
 
 # ------------------------------------------------------------------------------------------------ workloads

@@ -54,7 +54,7 @@ struct DeviceBuf {
 }  // namespace
 
 // bench.py counts this block as the per-step host→device bytes of the end-to-end path
-static_assert(sizeof(XpbdDevParams) == 120, "update DEV_PARAMS_BYTES in bench.py");
+static_assert(sizeof(XpbdDevParams) == 128, "update DEV_PARAMS_BYTES in bench.py");
 
 struct xpbd_ctx {
     int device = 0;
@@ -108,6 +108,8 @@ struct xpbd_ctx {
     std::vector<XpbdGrab> grabs;  // per cloth (host copy)
     std::vector<XpbdWind> winds;  // per cloth (host copy)
     float forced_timeout_ms = 0.f;
+    float w_min_free = INFINITY;  // smallest positive inverse mass of any cloth
+    float comp_max = 0.f;         // largest compliance of any cloth
     // cloth-resident Jacobi (kernel id 7): per launch class the cloths it solves; side streams run the classes
     // concurrently (fork / join events on the context stream)
     bool wide_palette = false;       // a cloth has more than 16 compliance values: per-incidence compliances
@@ -203,6 +205,8 @@ static void fill_dev_params(xpbd_ctx* ctx) {
     p.barrier_timeout_ns = (unsigned long long)((double)tmo * 1e6);
     p.tolerance = o.tolerance;
     p.max_iterations = t.inner_iterations;
+    const float alpha_max = ctx->comp_max * p.inv_dt_sq;  // the largest α̃ any kernel forms (RN product, monotone)
+    p.plain_terms = ctx->w_min_free >= 1e-8f && std::isfinite(p.inv_dt_sq) && std::isfinite(alpha_max) ? 1u : 0u;
     if (o.tolerance > 0.f || o.warm_start) p.lambda_mode = XPBD_LAMBDA_PER_SUBSTEP;
 }
 
@@ -292,6 +296,8 @@ extern "C" int xpbd_add_cloth(xpbd_ctx* ctx, const xpbd_cloth_desc* d, uint32_t*
         for (int k = 0; k < 3; ++k)
             if (!std::isfinite(c.pos[3 * i + k])) return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "non-finite position");
     }
+    for (uint32_t i = 0; i < c.n; ++i)
+        if (c.w[i] > 0.f) ctx->w_min_free = std::min(ctx->w_min_free, c.w[i]);
     if (c.e) {
         c.ci.assign(d->constraint_i, d->constraint_i + c.e);
         c.cj.assign(d->constraint_j, d->constraint_j + c.e);
@@ -306,6 +312,7 @@ extern "C" int xpbd_add_cloth(xpbd_ctx* ctx, const xpbd_cloth_desc* d, uint32_t*
             if (!(c.rest[e] >= 0.f) || !std::isfinite(c.rest[e]) || !(c.comp[e] >= 0.f) || !std::isfinite(c.comp[e]))
                 return fail(ctx, XPBD_ERR_INVALID_ARGUMENT, "rest length / compliance must be finite and >= 0");
         }
+        for (uint32_t e = 0; e < c.e; ++e) ctx->comp_max = std::max(ctx->comp_max, c.comp[e]);
     }
     c.order = d->order;
     if (d->order == XPBD_ORDER_PRESORTED) {

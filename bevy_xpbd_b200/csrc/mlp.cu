@@ -47,7 +47,15 @@ __device__ __forceinline__ void mma16816(float* d, const uint32_t a[4], uint32_t
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
-__device__ __forceinline__ float sigm(float z) { return 1.0f / (1.0f + __expf(-z)); }
+// σ(z) = (1 + tanh(z/2)) / 2 on the hardware tanh approximation (tanh.approx.f32, one instruction): its error (about
+// 2^-11 relative to tanh) stays well below the BF16 rounding of the activations that follows, and it replaces an
+// exponential and an IEEE division in the SiLU that every hidden unit of every constraint evaluates.
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sigm(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
 __device__ __forceinline__ float silu(float z) { return z * sigm(z); }
 __device__ __forceinline__ float dsilu(float z) {
     const float s = sigm(z);
@@ -201,9 +209,10 @@ struct TcSmem {
     uint64_t bar;
     uint32_t tmem;
 };
-// Dynamic shared memory per CTA: padded so that at most three CTAs share an SM (3 × 128 of its 512 tensor-memory
+// Dynamic shared memory per CTA: padded so that at most four CTAs share an SM (4 × 128 = its 512 tensor-memory
 // columns), so the allocation never waits.
-constexpr size_t kTcSmemBytes = 72 * 1024;
+constexpr size_t kTcSmemBytes = 50 * 1024;
+constexpr uint32_t kTcCtasPerSm = 4;
 constexpr uint32_t kTcCols = 128;
 constexpr uint32_t kTcIdesc = tc_idesc_bf16(128, 64);
 
@@ -638,7 +647,7 @@ cudaError_t launch_mlp_infer(const XpbdWorld& W, const XpbdMlp* mlp, int sms, cu
     cudaError_t e = tc_prepare((const void*)mlp_infer_kernel);
     if (e != cudaSuccess) return e;
     uint32_t grid = (W.e + 127) / 128;
-    if (grid > (uint32_t)sms * 3) grid = (uint32_t)sms * 3;
+    if (grid > (uint32_t)sms * kTcCtasPerSm) grid = (uint32_t)sms * kTcCtasPerSm;
     if (grid == 0) grid = 1;
     mlp_infer_kernel<<<grid, 128, kTcSmemBytes, st>>>(W, mlp);
     return cudaGetLastError();
@@ -648,7 +657,7 @@ cudaError_t launch_mlp_eval(const XpbdMlp* mlp, const float* feat, uint32_t n, f
     if (e != cudaSuccess) return e;
     uint32_t grid = (n + 127) / 128;
     if (grid == 0) grid = 1;
-    if (grid > 444) grid = 444;
+    if (grid > 148 * kTcCtasPerSm) grid = 148 * kTcCtasPerSm;
     mlp_eval_kernel<<<grid, 128, kTcSmemBytes, st>>>(mlp, feat, n, out);
     return cudaGetLastError();
 }

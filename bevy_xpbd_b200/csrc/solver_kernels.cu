@@ -316,7 +316,9 @@ __global__ void __launch_bounds__(BLOCK) jacobi_persistent_kernel(XpbdWorld W, u
 // Branch-free: a skipped term is selected as +0, which leaves the running sum unchanged (the sum starts at +0 and
 // adding terms never yields -0).
 // UNCHECKED: n̂ by fpdiv3_unchecked — only when the pass's coordinate check found every position in range.
-template <bool UNCHECKED>
+// PLAIN: XpbdDevParams::plain_terms holds — α̃ is finite (so −C − α̃·0 = −C) and the w sum of a free row's
+// constraint is >= its own inverse mass >= 1e-8 (so only the length test can skip the term).
+template <bool UNCHECKED, bool PLAIN>
 __device__ __forceinline__ F3 row_term(const F3 self, float wi, const float4 po, float rest, float alpha_t) {
     const F3 gv = sub3(self, f3(po));
     const float len = len3(gv);
@@ -328,8 +330,8 @@ __device__ __forceinline__ F3 row_term(const F3 self, float wi, const float4 po,
     }
     const float C = __fsub_rn(len, rest);
     const float wsum = __fadd_rn(__fadd_rn(wi, po.w), alpha_t);
-    const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
-    const bool use = !(len < 1e-8f) && !(wsum < 1e-8f);
+    const float dlam = __fdiv_rn(PLAIN ? -C : __fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
+    const bool use = PLAIN ? !(len < 1e-8f) : !(len < 1e-8f) && !(wsum < 1e-8f);
     return {use ? __fmul_rn(__fmul_rn(nrm.x, wi), dlam) : 0.0f, use ? __fmul_rn(__fmul_rn(nrm.y, wi), dlam) : 0.0f,
             use ? __fmul_rn(__fmul_rn(nrm.z, wi), dlam) : 0.0f};
 }
@@ -353,17 +355,19 @@ __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevPara
     const F3 self = f3(ps);
     if (!persist) {
         // λ = 0 at every pass (reference mode): pairs of independent terms, then the remainder, summed in
-        // incidence order
-        auto sum_terms = [&](auto unchecked_tag) {
-            constexpr bool U = decltype(unchecked_tag)::value;
+        // incidence order. The compliance source (palette or per-incidence array) is fixed per launch.
+        auto sum_terms = [&](auto unchecked_tag, auto plain_tag, auto wide_tag) {
+            constexpr bool U = decltype(unchecked_tag)::value, PL = decltype(plain_tag)::value;
+            constexpr bool WIDE = decltype(wide_tag)::value;
+            auto comp_of = [&](uint2 rec, uint32_t k) { return WIDE ? W.inc_comp[k] : pal[rec.x >> 28]; };
             uint32_t k = rs;
             for (; k + 2 <= re; k += 2) {  // pairs: measured faster than groups of four or six
                 F3 c[2];
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     const uint2 rec = recs[k + u];
-                    c[u] = row_term<U>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
-                                       __fmul_rn(inc_compliance(W, pal, rec, k + u), P.inv_dt_sq));
+                    c[u] = row_term<U, PL>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
+                                           __fmul_rn(comp_of(rec, k + u), P.inv_dt_sq));
                 }
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
@@ -374,17 +378,26 @@ __device__ __forceinline__ void jacobi_row(const XpbdWorld& W, const XpbdDevPara
             }
             for (; k < re; ++k) {
                 const uint2 rec = recs[k];
-                const F3 c = row_term<U>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
-                                         __fmul_rn(inc_compliance(W, pal, rec, k), P.inv_dt_sq));
+                const F3 c = row_term<U, PL>(self, ps.w, jin[rec.x & XPBD_OTHER_MASK], __uint_as_float(rec.y),
+                                             __fmul_rn(comp_of(rec, k), P.inv_dt_sq));
                 ax = __fadd_rn(ax, c.x);
                 ay = __fadd_rn(ay, c.y);
                 az = __fadd_rn(az, c.z);
             }
         };
-        if (unchecked)
-            sum_terms(std::true_type{});
+        const std::true_type yes;
+        const std::false_type no;
+        if (W.inc_comp) {  // batches with wide compliance sets
+            if (unchecked)
+                sum_terms(yes, no, yes);
+            else
+                sum_terms(no, no, yes);
+        } else if (unchecked && P.plain_terms)
+            sum_terms(yes, yes, no);
+        else if (unchecked)
+            sum_terms(yes, no, no);
         else
-            sum_terms(std::false_type{});
+            sum_terms(no, no, no);
     } else {
         for (uint32_t k = rs; k < re; k += 4) {
             float cx[4], cy[4], cz[4];

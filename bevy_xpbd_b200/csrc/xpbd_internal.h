@@ -40,6 +40,10 @@ struct XpbdDevParams {  // the per-call uniform block (ClothSimParamsGpu, cloth_
     unsigned long long barrier_timeout_ns;
     float tolerance;       // convergence solve: stop when max |C + α̃λ|/rest of the pre-update state <= tolerance
     uint32_t max_iterations;
+    // 1 when every α̃ = compliance·inv_dt_sq is finite and every free particle's inverse mass is >= 1e-8 (checked on
+    // the host): then −C − α̃·0 is −C bit for bit and no constraint at a free particle has w sum < 1e-8, so the
+    // reset-mode Jacobi term skips both evaluations
+    uint32_t plain_terms;
 };
 
 #define XPBD_MLP_IN 9
