@@ -1460,13 +1460,14 @@ static int ensure_collision_buffers(xpbd_ctx* ctx) {
         if (err == cudaSuccess) B.vals = dev_alloc<uint32_t>(ctx, N, &err);
         if (err == cudaSuccess) B.keys_sorted = dev_alloc<uint32_t>(ctx, N, &err);
         if (err == cudaSuccess) B.vals_sorted = dev_alloc<uint32_t>(ctx, N, &err);
-        if (err == cudaSuccess) B.table_start = dev_alloc<uint32_t>(ctx, (size_t)1 << B.table_bits, &err);
+        if (err == cudaSuccess) B.table = dev_alloc<uint2>(ctx, (size_t)1 << B.table_bits, &err);
+        if (err == cudaSuccess) B.pos_sorted = dev_alloc<float4>(ctx, N, &err);
         if (err == cudaSuccess) B.pair_count = dev_alloc<uint32_t>(ctx, N + 1, &err);
         B.sort_scratch_bytes = radix_sort_scratch_bytes(N);
         if (err == cudaSuccess) B.sort_scratch = dev_alloc<char>(ctx, B.sort_scratch_bytes, &err);
         if (err != cudaSuccess) return cuda_fail(ctx, err, "collision buffers");
         // table entries are validated on use; any initial content is safe
-        CK(cudaMemsetAsync(B.table_start, 0xFF, ((size_t)1 << B.table_bits) * 4, ctx->stream), "memset");
+        CK(cudaMemsetAsync(B.table, 0xFF, ((size_t)1 << B.table_bits) * sizeof(uint2), ctx->stream), "memset");
         ctx->coll_ready = true;
     }
     if (o.collision == XPBD_COLLISION_RING_FILTER && ctx->coll_ring_depth_built != o.ring_depth) {

@@ -309,10 +309,16 @@ cudaError_t launch_hash_keys(const float4* x, uint32_t n, float inv_cell, uint32
 }
 
 // ---------------------------------------------------------------------------------------------- bucket table
-__global__ void bucket_table_kernel(const uint32_t* __restrict__ skeys, uint32_t n, uint32_t* __restrict__ start) {
+// Bucket ranges of the sorted keys, and the positions gathered into sorted order so that the candidates of a bucket
+// are read from consecutive addresses.
+__global__ void bucket_table_kernel(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
+                                    const float4* __restrict__ pos, uint32_t n, uint2* __restrict__ table,
+                                    float4* __restrict__ pos_sorted) {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         const uint32_t k = skeys[p];
-        if (p == 0 || skeys[p - 1] != k) start[k] = p;
+        if (p == 0 || skeys[p - 1] != k) table[k].x = p;
+        if (p + 1 == n || skeys[p + 1] != k) table[k].y = p + 1;
+        pos_sorted[p] = pos[svals[p]];
     }
 }
 
@@ -329,7 +335,7 @@ cudaError_t collision_build(const XpbdWorld& W, const float4* pos, const Collisi
     uint32_t grid = (W.n + 255) / 256;
     if (grid > (uint32_t)sms * 8) grid = (uint32_t)sms * 8;
     if (grid == 0) grid = 1;
-    bucket_table_kernel<<<grid, 256, 0, st>>>(B.keys_sorted, W.n, B.table_start);
+    bucket_table_kernel<<<grid, 256, 0, st>>>(B.keys_sorted, B.vals_sorted, pos, W.n, B.table, B.pos_sorted);
     if (launches) *launches += 2;
     return cudaGetLastError();
 }
@@ -354,12 +360,11 @@ __device__ __forceinline__ bool ring_contains(const uint32_t* __restrict__ off, 
     return false;
 }
 
-// Pair (a<b) narrow phase of xpbd_cpu.rs:84-121 (filter 1: rest-distance test :94-100; filter 2: ring filter).
-// On acceptance returns the correction of particle `self` (a or b).
-__device__ __forceinline__ bool narrow_pair(const float4* __restrict__ src, const float4* __restrict__ rest,
+// Pair (a<b) narrow phase of xpbd_cpu.rs:84-121 (filter 1: rest-distance test :94-100; filter 2: ring filter), on
+// the positions pa, pb of a, b. On acceptance returns the correction of particle `self` (a or b).
+__device__ __forceinline__ bool narrow_pair(const float4 pa, const float4 pb, const float4* __restrict__ rest,
                                             const CollisionBuffers& B, uint32_t filter, float thickness,
                                             float coll_scale, uint32_t a, uint32_t b, uint32_t self, F3c& out) {
-    const float4 pa = src[a], pb = src[b];
     const float w_a = pa.w, w_b = pb.w;
     if (w_a <= 0.0f && w_b <= 0.0f) return false;
     const float t2 = __fmul_rn(thickness, thickness);
@@ -402,11 +407,12 @@ __device__ __forceinline__ void cell_face_gaps(float u, float f, float reach, fl
     hi2 = __fmul_rn(hi, hi);
 }
 
-// Visits every particle j != i in the (deduplicated) buckets of the 27 cells around i's cell, leaving out the cells
-// that hold no particle within `thickness` of i. The narrow phase accepts only pairs at most `thickness` apart, so
-// when thickness is below the cell size (every accepted partner then lies in one of the 27 cells) the accepted
-// partners are the same; a left-out cell is not marked as seen, so its bucket is still visited through any other
-// cell that hashes to it. Partners are summed in index order, so the visiting order does not change a result.
+// Visits every particle j != i, with its position, in the (deduplicated) buckets of the 27 cells around i's cell,
+// leaving out the cells that hold no particle within `thickness` of i. The narrow phase accepts only pairs at most
+// `thickness` apart, so when thickness is below the cell size (every accepted partner then lies in one of the 27
+// cells) the accepted partners are the same; a left-out cell is not marked as seen, so its bucket is still visited
+// through any other cell that hashes to it. Partners are summed in index order, so the visiting order does not
+// change a result.
 template <typename F>
 __device__ __forceinline__ void for_each_candidate(const float4* __restrict__ src, const CollisionBuffers& B,
                                                    uint32_t n, uint32_t i, float inv_cell, float thickness, F&& f) {
@@ -435,11 +441,16 @@ __device__ __forceinline__ void for_each_candidate(const float4* __restrict__ sr
                 for (int q = 0; q < nseen; ++q) dup |= (seen[q] == h);
                 if (dup) continue;
                 seen[nseen++] = h;
-                const uint32_t s = B.table_start[h];
+                // a bucket entry is this pass's when its first position holds the bucket's first key; then its end
+                // was written by the same pass
+                const uint2 t = B.table[h];
+                const uint32_t s = t.x;
                 if (s >= n || B.keys_sorted[s] != h || (s > 0 && B.keys_sorted[s - 1] == h)) continue;
-                for (uint32_t q = s; q < n && B.keys_sorted[q] == h; ++q) {
+                const uint32_t e = min(t.y, n);
+                for (uint32_t q = s; q < e; ++q) {
                     const uint32_t j = B.vals_sorted[q];
-                    if (j != i) f(j);
+                    const float4 pj = B.pos_sorted[q];
+                    if (j != i) f(j, pj);
                 }
             }
         }
@@ -456,19 +467,21 @@ __device__ __forceinline__ bool collect_partners(const float4* __restrict__ src,
                                                  uint32_t* pj, F3c* pc, int& cnt) {
     cnt = 0;
     bool overflow = false;
-    for_each_candidate(src, B, n, i, inv_cell, thickness, [&](uint32_t j) {
+    const float4 p_i = src[i];
+    for_each_candidate(src, B, n, i, inv_cell, thickness, [&](uint32_t j, const float4 p_j) {
         if ((long long)j <= lo) return;
         if (ONLY_GREATER && j < i) return;
+        const bool i_first = i < j;
+        const uint32_t a = i_first ? i : j, b = i_first ? j : i;
+        const float4 pa = i_first ? p_i : p_j, pb = i_first ? p_j : p_i;
         if (cnt == kPartnerCap && j > pj[kPartnerCap - 1]) {
             // cheap reject before the narrow test; it may be accepted, so remember that more partners remain
             F3c tmp;
-            const uint32_t a = min(i, j), b = max(i, j);
-            if (narrow_pair(src, rest, B, filter, thickness, coll_scale, a, b, i, tmp)) overflow = true;
+            if (narrow_pair(pa, pb, rest, B, filter, thickness, coll_scale, a, b, i, tmp)) overflow = true;
             return;
         }
         F3c corr;
-        const uint32_t a = min(i, j), b = max(i, j);
-        if (!narrow_pair(src, rest, B, filter, thickness, coll_scale, a, b, i, corr)) return;
+        if (!narrow_pair(pa, pb, rest, B, filter, thickness, coll_scale, a, b, i, corr)) return;
         if (cnt == kPartnerCap) overflow = true;  // evicts the largest
         int p = (cnt < kPartnerCap) ? cnt++ : kPartnerCap - 1;
         while (p > 0 && pj[p - 1] > j) {
@@ -535,10 +548,11 @@ __global__ void pair_count_kernel(XpbdWorld W, const float4* __restrict__ src, C
     const XpbdDevParams& P = *W.params;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.n; i += gridDim.x * blockDim.x) {
         uint32_t c = 0;
-        for_each_candidate(src, B, W.n, i, inv_cell, P.thickness, [&](uint32_t j) {
+        const float4 p_i = src[i];
+        for_each_candidate(src, B, W.n, i, inv_cell, P.thickness, [&](uint32_t j, const float4 p_j) {
             if (j < i) return;
             F3c tmp;
-            if (narrow_pair(src, W.rest, B, filter, P.thickness, P.coll_scale, i, j, i, tmp)) ++c;
+            if (narrow_pair(p_i, p_j, W.rest, B, filter, P.thickness, P.coll_scale, i, j, i, tmp)) ++c;
         });
         counts[i] = c;
     }
