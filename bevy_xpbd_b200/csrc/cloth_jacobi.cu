@@ -369,11 +369,18 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
                 if (ps.w <= 0.0f) continue;
                 const uint32_t rs = s_roff[p], re = s_roff[p + 1];
                 float ax = 0.0f, ay = 0.0f, az = 0.0f;
-                for (uint32_t k = rs; k < re; ++k) {
-                    const float4 t = s_term[k];
-                    ax = __fadd_rn(ax, t.x);
-                    ay = __fadd_rn(ay, t.y);
-                    az = __fadd_rn(az, t.z);
+                // eight terms loaded at once, then added in table order; a slot past the row's end adds +0, which
+                // leaves a sum started at +0 unchanged (such a sum never becomes -0)
+                for (uint32_t k = rs; k < re; k += 8) {
+                    float4 t[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) t[u] = k + u < re ? s_term[k + u] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        ax = __fadd_rn(ax, t[u].x);
+                        ay = __fadd_rn(ay, t[u].y);
+                        az = __fadd_rn(az, t[u].z);
+                    }
                 }
                 F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
                 if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
