@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "xpbd_cluster.h"
 #include "xpbd_fpdiv.h"
 #include "xpbd_internal.h"
@@ -116,7 +118,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // Endpoint i is always this CTA's particle (records are grouped by the rank owning i) and goes through the CTA's own
 // shared window (xs_base); endpoint j too for interior records (LOCAL), otherwise through the cluster window of the
 // CTA owning it.
-template <bool LOCAL>
+// PLAIN (XpbdDevParams::plain_terms): α̃ finite, so −C − α̃·0 = −C, and a constraint with a free endpoint has a w sum
+// >= 1e-8 (constraints between two pinned particles return before), so the w-sum test is skipped.
+template <bool LOCAL, bool PLAIN>
 __device__ __forceinline__ void gs_solve(const uint4 cr, const uint32_t* s_rank_base, uint32_t xs_base, uint32_t shift,
                                          uint32_t mask, const XpbdDevParams& P) {
     const uint32_t ai = xs_base + ((cr.x & mask) << 4);
@@ -137,8 +141,8 @@ __device__ __forceinline__ void gs_solve(const uint4 cr, const uint32_t* s_rank_
     const float C = __fsub_rn(len, __uint_as_float(cr.z));
     const float alpha_t = __fmul_rn(__uint_as_float(cr.w), P.inv_dt_sq);
     const float wsum = __fadd_rn(__fadd_rn(w_i, w_j), alpha_t);
-    if (wsum < 1e-8f) return;
-    const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
+    if (!PLAIN && wsum < 1e-8f) return;
+    const float dlam = __fdiv_rn(PLAIN ? -C : __fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
     const V3 og = {__fmul_rn(P.omega, gv.x), __fmul_rn(P.omega, gv.y), __fmul_rn(P.omega, gv.z)};
     const V3 dx_i = vclamp(vmul(vmul(og, w_i), dlam));
     V3 dxj = vmul(vmul(og, w_j), dlam);
@@ -257,11 +261,18 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
                 }
                 // records touching boundary particles, then the cluster barrier's arrive, then the records of this
                 // CTA's interior particles (no other CTA reads or writes those) while the barrier completes
-                for (uint32_t e = tid; e < nb && !failed; e += nthr)
-                    gs_solve<false>(rec[e], s_rank_base, xs_base, shift, mask, P);
-                cluster_arrive();
-                for (uint32_t e = nb + tid; e < e1 - e0 && !failed; e += nthr)
-                    gs_solve<true>(rec[e], s_rank_base, xs_base, shift, mask, P);
+                auto sweep = [&](auto plain_tag) {
+                    constexpr bool PL = decltype(plain_tag)::value;
+                    for (uint32_t e = tid; e < nb && !failed; e += nthr)
+                        gs_solve<false, PL>(rec[e], s_rank_base, xs_base, shift, mask, P);
+                    cluster_arrive();
+                    for (uint32_t e = nb + tid; e < e1 - e0 && !failed; e += nthr)
+                        gs_solve<true, PL>(rec[e], s_rank_base, xs_base, shift, mask, P);
+                };
+                if (P.plain_terms)
+                    sweep(std::true_type{});
+                else
+                    sweep(std::false_type{});
                 __syncthreads();  // this CTA's interior updates before anyone's next color
                 cluster_wait();
             }
