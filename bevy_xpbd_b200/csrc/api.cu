@@ -1267,7 +1267,7 @@ static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
         if (q > 1024) continue;
         std::vector<uint4> rec;
         std::vector<uint32_t> lroff((size_t)cl * (q + 1), 0), rbase(cl, 0);
-        uint32_t m_max = 0;
+        uint32_t m_max = 0, longest = 1;
         for (uint32_t r = 0; r < cl; ++r) {
             rbase[r] = (uint32_t)rec.size();
             const uint32_t p0 = r * q, p1 = std::min(N, p0 + q);
@@ -1279,15 +1279,17 @@ static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
                                                          : pal[(size_t)cloth_of[p] * XPBD_PALETTE + (inc[k].x >> 28)];
                     uint32_t cb;
                     memcpy(&cb, &comp, 4);
-                    rec.push_back(make_uint4(p - p0, ((o / q) << 16) | (o % q), inc[k].y, cb));
+                    rec.push_back(make_uint4((p - p0) | ((k - roff[p]) << 16), ((o / q) << 16) | (o % q), inc[k].y, cb));
                 }
+                longest = std::max(longest, roff[p + 1] - roff[p]);
             }
             const uint32_t m = (uint32_t)rec.size() - rbase[r];
             for (uint32_t p = (p1 > p0 ? p1 - p0 : 0); p <= q; ++p) lroff[(size_t)r * (q + 1) + p] = m;
             m_max = std::max(m_max, m);
         }
         const uint32_t block = std::min<uint32_t>(1024, std::max<uint32_t>(32, (std::max(m_max, q) + 31) / 32 * 32));
-        if (m_max > 4096 || !small_batch_supported(cl, block, q, m_max)) {
+        const uint32_t stride = longest | 1u;
+        if (m_max > 4096 || longest > 0xFFFFu || !small_batch_supported(cl, block, q, m_max, stride)) {
             cudaGetLastError();
             continue;
         }
@@ -1301,7 +1303,7 @@ static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
         CK(cudaMemcpyAsync(d_roff, lroff.data(), lroff.size() * 4, cudaMemcpyHostToDevice, st), "upload");
         CK(cudaMemcpyAsync(d_rbase, rbase.data(), cl * 4, cudaMemcpyHostToDevice, st), "upload");
         CK(cudaStreamSynchronize(st), "upload sync");
-        ctx->small = SmallBatch{d_rec, d_roff, d_rbase, q, m_max};
+        ctx->small = SmallBatch{d_rec, d_roff, d_rbase, q, m_max, stride};
         ctx->small_cl = cl;
         ctx->small_block = block;
         ctx->small_ok = true;

@@ -298,8 +298,12 @@ cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTab
 // terms in table order and writes its new position into the other buffer; a cluster barrier ends the pass. The
 // constraint is evaluated from both ends (as the thread-per-particle kernel does), which costs instructions but
 // keeps the pass to one barrier: for a small cloth the pass is latency-bound, not issue-bound.
-size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max) {
-    return 2 * (size_t)q * 16 + (size_t)m_max * 32 + ((size_t)(q + 1) * 4 + 15) / 16 * 16;
+// The terms sit in shared memory row by row with an odd stride of float4 slots (row p, slot u at p·stride + u): an
+// incidence writes its slot, and when the row owners read slot u of their rows, eight consecutive owners (one
+// 128-byte phase of a 16-byte load) fall on eight different bank groups. Rows packed back to back (an average of
+// 12 slots apart) put half of them on the same banks, and the owners' reads were the longest part of the pass.
+size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max, uint32_t stride) {
+    return 2 * (size_t)q * 16 + (size_t)m_max * 16 + (size_t)q * stride * 16 + ((size_t)(q + 1) * 4 + 15) / 16 * 16;
 }
 
 template <int CL>
@@ -309,7 +313,9 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
     float4* s_pos0 = reinterpret_cast<float4*>(smem);
     uint4* s_rec = reinterpret_cast<uint4*>(smem + 2 * (size_t)q * 16);
     float4* s_term = reinterpret_cast<float4*>(smem + 2 * (size_t)q * 16 + (size_t)B.m_max * 16);
-    uint32_t* s_roff = reinterpret_cast<uint32_t*>(smem + 2 * (size_t)q * 16 + (size_t)B.m_max * 32);
+    uint32_t* s_roff =
+        reinterpret_cast<uint32_t*>(smem + 2 * (size_t)q * 16 + (size_t)B.m_max * 16 + (size_t)q * B.stride * 16);
+    const uint32_t stride = B.stride;
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
     const uint32_t rank = cluster_rank();
     const uint32_t p0 = rank * q;
@@ -342,7 +348,8 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
             const uint32_t src = pos_base + b * q * 16u;
             for (uint32_t k = tid; k < m; k += nthr) {
                 const uint4 r = s_rec[k];
-                const float4 ps = ld_local(src + r.x * 16u);
+                const uint32_t self = r.x & 0xFFFFu;  // {slot in the row << 16 | self local}
+                const float4 ps = ld_local(src + self * 16u);
                 const uint32_t ro = r.y >> 16;  // {rank << 16 | local}
                 const uint32_t ao = src + (r.y & 0xFFFFu) * 16u;
                 const float4 po = ro == rank ? ld_local(ao) : ld_dsmem(map_rank(ao, ro));
@@ -360,7 +367,7 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
                     t = make_float4(__fmul_rn(__fmul_rn(n.x, ps.w), dlam), __fmul_rn(__fmul_rn(n.y, ps.w), dlam),
                                     __fmul_rn(__fmul_rn(n.z, ps.w), dlam), 0.0f);
                 }
-                s_term[k] = t;
+                s_term[self * stride + (r.x >> 16)] = t;
             }
             __syncthreads();
             const bool last = it + 1 == I;
@@ -371,10 +378,11 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
                 float ax = 0.0f, ay = 0.0f, az = 0.0f;
                 // eight terms loaded at once, then added in table order; a slot past the row's end adds +0, which
                 // leaves a sum started at +0 unchanged (such a sum never becomes -0)
-                for (uint32_t k = rs; k < re; k += 8) {
+                const float4* row = s_term + p * stride;
+                for (uint32_t k = 0; k < re - rs; k += 8) {
                     float4 t[8];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) t[u] = k + u < re ? s_term[k + u] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int u = 0; u < 8; ++u) t[u] = k + u < re - rs ? row[k + u] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
                         ax = __fadd_rn(ax, t[u].x);
@@ -437,10 +445,10 @@ static cudaLaunchConfig_t small_cfg(uint32_t cl, uint32_t block, size_t smem, cu
     return cfg;
 }
 
-bool small_batch_supported(uint32_t cl, uint32_t block, uint32_t q, uint32_t m_max) {
+bool small_batch_supported(uint32_t cl, uint32_t block, uint32_t q, uint32_t m_max, uint32_t stride) {
     const void* fn = small_fn(cl);
     if (!fn || block > 1024 || q > block) return false;
-    const size_t smem = small_batch_smem_bytes(q, m_max);
+    const size_t smem = small_batch_smem_bytes(q, m_max, stride);
     if (smem > 220 * 1024) return false;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
     if (cl > 8 && cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
@@ -460,7 +468,7 @@ cudaError_t launch_small_batch(uint32_t cl, uint32_t block, const XpbdWorld& W, 
     const void* fn = small_fn(cl);
     if (!fn) return cudaErrorInvalidValue;
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = small_cfg(cl, block, small_batch_smem_bytes(B.q, B.m_max), st, attr);
+    cudaLaunchConfig_t cfg = small_cfg(cl, block, small_batch_smem_bytes(B.q, B.m_max, B.stride), st, attr);
     XpbdWorld w = W;
     SmallBatch b = B;
     void* args[] = {&w, &b, &substeps};

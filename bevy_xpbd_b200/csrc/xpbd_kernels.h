@@ -62,14 +62,16 @@ cudaError_t cloth_kernel_prepare();  // opt-in shared-memory sizes (host, once)
 bool cloth_class_launchable(int cls);  // a cluster of the class fits on this device
 // A whole small batch in one cluster of cl (8 or 16) CTAs, thread per incidence (cloth_jacobi.cu).
 struct SmallBatch {
-    const uint4* rec;       // per incidence, rank-major: {self local, other endpoint (rank << 16 | local), rest, comp}
+    const uint4* rec;       // per incidence, rank-major: {self local | slot in its row << 16, other endpoint
+                            // (rank << 16 | local), rest, comp}
     const uint32_t* roff;   // per rank: q + 1 local row starts into the rank's incidences
     const uint32_t* rbase;  // per rank: first incidence of the rank in rec
     uint32_t q;             // particles per rank
     uint32_t m_max;         // largest incidence count of a rank
+    uint32_t stride;        // term slots per row in shared memory: odd, >= the longest row
 };
-size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max);
-bool small_batch_supported(uint32_t cl, uint32_t block, uint32_t q, uint32_t m_max);
+size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max, uint32_t stride);
+bool small_batch_supported(uint32_t cl, uint32_t block, uint32_t q, uint32_t m_max, uint32_t stride);
 cudaError_t launch_small_batch(uint32_t cl, uint32_t block, const XpbdWorld& W, const SmallBatch& B,
                                uint32_t substeps, cudaStream_t st);
 
