@@ -302,8 +302,10 @@ cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTab
 // incidence writes its slot, and when the row owners read slot u of their rows, eight consecutive owners (one
 // 128-byte phase of a 16-byte load) fall on eight different bank groups. Rows packed back to back (an average of
 // 12 slots apart) put half of them on the same banks, and the owners' reads were the longest part of the pass.
+// The particles' x and v stay in shared memory for the whole frame (the predict and the velocity update of every
+// substep read and write them there; global memory is read at the start and written at the end).
 size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max, uint32_t stride) {
-    return 2 * (size_t)q * 16 + (size_t)m_max * 16 + (size_t)q * stride * 16 + ((size_t)(q + 1) * 4 + 15) / 16 * 16;
+    return 4 * (size_t)q * 16 + (size_t)m_max * 16 + (size_t)q * stride * 16 + ((size_t)(q + 1) * 4 + 15) / 16 * 16;
 }
 
 template <int CL>
@@ -311,10 +313,12 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t q = B.q;
     float4* s_pos0 = reinterpret_cast<float4*>(smem);
-    uint4* s_rec = reinterpret_cast<uint4*>(smem + 2 * (size_t)q * 16);
-    float4* s_term = reinterpret_cast<float4*>(smem + 2 * (size_t)q * 16 + (size_t)B.m_max * 16);
+    float4* s_x = s_pos0 + 2 * (size_t)q;
+    float4* s_v = s_x + q;
+    uint4* s_rec = reinterpret_cast<uint4*>(smem + 4 * (size_t)q * 16);
+    float4* s_term = reinterpret_cast<float4*>(smem + 4 * (size_t)q * 16 + (size_t)B.m_max * 16);
     uint32_t* s_roff =
-        reinterpret_cast<uint32_t*>(smem + 2 * (size_t)q * 16 + (size_t)B.m_max * 16 + (size_t)q * B.stride * 16);
+        reinterpret_cast<uint32_t*>(smem + 4 * (size_t)q * 16 + (size_t)B.m_max * 16 + (size_t)q * B.stride * 16);
     const uint32_t stride = B.stride;
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
     const uint32_t rank = cluster_rank();
@@ -324,6 +328,10 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
     const uint32_t m = B.roff[rank * (q + 1) + np];
     for (uint32_t k = tid; k <= np; k += nthr) s_roff[k] = B.roff[rank * (q + 1) + k];
     for (uint32_t k = tid; k < m; k += nthr) s_rec[k] = B.rec[B.rbase[rank] + k];
+    for (uint32_t p = tid; p < np; p += nthr) {
+        s_x[p] = W.x[p0 + p];
+        s_v[p] = W.v[p0 + p];
+    }
     const uint32_t pos_base = smem_u32(s_pos0);
     uint32_t b = 0;  // buffer the next predict writes: never the one a peer may still be reading
     const uint32_t I = P.iterations;
@@ -331,10 +339,10 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
     for (uint32_t s = 0; s < substeps; ++s) {
         for (uint32_t p = tid; p < np; p += nthr) {
             const uint32_t g = p0 + p;
-            const float4 x4 = W.x[g];
+            const float4 x4 = s_x[p];
             float4 out = x4;
             if (x4.w > 0.0f) {
-                F3 vel = f3(W.v[g]);
+                F3 vel = f3(s_v[p]);
                 const F3 pos = predict_w(W, g, f3(x4), vel, P);
                 out = make_float4(pos.x, pos.y, pos.z, x4.w);
             }
@@ -395,11 +403,10 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
                 delta = clamp_correction(delta);
                 F3 xn = add3(f3(ps), delta);
                 if (last) {
-                    const uint32_t g = p0 + p;
                     F3 vel;
-                    xn = finalize_particle(xn, f3(W.x[g]), vel, P, W.status);
-                    W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
-                    W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+                    xn = finalize_particle(xn, f3(s_x[p]), vel, P, W.status);
+                    s_x[p] = make_float4(xn.x, xn.y, xn.z, ps.w);
+                    s_v[p] = make_float4(vel.x, vel.y, vel.z, 0.0f);
                 }
                 s_pos0[(b ^ 1u) * q + p] = make_float4(xn.x, xn.y, xn.z, ps.w);
             }
@@ -410,15 +417,18 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
             for (uint32_t p = tid; p < np; p += nthr) {
                 const float4 ps = s_pos0[b * q + p];
                 if (ps.w <= 0.0f) continue;
-                const uint32_t g = p0 + p;
                 F3 vel;
-                const F3 xn = finalize_particle(f3(ps), f3(W.x[g]), vel, P, W.status);
-                W.x[g] = make_float4(xn.x, xn.y, xn.z, ps.w);
-                W.v[g] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+                const F3 xn = finalize_particle(f3(ps), f3(s_x[p]), vel, P, W.status);
+                s_x[p] = make_float4(xn.x, xn.y, xn.z, ps.w);
+                s_v[p] = make_float4(vel.x, vel.y, vel.z, 0.0f);
             }
         }
         // the last pass read buffer b ^ 1 (peers may still be reading it) and wrote b: the next predict writes b
         __syncthreads();
+    }
+    for (uint32_t p = tid; p < np; p += nthr) {  // each particle's own thread wrote its x and v
+        W.x[p0 + p] = s_x[p];
+        W.v[p0 + p] = s_v[p];
     }
     cluster_sync();
 }
