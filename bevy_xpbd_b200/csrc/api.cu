@@ -1468,8 +1468,9 @@ static int ensure_collision_buffers(xpbd_ctx* ctx) {
         B.sort_scratch_bytes = radix_sort_scratch_bytes(N);
         if (err == cudaSuccess) B.sort_scratch = dev_alloc<char>(ctx, B.sort_scratch_bytes, &err);
         if (err != cudaSuccess) return cuda_fail(ctx, err, "collision buffers");
-        // table entries are validated on use; any initial content is safe
+        // every entry empty, and a valid "previous build" of key 0 for the first build to clear
         CK(cudaMemsetAsync(B.table, 0xFF, ((size_t)1 << B.table_bits) * sizeof(uint2), ctx->stream), "memset");
+        CK(cudaMemsetAsync(B.keys_sorted, 0, (size_t)N * 4, ctx->stream), "memset");
         ctx->coll_ready = true;
     }
     if (o.collision == XPBD_COLLISION_RING_FILTER && ctx->coll_ring_depth_built != o.ring_depth) {

@@ -33,9 +33,13 @@ __device__ __forceinline__ uint32_t hash_cell(int3 c, uint32_t mask) {
     return (((uint32_t)c.x * 73856093u) ^ ((uint32_t)c.y * 19349663u) ^ ((uint32_t)c.z * 83492791u)) & mask;
 }
 
+// With a bucket table: also marks empty the entries of the previous build's keys (still in `prev_sorted`, which
+// the sort that follows overwrites), so that every valid-looking entry belongs to the current build.
 __global__ void hash_keys_kernel(const float4* __restrict__ x, uint32_t n, float inv_cell, uint32_t mask,
-                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                                 uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                 const uint32_t* __restrict__ prev_sorted, uint2* __restrict__ table) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (table) table[prev_sorted[i]] = make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
         keys[i] = hash_cell(cell_of(x[i], inv_cell), mask);
         if (vals) vals[i] = i;
     }
@@ -304,7 +308,7 @@ cudaError_t launch_hash_keys(const float4* x, uint32_t n, float inv_cell, uint32
     uint32_t grid = (n + 255) / 256;
     if (grid > 148u * 16u) grid = 148u * 16u;
     hash_keys_kernel<<<grid, 256, 0, st>>>(x, n, inv_cell, (bits >= 32) ? 0xFFFFFFFFu : ((1u << bits) - 1u), keys,
-                                           vals);
+                                           vals, nullptr, nullptr);
     return cudaGetLastError();
 }
 
@@ -324,7 +328,14 @@ __global__ void bucket_table_kernel(const uint32_t* __restrict__ skeys, const ui
 
 cudaError_t collision_build(const XpbdWorld& W, const float4* pos, const CollisionBuffers& B, float inv_cell,
                             int sms, cudaStream_t st, uint64_t* launches) {
-    cudaError_t e = launch_hash_keys(pos, W.n, inv_cell, B.table_bits, B.keys, B.vals, st);
+    if (W.n > 0) {
+        uint32_t g = (W.n + 255) / 256;
+        if (g > 148u * 16u) g = 148u * 16u;
+        hash_keys_kernel<<<g, 256, 0, st>>>(pos, W.n, inv_cell,
+                                            (B.table_bits >= 32) ? 0xFFFFFFFFu : ((1u << B.table_bits) - 1u), B.keys,
+                                            B.vals, B.keys_sorted, B.table);
+    }
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // Keys are below 2^table_bits: the passes over the all-zero high digits would be identity permutations.
     uint32_t passes = B.table_bits >= 32 ? 4u : (B.table_bits + 7u) / 8u;
@@ -441,11 +452,10 @@ __device__ __forceinline__ void for_each_candidate(const float4* __restrict__ sr
                 for (int q = 0; q < nseen; ++q) dup |= (seen[q] == h);
                 if (dup) continue;
                 seen[nseen++] = h;
-                // a bucket entry is this pass's when its first position holds the bucket's first key; then its end
-                // was written by the same pass
+                // entries of buckets absent from this build were marked empty by it (hash_keys_kernel)
                 const uint2 t = B.table[h];
                 const uint32_t s = t.x;
-                if (s >= n || B.keys_sorted[s] != h || (s > 0 && B.keys_sorted[s - 1] == h)) continue;
+                if (s >= n) continue;
                 const uint32_t e = min(t.y, n);
                 for (uint32_t q = s; q < e; ++q) {
                     const uint32_t j = B.vals_sorted[q];

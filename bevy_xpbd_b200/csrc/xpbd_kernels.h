@@ -110,8 +110,8 @@ struct CollisionBuffers {
     uint32_t* vals;         // n
     uint32_t* keys_sorted;  // n
     uint32_t* vals_sorted;  // n
-    uint2* table;           // 2^bits bucket -> {first, one past the last} sorted position (validated on use
-                            // through keys_sorted, never cleared)
+    uint2* table;           // 2^bits bucket -> {first, one past the last} sorted position; each build marks the
+                            // previous build's buckets empty (0xFFFFFFFF) before writing its own
     float4* pos_sorted;     // n: the positions in sorted order, gathered by the bucket pass
     uint32_t* pair_count;   // n + 1 (pair extraction only)
     void* sort_scratch;
