@@ -820,6 +820,23 @@ static bool build_cluster_table(xpbd_ctx* ctx, uint32_t cl) {
                 rec[cur[g]++] = r;
                 if (b) ++nbd[g];
             }
+    // Within the boundary and the interior part of every group, deal the records round-robin over the eight
+    // 16-byte bank groups of their first endpoint's slot (local index mod 8), so that the eight lanes of one phase
+    // of a warp's 16-byte shared-memory access mostly hit different banks. A color's records share no particle, so
+    // their order within the color leaves every result bit unchanged.
+    std::vector<uint4> bucket[8];
+    auto spread_banks = [&](size_t lo, size_t hi) {
+        for (auto& v : bucket) v.clear();
+        for (size_t k = lo; k < hi; ++k) bucket[rec[k].x & 7u].push_back(rec[k]);
+        size_t next[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (size_t k = lo; k < hi;)
+            for (int q = 0; q < 8 && k < hi; ++q)
+                if (next[q] < bucket[q].size()) rec[k++] = bucket[q][next[q]++];
+    };
+    for (size_t g = 0; g + 1 < cnt.size(); ++g) {
+        spread_banks(cnt[g], cnt[g] + nbd[g]);
+        spread_banks(cnt[g] + nbd[g], cnt[g + 1]);
+    }
     cudaError_t err = cudaSuccess;
     uint4* drec = dev_alloc<uint4>(ctx, rec.size(), &err);
     uint32_t *doff = nullptr, *dnbd = nullptr;
