@@ -820,19 +820,40 @@ static bool build_cluster_table(xpbd_ctx* ctx, uint32_t cl) {
                 rec[cur[g]++] = r;
                 if (b) ++nbd[g];
             }
-    // Within the boundary and the interior part of every group, deal the records round-robin over the eight
-    // 16-byte bank groups of their first endpoint's slot (local index mod 8), so that the eight lanes of one phase
-    // of a warp's 16-byte shared-memory access mostly hit different banks. A color's records share no particle, so
-    // their order within the color leaves every result bit unchanged.
-    std::vector<uint4> bucket[8];
+    // Within the boundary and the interior part of every group, the records are dealt in runs of eight (the eight
+    // lanes of one phase of a warp's 16-byte shared-memory access) whose endpoints lie in different 16-byte bank
+    // groups (slot mod 8) for both endpoints where the remaining records allow: each run takes, largest first, from
+    // the (first slot mod 8, second slot mod 8) classes whose banks are still free, then fills up with any. A color's
+    // records share no particle, so their order within the color leaves every result bit unchanged.
+    std::vector<uint4> bucket[64];
     auto spread_banks = [&](size_t lo, size_t hi) {
         for (auto& v : bucket) v.clear();
-        for (size_t k = lo; k < hi; ++k) bucket[rec[k].x & 7u].push_back(rec[k]);
-        size_t next[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (size_t k = lo; k < hi;)
-            for (int q = 0; q < 8 && k < hi; ++q)
-                if (next[q] < bucket[q].size()) rec[k++] = bucket[q][next[q]++];
+        for (size_t k = lo; k < hi; ++k) bucket[(rec[k].x & 7u) * 8u + (rec[k].y & 7u)].push_back(rec[k]);
+        size_t next[64] = {};
+        uint32_t byrem[64];
+        for (size_t k = lo; k < hi;) {
+            for (uint32_t q = 0; q < 64; ++q) byrem[q] = q;
+            std::sort(byrem, byrem + 64, [&](uint32_t a, uint32_t b) {
+                return bucket[a].size() - next[a] > bucket[b].size() - next[b];
+            });
+            uint32_t used_i = 0, used_j = 0, taken = 0;
+            for (int pass = 0; pass < 2 && taken < 8 && k < hi; ++pass)
+                for (uint32_t t = 0; t < 64 && taken < 8 && k < hi; ++t) {
+                    const uint32_t q = byrem[t], bi = q >> 3, bj = q & 7u;
+                    if (next[q] == bucket[q].size()) continue;
+                    if (pass == 0 && (((used_i >> bi) & 1u) || ((used_j >> bj) & 1u))) continue;
+                    used_i |= 1u << bi;
+                    used_j |= 1u << bj;
+                    rec[k++] = bucket[q][next[q]++];
+                    ++taken;
+                }
+        }
     };
+    const uint32_t lmask = (1u << shift) - 1u;
+    for (uint4& r : rec) {  // endpoints as the kernel addresses them: rank << shift | shared-memory slot
+        r.x = (r.x & ~lmask) | cluster_slot(r.x & lmask);
+        r.y = (r.y & ~lmask) | cluster_slot(r.y & lmask);
+    }
     for (size_t g = 0; g + 1 < cnt.size(); ++g) {
         spread_banks(cnt[g], cnt[g] + nbd[g]);
         spread_banks(cnt[g] + nbd[g], cnt[g + 1]);

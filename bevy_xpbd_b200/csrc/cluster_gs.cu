@@ -3,7 +3,7 @@
 // Same arithmetic as the grid-wide solver (gs_constraint, xpbd_cpu.rs:349-385; WGSL gs_edges,
 // cloth_sim.wgsl:154-210), different execution. A cluster of CL CTAs (8 portable or 16 non-portable) keeps the whole
 // working state — every particle as float4 {x, y, z, inverse mass} — in distributed shared memory: CTA r owns
-// particles [r*P, (r+1)*P) with P a power of two. A color batch is split by the CTA owning its first endpoint; each
+// particles [r*P, (r+1)*P) with P a power of two, local particle p in slot cluster_slot(p). A color batch is split by the CTA owning its first endpoint; each
 // CTA streams its chunk of constraint records from global memory into shared memory with a TMA bulk copy
 // (cp.async.bulk, completion on an mbarrier), double-buffered so the next color's chunk lands while the current one
 // is solved, and reads/writes both endpoints through shared::cluster loads and stores. Colors are separated by the
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
             const uint32_t i = base + k;
             const float4 x4 = W.x[i];
             if (x4.w <= 0.0f) {
-                xs[k] = x4;
+                xs[cluster_slot(k)] = x4;
                 continue;
             }
             V3 xo = v3(x4);
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
                     p = vadd(p, pull);
                 }
             }
-            xs[k] = make_float4(p.x, p.y, p.z, x4.w);
+            xs[cluster_slot(k)] = make_float4(p.x, p.y, p.z, x4.w);
         }
         pending = true;
         cluster_sync();
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
         if (!last || (flags & kEndFinalize)) {
             for (uint32_t k = tid; k < cnt; k += nthr) {
                 const uint32_t i = base + k;
-                const float4 p4 = xs[k];
+                const float4 p4 = xs[cluster_slot(k)];
                 if (p4.w <= 0.0f) continue;
                 const V3 xo = v3(W.x[i]);
                 V3 vel = v3(W.v[i]);
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, Cluste
             }
             pending = false;
         } else {
-            for (uint32_t k = tid; k < cnt; k += nthr) W.jac[0][base + k] = xs[k];
+            for (uint32_t k = tid; k < cnt; k += nthr) W.jac[0][base + k] = xs[cluster_slot(k)];
         }
         __syncthreads();
     }

@@ -92,8 +92,12 @@ cudaError_t launch_strip_gs(uint32_t cl, uint32_t block, const XpbdWorld& W, con
                             cudaStream_t st);
 
 // ---- cluster Gauss–Seidel (cluster_gs.cu)
+// Shared-memory slot of a CTA's local particle p in the cluster Gauss–Seidel kernel: bits 3-5 of p flip its low
+// three bits, a bijection within every 64 slots that spreads the particles one color touches (often every other one
+// along a row) over the eight 16-byte bank groups.
+__host__ __device__ __forceinline__ uint32_t cluster_slot(uint32_t p) { return p ^ ((p >> 3) & 7u); }
 struct ClusterTable {
-    const uint4* rec;    // constraint records grouped by (color, owning rank)
+    const uint4* rec;    // constraint records grouped by (color, owning rank); endpoints as rank << shift | slot
     const uint32_t* off; // ncolors * CL + 1 offsets into rec
     const uint32_t* nbd; // per (color, rank) group: leading records that touch a boundary particle
     uint32_t shift;      // particles per CTA = 1 << shift
