@@ -785,6 +785,35 @@ static uint32_t ceil_log2(uint32_t v) {
     return s;
 }
 
+// Reorders rec[lo, hi) into runs of eight records (the eight lanes of one phase of a warp's 16-byte shared-memory
+// access) whose two shared-memory slots lie in different 16-byte bank groups, as far as the remaining records allow:
+// `banks(r)` names a record's class (first slot mod 8) · 8 + (second slot mod 8); each run takes, from the classes
+// with the most records left first, those whose banks are still free in the run, then fills up with any.
+template <typename Banks>
+static void deal_bank_runs(std::vector<uint4>& rec, size_t lo, size_t hi, Banks banks) {
+    std::vector<uint4> bucket[64];
+    for (size_t k = lo; k < hi; ++k) bucket[banks(rec[k])].push_back(rec[k]);
+    size_t next[64] = {};
+    uint32_t byrem[64];
+    for (size_t k = lo; k < hi;) {
+        for (uint32_t q = 0; q < 64; ++q) byrem[q] = q;
+        std::sort(byrem, byrem + 64, [&](uint32_t a, uint32_t b) {
+            return bucket[a].size() - next[a] > bucket[b].size() - next[b];
+        });
+        uint32_t used_i = 0, used_j = 0, taken = 0;
+        for (int pass = 0; pass < 2 && taken < 8 && k < hi; ++pass)
+            for (uint32_t t = 0; t < 64 && taken < 8 && k < hi; ++t) {
+                const uint32_t q = byrem[t], bi = q >> 3, bj = q & 7u;
+                if (next[q] == bucket[q].size()) continue;
+                if (pass == 0 && (((used_i >> bi) & 1u) || ((used_j >> bj) & 1u))) continue;
+                used_i |= 1u << bi;
+                used_j |= 1u << bj;
+                rec[k++] = bucket[q][next[q]++];
+                ++taken;
+            }
+    }
+}
+
 // Groups the color-major constraint table by (color, rank owning the first endpoint) for a cluster of `cl` CTAs.
 static bool build_cluster_table(xpbd_ctx* ctx, uint32_t cl) {
     if (ctx->ct_cl == cl) return true;
@@ -820,43 +849,18 @@ static bool build_cluster_table(xpbd_ctx* ctx, uint32_t cl) {
                 rec[cur[g]++] = r;
                 if (b) ++nbd[g];
             }
-    // Within the boundary and the interior part of every group, the records are dealt in runs of eight (the eight
-    // lanes of one phase of a warp's 16-byte shared-memory access) whose endpoints lie in different 16-byte bank
-    // groups (slot mod 8) for both endpoints where the remaining records allow: each run takes, largest first, from
-    // the (first slot mod 8, second slot mod 8) classes whose banks are still free, then fills up with any. A color's
-    // records share no particle, so their order within the color leaves every result bit unchanged.
-    std::vector<uint4> bucket[64];
-    auto spread_banks = [&](size_t lo, size_t hi) {
-        for (auto& v : bucket) v.clear();
-        for (size_t k = lo; k < hi; ++k) bucket[(rec[k].x & 7u) * 8u + (rec[k].y & 7u)].push_back(rec[k]);
-        size_t next[64] = {};
-        uint32_t byrem[64];
-        for (size_t k = lo; k < hi;) {
-            for (uint32_t q = 0; q < 64; ++q) byrem[q] = q;
-            std::sort(byrem, byrem + 64, [&](uint32_t a, uint32_t b) {
-                return bucket[a].size() - next[a] > bucket[b].size() - next[b];
-            });
-            uint32_t used_i = 0, used_j = 0, taken = 0;
-            for (int pass = 0; pass < 2 && taken < 8 && k < hi; ++pass)
-                for (uint32_t t = 0; t < 64 && taken < 8 && k < hi; ++t) {
-                    const uint32_t q = byrem[t], bi = q >> 3, bj = q & 7u;
-                    if (next[q] == bucket[q].size()) continue;
-                    if (pass == 0 && (((used_i >> bi) & 1u) || ((used_j >> bj) & 1u))) continue;
-                    used_i |= 1u << bi;
-                    used_j |= 1u << bj;
-                    rec[k++] = bucket[q][next[q]++];
-                    ++taken;
-                }
-        }
-    };
+    // Within the boundary and the interior part of every group, the records are dealt in bank-spread runs of eight
+    // (deal_bank_runs). A color's records share no particle, so their order within the color leaves every result
+    // bit unchanged.
     const uint32_t lmask = (1u << shift) - 1u;
     for (uint4& r : rec) {  // endpoints as the kernel addresses them: rank << shift | shared-memory slot
         r.x = (r.x & ~lmask) | cluster_slot(r.x & lmask);
         r.y = (r.y & ~lmask) | cluster_slot(r.y & lmask);
     }
+    auto gs_banks = [](const uint4& r) { return (r.x & 7u) * 8u + (r.y & 7u); };
     for (size_t g = 0; g + 1 < cnt.size(); ++g) {
-        spread_banks(cnt[g], cnt[g] + nbd[g]);
-        spread_banks(cnt[g] + nbd[g], cnt[g + 1]);
+        deal_bank_runs(rec, cnt[g], cnt[g] + nbd[g], gs_banks);
+        deal_bank_runs(rec, cnt[g] + nbd[g], cnt[g + 1], gs_banks);
     }
     cudaError_t err = cudaSuccess;
     uint4* drec = dev_alloc<uint4>(ctx, rec.size(), &err);
