@@ -51,6 +51,14 @@ __device__ __forceinline__ V3 vclamp(V3 dx) {
     if (ml > kCap && ml > 0.0f) return vmul(dx, __fdiv_rn(kCap, ml));
     return dx;
 }
+// vclamp of dx = RN(RN(og·w)·dlam) with og = RN(ω·n̂), given bound = RN(RN(ω·w)·dlam): |n̂| <= 1 + 2^-22 (each
+// component a correctly rounded quotient by a length rounded at most 2.5 ulp low), so |dx| <= |bound|·(1 + 2^-20); when
+// |bound| <= 0.27 the rounded |dx|² is below 0.0730 and the reference's clamp (|dx|² > 0.28², xpbd_cpu.rs:28-36)
+// cannot apply, which skips the squared length. NaN or larger bounds take the full test.
+__device__ __forceinline__ V3 vclamp_bounded(V3 dx, float bound) {
+    if (fabsf(bound) <= 0.27f) return dx;
+    return vclamp(dx);
+}
 __device__ __forceinline__ bool vfinite(V3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
 
 __device__ __forceinline__ V3 predict(uint32_t i, V3 sim, V3& vel, const XpbdDevParams& P, const XpbdWorld& W) {
@@ -144,9 +152,9 @@ __device__ __forceinline__ void gs_solve(const uint4 cr, const uint32_t* s_rank_
     if (!PLAIN && wsum < 1e-8f) return;
     const float dlam = __fdiv_rn(PLAIN ? -C : __fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
     const V3 og = {__fmul_rn(P.omega, gv.x), __fmul_rn(P.omega, gv.y), __fmul_rn(P.omega, gv.z)};
-    const V3 dx_i = vclamp(vmul(vmul(og, w_i), dlam));
+    const V3 dx_i = vclamp_bounded(vmul(vmul(og, w_i), dlam), __fmul_rn(__fmul_rn(P.omega, w_i), dlam));
     V3 dxj = vmul(vmul(og, w_j), dlam);
-    const V3 dx_j = vclamp(V3{-dxj.x, -dxj.y, -dxj.z});
+    const V3 dx_j = vclamp_bounded(V3{-dxj.x, -dxj.y, -dxj.z}, __fmul_rn(__fmul_rn(P.omega, w_j), dlam));
     if (w_i > 0.0f) {
         const V3 n = vadd(p_i, dx_i);
         st_local(ai, make_float4(n.x, n.y, n.z, w_i));
