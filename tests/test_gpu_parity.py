@@ -456,3 +456,35 @@ def test_any_number_of_compliance_values_bit_exact(solver, kernel, lam):
         o = oracle_sim(sp, prm, cfg)
         o.substeps(30)
         assert max_abs(plug.positions(k), o.state()[0]) == 0.0, k
+
+
+@pytest.mark.parametrize("solver,kernel,cluster", [
+    (P.SOLVER_JACOBI, 3, 0), (P.SOLVER_JACOBI, 5, 0), (P.SOLVER_JACOBI, 4, 0),
+    (P.SOLVER_GAUSS_SEIDEL, 0, 16), (P.SOLVER_GAUSS_SEIDEL, 0, 1)],
+    ids=["rows", "small_batch", "cloth_resident", "gs_cluster", "gs_grid"])
+def test_tiny_inverse_mass_next_to_a_pin_bit_exact(solver, kernel, cluster):
+    """A free particle of inverse mass 1e-9 beside a pinned corner: the stretch constraint between them has a w sum
+    below 1e-8, which the reference skips (xpbd_cpu.rs:174-178, :369-372). Such an input also turns off the kernels'
+    shortcut that assumes every free particle's inverse mass is at least 1e-8, so the general terms run."""
+    sp = wl.make_sheet(24, 1.0, 1.0, "corners", seed=41)
+    w = sp.inv_mass.copy()
+    corner = int(np.flatnonzero(w == 0)[0])
+    nbrs = np.concatenate([sp.constraint_j[sp.constraint_i == corner], sp.constraint_i[sp.constraint_j == corner]])
+    heavy = int(nbrs[0])
+    w[heavy] = np.float32(1e-9)
+    sp.inv_mass = w
+    pair = ((sp.constraint_i == corner) & (sp.constraint_j == heavy)) | \
+           ((sp.constraint_i == heavy) & (sp.constraint_j == corner))
+    comp = sp.compliance.copy()
+    comp[pair] = 0.0
+    sp.compliance = comp
+    prm = params_for(10, 10, 1.0 if solver == P.SOLVER_JACOBI else 0.9)
+    cfg = _cfg(solver=solver, relaxation=P.RELAX_AVERAGE if solver == P.SOLVER_JACOBI else P.RELAX_OMEGA,
+               solve_substeps=10, jacobi_kernel=kernel, cluster_ctas=cluster)
+    plug = gpu_sim(sp, prm, cfg)
+    plug.step(frames=2)
+    o = oracle_sim(sp, prm, cfg)
+    o.substeps(20)
+    xo, vo = o.state()
+    assert max_abs(plug.positions(), xo) == 0.0
+    assert max_abs(plug.velocities(), vo) == 0.0
