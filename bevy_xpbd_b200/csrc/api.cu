@@ -1330,7 +1330,7 @@ static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
             m_max = std::max(m_max, m);
         }
         const uint32_t block = std::min<uint32_t>(1024, std::max<uint32_t>(32, (std::max(m_max, q) + 31) / 32 * 32));
-        const uint32_t stride = longest | 1u;
+        const uint32_t stride = (longest + 3u) / 4u * 4u + 1u;  // odd; the kernel reads stride - 1 slots per row
         if (m_max > 4096 || longest > 0xFFFFu || !small_batch_supported(cl, block, q, m_max, stride)) {
             cudaGetLastError();
             continue;

@@ -300,12 +300,15 @@ cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTab
 // keeps the pass to one barrier: for a small cloth the pass is latency-bound, not issue-bound.
 // The terms sit in shared memory row by row with an odd stride of float4 slots (row p, slot u at p·stride + u): an
 // incidence writes its slot, and when the row owners read slot u of their rows, eight consecutive owners (one
-// 128-byte phase of a 16-byte load) fall on eight different bank groups. Rows packed back to back (an average of
-// 12 slots apart) put half of them on the same banks, and the owners' reads were the longest part of the pass.
+// 128-byte phase of a 16-byte load) fall on eight different bank groups. The stride is 4·ceil(longest row / 4) + 1;
+// the slots past a row's end are zeroed once and never written, so an owner reads stride − 1 slots without a bound
+// test (a +0 term leaves a sum started at +0 unchanged: such a sum never becomes −0). Each row's 1/degree is
+// computed once per launch, so the degree-averaged update needs only the shared-reciprocal steps.
 // The particles' x and v stay in shared memory for the whole frame (the predict and the velocity update of every
 // substep read and write them there; global memory is read at the start and written at the end).
 size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max, uint32_t stride) {
-    return 4 * (size_t)q * 16 + (size_t)m_max * 16 + (size_t)q * stride * 16 + ((size_t)(q + 1) * 4 + 15) / 16 * 16;
+    return 4 * (size_t)q * 16 + (size_t)m_max * 16 + (size_t)q * stride * 16 + ((size_t)(q + 1) * 4 + 15) / 16 * 16 +
+           ((size_t)q * 4 + 15) / 16 * 16;
 }
 
 template <int CL>
@@ -320,6 +323,7 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
     uint32_t* s_roff =
         reinterpret_cast<uint32_t*>(smem + 4 * (size_t)q * 16 + (size_t)B.m_max * 16 + (size_t)q * B.stride * 16);
     const uint32_t stride = B.stride;
+    float* s_rdeg = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(s_roff) + ((size_t)(q + 1) * 4 + 15) / 16 * 16);
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
     const uint32_t rank = cluster_rank();
     const uint32_t p0 = rank * q;
@@ -328,6 +332,11 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
     const uint32_t m = B.roff[rank * (q + 1) + np];
     for (uint32_t k = tid; k <= np; k += nthr) s_roff[k] = B.roff[rank * (q + 1) + k];
     for (uint32_t k = tid; k < m; k += nthr) s_rec[k] = B.rec[B.rbase[rank] + k];
+    for (uint32_t k = tid; k < q * stride; k += nthr) s_term[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t p = tid; p < np; p += nthr) {
+        const uint32_t deg = B.roff[rank * (q + 1) + p + 1] - B.roff[rank * (q + 1) + p];
+        s_rdeg[p] = deg ? __frcp_rn((float)deg) : 0.f;
+    }
     for (uint32_t p = tid; p < np; p += nthr) {
         s_x[p] = W.x[p0 + p];
         s_v[p] = W.v[p0 + p];
@@ -384,22 +393,22 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
                 if (ps.w <= 0.0f) continue;
                 const uint32_t rs = s_roff[p], re = s_roff[p + 1];
                 float ax = 0.0f, ay = 0.0f, az = 0.0f;
-                // eight terms loaded at once, then added in table order; a slot past the row's end adds +0, which
-                // leaves a sum started at +0 unchanged (such a sum never becomes -0)
+                // four terms loaded at once, then added in table order; the slots past the row's end hold +0
                 const float4* row = s_term + p * stride;
-                for (uint32_t k = 0; k < re - rs; k += 8) {
-                    float4 t[8];
+                for (uint32_t k = 0; k + 1 < stride; k += 4) {
+                    float4 t[4];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) t[u] = k + u < re - rs ? row[k + u] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int u = 0; u < 4; ++u) t[u] = row[k + u];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) {
+                    for (int u = 0; u < 4; ++u) {
                         ax = __fadd_rn(ax, t[u].x);
                         ay = __fadd_rn(ay, t[u].y);
                         az = __fadd_rn(az, t[u].z);
                     }
                 }
                 F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
-                if (P.relaxation == 1u && re > rs) delta = div3(delta, (float)(re - rs));
+                if (P.relaxation == 1u && re > rs)
+                    fpdiv3_rcp(delta.x, delta.y, delta.z, (float)(re - rs), s_rdeg[p], delta.x, delta.y, delta.z);
                 delta = clamp_correction(delta);
                 F3 xn = add3(f3(ps), delta);
                 if (last) {

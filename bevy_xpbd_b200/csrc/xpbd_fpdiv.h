@@ -68,6 +68,21 @@ __device__ __forceinline__ bool coord_outside_fast_range(float c) {
     return ((m < 0x1p-37f) & (m != 0.0f)) | !(m <= 0x1p58f);
 }
 
+// {ax, ay, az} / b with y = RN(1/b) computed beforehand (2^-60 <= b <= 2^60, e.g. a constraint count), each
+// correctly rounded: the shared-reciprocal steps when the numerators pass the range test, else the division.
+__device__ __forceinline__ void fpdiv3_rcp(float ax, float ay, float az, float b, float y, float& qx, float& qy,
+                                           float& qz) {
+    if (fpdiv_num_ok(ax) && fpdiv_num_ok(ay) && fpdiv_num_ok(az)) {
+        qx = fpdiv_step(ax, b, y);
+        qy = fpdiv_step(ay, b, y);
+        qz = fpdiv_step(az, b, y);
+    } else {
+        qx = __fdiv_rn(ax, b);
+        qy = __fdiv_rn(ay, b);
+        qz = __fdiv_rn(az, b);
+    }
+}
+
 // {ax, ay, az} / b, each correctly rounded.
 __device__ __forceinline__ void fpdiv3(float ax, float ay, float az, float b, float& qx, float& qy, float& qz) {
     const float mb = fabsf(b);

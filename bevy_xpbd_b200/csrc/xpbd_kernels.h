@@ -68,7 +68,7 @@ struct SmallBatch {
     const uint32_t* rbase;  // per rank: first incidence of the rank in rec
     uint32_t q;             // particles per rank
     uint32_t m_max;         // largest incidence count of a rank
-    uint32_t stride;        // term slots per row in shared memory: odd, >= the longest row
+    uint32_t stride;        // term slots per row in shared memory: 4·ceil(longest row / 4) + 1 (odd)
 };
 size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max, uint32_t stride);
 bool small_batch_supported(uint32_t cl, uint32_t block, uint32_t q, uint32_t m_max, uint32_t stride);
