@@ -1308,42 +1308,66 @@ static int ensure_small_batch(xpbd_ctx* ctx, bool* usable) {
         const uint32_t q = (N + cl - 1) / cl;
         if (q > 1024) continue;
         std::vector<uint4> rec;
-        std::vector<uint32_t> lroff((size_t)cl * (q + 1), 0), rbase(cl, 0);
+        std::vector<uint32_t> lroff((size_t)cl * (q + 1), 0), rbase(cl + 1, 0);
         uint32_t m_max = 0, longest = 1;
+        // A constraint with both endpoints on one rank is one record (solved once, both endpoint terms written);
+        // a constraint between ranks, or towards a pinned particle (whose row is empty), is a record of the free
+        // endpoint's row alone. The k-th incidence of row p towards o and the k-th of row o towards p are the same
+        // constraint (both rows list their constraints in table order), which pairs up repeated constraints.
+        auto slot_in_row = [&](uint32_t row, uint32_t toward, uint32_t nth) {
+            for (uint32_t t = roff[row]; t < roff[row + 1]; ++t)
+                if ((inc[t].x & XPBD_OTHER_MASK) == toward && nth-- == 0) return t - roff[row];
+            return 0xFFFFFFFFu;
+        };
+        bool paired = true;
         for (uint32_t r = 0; r < cl; ++r) {
             rbase[r] = (uint32_t)rec.size();
             const uint32_t p0 = r * q, p1 = std::min(N, p0 + q);
             for (uint32_t p = p0; p < p1; ++p) {
-                lroff[(size_t)r * (q + 1) + (p - p0)] = (uint32_t)rec.size() - rbase[r];
+                lroff[(size_t)r * (q + 1) + (p - p0)] = roff[p] - roff[p0];
                 for (uint32_t k = roff[p]; k < roff[p + 1]; ++k) {
                     const uint32_t o = inc[k].x & XPBD_OTHER_MASK;
+                    uint32_t slot = 0xFFFFFFFFu;  // the constraint's slot in row o when that row is on this rank
+                    if (o >= p0 && o < p1) {
+                        uint32_t nth = 0;  // occurrence of o among the earlier incidences of row p
+                        for (uint32_t t = roff[p]; t < k; ++t) nth += (inc[t].x & XPBD_OTHER_MASK) == o;
+                        slot = slot_in_row(o, p, nth);
+                    }
+                    if (slot != 0xFFFFFFFFu && o < p) continue;  // recorded from row o
                     const float comp = ctx->wide_palette ? icomp[k]
                                                          : pal[(size_t)cloth_of[p] * XPBD_PALETTE + (inc[k].x >> 28)];
                     uint32_t cb;
                     memcpy(&cb, &comp, 4);
-                    rec.push_back(make_uint4((p - p0) | ((k - roff[p]) << 16), ((o / q) << 16) | (o % q), inc[k].y, cb));
+                    uint32_t code = ((o / q) << 12) | (o % q);
+                    if (slot != 0xFFFFFFFFu) {
+                        if (slot > 0x7FFFu) paired = false;  // (cannot happen: longest <= 0x7FFF is required below)
+                        code |= 0x80000000u | ((slot & 0x7FFFu) << 16);
+                    }
+                    rec.push_back(make_uint4((p - p0) | ((k - roff[p]) << 16), code, inc[k].y, cb));
                 }
                 longest = std::max(longest, roff[p + 1] - roff[p]);
             }
             const uint32_t m = (uint32_t)rec.size() - rbase[r];
-            for (uint32_t p = (p1 > p0 ? p1 - p0 : 0); p <= q; ++p) lroff[(size_t)r * (q + 1) + p] = m;
+            const uint32_t deg_total = p1 > p0 ? roff[p1] - roff[p0] : 0u;
+            for (uint32_t p = (p1 > p0 ? p1 - p0 : 0); p <= q; ++p) lroff[(size_t)r * (q + 1) + p] = deg_total;
             m_max = std::max(m_max, m);
         }
+        rbase[cl] = (uint32_t)rec.size();
         const uint32_t block = std::min<uint32_t>(1024, std::max<uint32_t>(32, (std::max(m_max, q) + 31) / 32 * 32));
         const uint32_t stride = (longest + 3u) / 4u * 4u + 1u;  // odd; the kernel reads stride - 1 slots per row
-        if (m_max > 4096 || longest > 0xFFFFu || !small_batch_supported(cl, block, q, m_max, stride)) {
+        if (!paired || m_max > 4096 || longest > 0x7FFFu || !small_batch_supported(cl, block, q, m_max, stride)) {
             cudaGetLastError();
             continue;
         }
         cudaError_t err = cudaSuccess;
         uint4* d_rec = dev_alloc<uint4>(ctx, std::max<size_t>(1, rec.size()), &err);
         uint32_t* d_roff = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, lroff.size(), &err) : nullptr;
-        uint32_t* d_rbase = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, cl, &err) : nullptr;
+        uint32_t* d_rbase = err == cudaSuccess ? dev_alloc<uint32_t>(ctx, cl + 1, &err) : nullptr;
         if (err != cudaSuccess) return cuda_fail(ctx, err, "small-batch tables");
         if (!rec.empty())
             CK(cudaMemcpyAsync(d_rec, rec.data(), rec.size() * 16, cudaMemcpyHostToDevice, st), "upload");
         CK(cudaMemcpyAsync(d_roff, lroff.data(), lroff.size() * 4, cudaMemcpyHostToDevice, st), "upload");
-        CK(cudaMemcpyAsync(d_rbase, rbase.data(), cl * 4, cudaMemcpyHostToDevice, st), "upload");
+        CK(cudaMemcpyAsync(d_rbase, rbase.data(), (cl + 1) * 4, cudaMemcpyHostToDevice, st), "upload");
         CK(cudaStreamSynchronize(st), "upload sync");
         ctx->small = SmallBatch{d_rec, d_roff, d_rbase, q, m_max, stride};
         ctx->small_cl = cl;

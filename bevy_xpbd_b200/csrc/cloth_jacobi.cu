@@ -292,12 +292,13 @@ cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTab
 // Latency path for a single small cloth (or a few): the whole batch spread over one cluster of CL CTAs, thread per
 // incidence, one cluster barrier per pass. Rank r owns particles [r·q, (r+1)·q) and their neighbour-table rows; its
 // shared memory holds the two Jacobi position buffers of those particles (the reference's jac_a / jac_b ping-pong),
-// the rows' incidence records and one correction term per incidence. A pass: every thread evaluates one incidence —
-// the reference's Δλ recomputed from the row's endpoint, times n̂·w_self (jacobi_edges + jacobi_gather,
-// xpbd_cpu.rs:139-226) — reading the other endpoint from its owner's shared memory; then each particle sums its row's
-// terms in table order and writes its new position into the other buffer; a cluster barrier ends the pass. The
-// constraint is evaluated from both ends (as the thread-per-particle kernel does), which costs instructions but
-// keeps the pass to one barrier: for a small cloth the pass is latency-bound, not issue-bound.
+// the rank's constraint records and one correction term per incidence. A pass: every thread evaluates one record —
+// the reference's Δλ, times n̂·w of an endpoint (jacobi_edges + jacobi_gather, xpbd_cpu.rs:139-226) — reading the
+// other endpoint from its owner's shared memory; a constraint whose endpoints are both on this rank is solved once and
+// writes both endpoints' terms, one that joins two ranks is evaluated on each side for its own endpoint; then each
+// particle sums its row's terms in table order and writes its new position into the other buffer; a cluster barrier
+// ends the pass. Evaluating the cross-rank constraints twice keeps the pass to one barrier: for a small cloth the
+// pass is latency-bound.
 // The terms sit in shared memory row by row with an odd stride of float4 slots (row p, slot u at p·stride + u): an
 // incidence writes its slot, and when the row owners read slot u of their rows, eight consecutive owners (one
 // 128-byte phase of a 16-byte load) fall on eight different bank groups. The stride is 4·ceil(longest row / 4) + 1;
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
     const uint32_t p0 = rank * q;
     const uint32_t np = p0 < W.n ? min(q, W.n - p0) : 0u;
     const XpbdDevParams P = *W.params;
-    const uint32_t m = B.roff[rank * (q + 1) + np];
+    const uint32_t m = B.rbase[rank + 1] - B.rbase[rank];  // records of this rank
     for (uint32_t k = tid; k <= np; k += nthr) s_roff[k] = B.roff[rank * (q + 1) + k];
     for (uint32_t k = tid; k < m; k += nthr) s_rec[k] = B.rec[B.rbase[rank] + k];
     for (uint32_t k = tid; k < q * stride; k += nthr) s_term[k] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -367,14 +368,14 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
                 const uint4 r = s_rec[k];
                 const uint32_t self = r.x & 0xFFFFu;  // {slot in the row << 16 | self local}
                 const float4 ps = ld_local(src + self * 16u);
-                const uint32_t ro = r.y >> 16;  // {rank << 16 | local}
-                const uint32_t ao = src + (r.y & 0xFFFFu) * 16u;
+                const uint32_t ro = (r.y >> 12) & 0xFu;  // {local | rank << 12 | slot << 16 | both << 31}
+                const uint32_t ao = src + (r.y & 0xFFFu) * 16u;
                 const float4 po = ro == rank ? ld_local(ao) : ld_dsmem(map_rank(ao, ro));
                 const F3 gv = sub3(f3(ps), f3(po));
                 const float len = len3(gv);
                 const float alpha_t = __fmul_rn(__uint_as_float(r.w), P.inv_dt_sq);
                 const float wsum = __fadd_rn(__fadd_rn(ps.w, po.w), alpha_t);
-                float4 t = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                float4 t = make_float4(0.0f, 0.0f, 0.0f, 0.0f), to = t;
                 if (!(len < 1e-8f) && !(wsum < 1e-8f)) {
                     F3 n;
                     if (!fpdiv3_by_length_fast(gv.x, gv.y, gv.z, len, n.x, n.y, n.z))
@@ -383,8 +384,13 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
                     const float dlam = __fdiv_rn(__fsub_rn(-C, __fmul_rn(alpha_t, 0.0f)), wsum);
                     t = make_float4(__fmul_rn(__fmul_rn(n.x, ps.w), dlam), __fmul_rn(__fmul_rn(n.y, ps.w), dlam),
                                     __fmul_rn(__fmul_rn(n.z, ps.w), dlam), 0.0f);
+                    // the other endpoint's term as its own row evaluates it: the difference, n̂ and so every
+                    // product negate exactly, |d|, C, the w sum (two terms commute) and Δλ are the same
+                    to = make_float4(__fmul_rn(__fmul_rn(-n.x, po.w), dlam), __fmul_rn(__fmul_rn(-n.y, po.w), dlam),
+                                     __fmul_rn(__fmul_rn(-n.z, po.w), dlam), 0.0f);
                 }
                 s_term[self * stride + (r.x >> 16)] = t;
+                if (r.y >> 31) s_term[(r.y & 0xFFFu) * stride + ((r.y >> 16) & 0x7FFFu)] = to;
             }
             __syncthreads();
             const bool last = it + 1 == I;

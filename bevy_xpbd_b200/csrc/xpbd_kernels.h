@@ -62,12 +62,13 @@ cudaError_t cloth_kernel_prepare();  // opt-in shared-memory sizes (host, once)
 bool cloth_class_launchable(int cls);  // a cluster of the class fits on this device
 // A whole small batch in one cluster of cl (8 or 16) CTAs, thread per incidence (cloth_jacobi.cu).
 struct SmallBatch {
-    const uint4* rec;       // per incidence, rank-major: {self local | slot in its row << 16, other endpoint
-                            // (rank << 16 | local), rest, comp}
-    const uint32_t* roff;   // per rank: q + 1 local row starts into the rank's incidences
-    const uint32_t* rbase;  // per rank: first incidence of the rank in rec
+    const uint4* rec;       // rank-major records {self local | slot in its row << 16, other endpoint (local | rank << 12
+                            // | slot in the other's row << 16 | 1 << 31 when that row is on the same rank: one record
+                            // for both endpoints), rest, comp}
+    const uint32_t* roff;   // per rank: q + 1 local row starts (prefix sums of the row lengths)
+    const uint32_t* rbase;  // cl + 1: first record of each rank in rec
     uint32_t q;             // particles per rank
-    uint32_t m_max;         // largest incidence count of a rank
+    uint32_t m_max;         // largest record count of a rank
     uint32_t stride;        // term slots per row in shared memory: 4·ceil(longest row / 4) + 1 (odd)
 };
 size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max, uint32_t stride);
