@@ -303,13 +303,12 @@ cudaError_t launch_cloth_jacobi(int cls, const XpbdWorld& W, const ClothSolveTab
 // incidence writes its slot, and when the row owners read slot u of their rows, eight consecutive owners (one
 // 128-byte phase of a 16-byte load) fall on eight different bank groups. The stride is 4·ceil(longest row / 4) + 1;
 // the slots past a row's end are zeroed once and never written, so an owner reads stride − 1 slots without a bound
-// test (a +0 term leaves a sum started at +0 unchanged: such a sum never becomes −0). Each row's 1/degree is
-// computed once per launch, so the degree-averaged update needs only the shared-reciprocal steps.
+// test (a +0 term leaves a sum started at +0 unchanged: such a sum never becomes −0). Each row owner computes its
+// 1/degree once per launch, so the degree-averaged update needs only the shared-reciprocal steps.
 // The particles' x and v stay in shared memory for the whole frame (the predict and the velocity update of every
 // substep read and write them there; global memory is read at the start and written at the end).
 size_t small_batch_smem_bytes(uint32_t q, uint32_t m_max, uint32_t stride) {
-    return 4 * (size_t)q * 16 + (size_t)m_max * 16 + (size_t)q * stride * 16 + ((size_t)(q + 1) * 4 + 15) / 16 * 16 +
-           ((size_t)q * 4 + 15) / 16 * 16;
+    return 4 * (size_t)q * 16 + (size_t)m_max * 16 + (size_t)q * stride * 16;
 }
 
 template <int CL>
@@ -321,23 +320,19 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
     float4* s_v = s_x + q;
     uint4* s_rec = reinterpret_cast<uint4*>(smem + 4 * (size_t)q * 16);
     float4* s_term = reinterpret_cast<float4*>(smem + 4 * (size_t)q * 16 + (size_t)B.m_max * 16);
-    uint32_t* s_roff =
-        reinterpret_cast<uint32_t*>(smem + 4 * (size_t)q * 16 + (size_t)B.m_max * 16 + (size_t)q * B.stride * 16);
     const uint32_t stride = B.stride;
-    float* s_rdeg = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(s_roff) + ((size_t)(q + 1) * 4 + 15) / 16 * 16);
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
     const uint32_t rank = cluster_rank();
     const uint32_t p0 = rank * q;
     const uint32_t np = p0 < W.n ? min(q, W.n - p0) : 0u;
     const XpbdDevParams P = *W.params;
     const uint32_t m = B.rbase[rank + 1] - B.rbase[rank];  // records of this rank
-    for (uint32_t k = tid; k <= np; k += nthr) s_roff[k] = B.roff[rank * (q + 1) + k];
+    // the launch has at least q threads (small_batch_supported): thread p owns row p for the whole frame, and keeps
+    // its degree and its reciprocal in registers
+    const uint32_t my_deg = tid < np ? B.roff[rank * (q + 1) + tid + 1] - B.roff[rank * (q + 1) + tid] : 0u;
+    const float my_rdeg = my_deg ? __frcp_rn((float)my_deg) : 0.f;
     for (uint32_t k = tid; k < m; k += nthr) s_rec[k] = B.rec[B.rbase[rank] + k];
     for (uint32_t k = tid; k < q * stride; k += nthr) s_term[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (uint32_t p = tid; p < np; p += nthr) {
-        const uint32_t deg = B.roff[rank * (q + 1) + p + 1] - B.roff[rank * (q + 1) + p];
-        s_rdeg[p] = deg ? __frcp_rn((float)deg) : 0.f;
-    }
     for (uint32_t p = tid; p < np; p += nthr) {
         s_x[p] = W.x[p0 + p];
         s_v[p] = W.v[p0 + p];
@@ -394,10 +389,9 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
             }
             __syncthreads();
             const bool last = it + 1 == I;
-            for (uint32_t p = tid; p < np; p += nthr) {
-                const float4 ps = s_pos0[b * q + p];
-                if (ps.w <= 0.0f) continue;
-                const uint32_t rs = s_roff[p], re = s_roff[p + 1];
+            const uint32_t p = tid;
+            const float4 ps = p < np ? s_pos0[b * q + p] : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ps.w > 0.0f) {  // a free particle of this rank (pinned ones keep their position)
                 float ax = 0.0f, ay = 0.0f, az = 0.0f;
                 // four terms loaded at once, then added in table order; the slots past the row's end hold +0
                 const float4* row = s_term + p * stride;
@@ -413,8 +407,8 @@ __global__ void __launch_bounds__(1024, 1) jacobi_small_batch_kernel(XpbdWorld W
                     }
                 }
                 F3 delta = {__fmul_rn(P.omega, ax), __fmul_rn(P.omega, ay), __fmul_rn(P.omega, az)};
-                if (P.relaxation == 1u && re > rs)
-                    fpdiv3_rcp(delta.x, delta.y, delta.z, (float)(re - rs), s_rdeg[p], delta.x, delta.y, delta.z);
+                if (P.relaxation == 1u && my_deg > 0u)
+                    fpdiv3_rcp(delta.x, delta.y, delta.z, (float)my_deg, my_rdeg, delta.x, delta.y, delta.z);
                 delta = clamp_correction(delta);
                 F3 xn = add3(f3(ps), delta);
                 if (last) {
