@@ -839,7 +839,7 @@ static bool build_cluster_table(xpbd_ctx* ctx, uint32_t cl) {
     std::vector<uint4> rec(ctx->W.e);
     std::vector<uint32_t> nbd((size_t)ncol * cl, 0);
     std::vector<uint32_t> cur(cnt.begin(), cnt.end() - 1);
-    for (int pass = 0; pass < 2; ++pass)  // boundary records, then interior records, each in table order
+    for (int pass = 0; pass < 2; ++pass)  // boundary records, then interior records (bank-dealt below)
         for (uint32_t c = 0; c < ncol; ++c)
             for (uint32_t e = ctx->color_off_host[c]; e < ctx->color_off_host[c + 1]; ++e) {
                 const uint4 r = ctx->con_host[e];

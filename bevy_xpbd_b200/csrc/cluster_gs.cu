@@ -170,7 +170,8 @@ __device__ __forceinline__ void gs_solve(const uint4 cr, const uint32_t* s_rank_
 
 }  // namespace
 
-// T.off[(c * CL + r)] .. T.off[c * CL + r + 1]: records of color c owned by rank r (uint4 {i, j, rest, comp}).
+// T.off[(c * CL + r)] .. T.off[c * CL + r + 1]: records of color c owned by rank r (uint4 {i, j, rest, comp}, the
+// endpoints as rank << shift | shared-memory slot).
 template <int CL>
 __global__ void __launch_bounds__(1024, 1) gs_cluster_kernel(XpbdWorld W, ClusterTable T, uint32_t flags,
                                                               uint32_t substeps, uint32_t pend) {
