@@ -3,10 +3,10 @@
 // Same arithmetic as the grid-wide solver (gs_constraint, xpbd_cpu.rs:349-385; WGSL gs_edges,
 // cloth_sim.wgsl:154-210), different execution. A cluster of CL CTAs (8 portable or 16 non-portable) keeps the whole
 // working state — every particle as float4 {x, y, z, inverse mass} — in distributed shared memory: CTA r owns
-// particles [r*P, (r+1)*P) with P a power of two, local particle p in slot cluster_slot(p). A color batch is split by the CTA owning its first endpoint; each
-// CTA streams its chunk of constraint records from global memory into shared memory with a TMA bulk copy
-// (cp.async.bulk, completion on an mbarrier), double-buffered so the next color's chunk lands while the current one
-// is solved, and reads/writes both endpoints through shared::cluster loads and stores. Colors are separated by the
+// particles [r*P, (r+1)*P) with P a power of two, local particle p in slot cluster_slot(p). A color batch is split by
+// the CTA owning its first endpoint; each CTA streams its chunk of constraint records from global memory into shared
+// memory with a TMA bulk copy (cp.async.bulk, completion on an mbarrier), double-buffered so the next color's chunk
+// lands while the current one is solved, and reads/writes both endpoints through shared::cluster loads and stores. Colors are separated by the
 // hardware cluster barrier (barrier.cluster arrive.release / wait.acquire) instead of a global-memory grid barrier.
 // Every CTA executes the same barrier sequence (no early exit); mbarrier waits are bounded and report
 // XPBD_DEV_BARRIER_TIMEOUT if exceeded.
@@ -52,9 +52,9 @@ __device__ __forceinline__ V3 vclamp(V3 dx) {
     return dx;
 }
 // vclamp of dx = RN(RN(og·w)·dlam) with og = RN(ω·n̂), given bound = RN(RN(ω·w)·dlam): |n̂| <= 1 + 2^-22 (each
-// component a correctly rounded quotient by a length rounded at most 2.5 ulp low), so |dx| <= |bound|·(1 + 2^-20); when
-// |bound| <= 0.27 the rounded |dx|² is below 0.0730 and the reference's clamp (|dx|² > 0.28², xpbd_cpu.rs:28-36)
-// cannot apply, which skips the squared length. NaN or larger bounds take the full test.
+// component a correctly rounded quotient by a length rounded at most 2.5 ulp low), so |dx| <= |bound|·(1 + 2^-20);
+// when |bound| <= 0.27 the rounded |dx|² is below 0.0730 and the reference's clamp (|dx|² > 0.28²,
+// xpbd_cpu.rs:28-36) cannot apply, which skips the squared length. NaN or larger bounds take the full test.
 __device__ __forceinline__ V3 vclamp_bounded(V3 dx, float bound) {
     if (fabsf(bound) <= 0.27f) return dx;
     return vclamp(dx);
