@@ -6,8 +6,9 @@
 // particles [r*P, (r+1)*P) with P a power of two, local particle p in slot cluster_slot(p). A color batch is split by
 // the CTA owning its first endpoint; each CTA streams its chunk of constraint records from global memory into shared
 // memory with a TMA bulk copy (cp.async.bulk, completion on an mbarrier), double-buffered so the next color's chunk
-// lands while the current one is solved, and reads/writes both endpoints through shared::cluster loads and stores. Colors are separated by the
-// hardware cluster barrier (barrier.cluster arrive.release / wait.acquire) instead of a global-memory grid barrier.
+// lands while the current one is solved, and reads/writes both endpoints through shared::cluster loads and stores.
+// Colors are separated by the hardware cluster barrier (barrier.cluster arrive.release / wait.acquire) instead of a
+// global-memory grid barrier.
 // Every CTA executes the same barrier sequence (no early exit); mbarrier waits are bounded and report
 // XPBD_DEV_BARRIER_TIMEOUT if exceeded.
 #include <cuda_runtime.h>
