@@ -111,7 +111,7 @@ typedef struct xpbd_solver_opts {
                                          pass; λ cleared per pass, no collision, every cloth at most 65,536
                                          particles with particle-disjoint color batches — otherwise 3 runs),
                                          5 small batch (at most 8,192 particles: the whole batch in one cluster,
-                                         thread per incidence; the default up to 4,096 particles) */
+                                         thread per constraint record; the default up to 4,096 particles) */
     float tolerance;                  /* > 0 (or warm_start != 0): convergence solve — Jacobi, λ kept per substep,
                                          iterate until max |C + α̃λ|/rest <= tolerance, at most inner_iterations */
     uint32_t gs_strips;               /* Gauss–Seidel over several clusters: 0 / 1 none (xpbd_autotune may pick
