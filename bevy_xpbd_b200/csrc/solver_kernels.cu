@@ -38,6 +38,13 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+// atomicAdd with release semantics at GPU scope: the block's writes (ordered before it by __syncthreads) become
+// visible to any thread that acquires the counter value it produces.
+__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -46,7 +53,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // All blocks of the grid meet here. One atomic per block: block 0 adds 2^31 - (expected - 1), every other block adds
 // 1, so the counter's top bit flips exactly when the last block arrives and the low bits return to their value;
-// each block then polls for the flip. Waits are bounded: after `barrier_timeout_ns` (or once another block reported
+// each block then polls for the flip. Each add is a release and the poll an acquire: the adds form one release
+// sequence on the counter, so the load that sees the flip orders every block's earlier writes before the block's
+// later reads (no separate fences). Waits are bounded: after `barrier_timeout_ns` (or once another block reported
 // an error) the waiting block records XPBD_DEV_BARRIER_TIMEOUT and every caller returns false, so a launch that
 // cannot complete (blocks not co-resident, forced test timeout) ends instead of hanging.
 __device__ bool grid_barrier(const XpbdWorld& W, const XpbdDevParams& P) {
@@ -57,8 +66,7 @@ __device__ bool grid_barrier(const XpbdWorld& W, const XpbdDevParams& P) {
         XpbdGridSync* gs = W.sync;
         const unsigned expected = gridDim.x + gs->expected_extra;
         const unsigned inc = (blockIdx.x == 0) ? (0x80000000u - (expected - 1u)) : 1u;
-        __threadfence();
-        const unsigned old = atomicAdd(&gs->count, inc);
+        const unsigned old = atom_add_release(&gs->count, inc);
         unsigned spins = 0;
         unsigned long long t0 = 0;
         while (((old ^ ld_acquire(&gs->count)) & 0x80000000u) == 0u) {
@@ -74,8 +82,7 @@ __device__ bool grid_barrier(const XpbdWorld& W, const XpbdDevParams& P) {
                 if (spins > (1u << 16)) __nanosleep(128);
             }
         }
-        __threadfence();
-        s_ok = ok;
+        s_ok = ok;  // the acquiring load that saw the flip orders the other blocks' writes before what follows
     }
     __syncthreads();
     return s_ok != 0;
