@@ -171,3 +171,38 @@ def test_small_batch_kernel_odd_pass_counts_and_grab(iters):
     o = oracle_sim(sp, prm, cfg)
     o.substeps(23)
     assert max_abs(plug.positions(), o.state()[0]) == 0.0
+
+
+@pytest.mark.parametrize("kernel", [5, 3], ids=["small_batch", "thread_rows"])
+def test_repeated_constraints_between_one_pair_bit_exact(kernel):
+    """Several constraints joining the same two particles (different rest lengths and compliances, in both endpoint
+    orders), inside one CTA of the small-batch cluster and across two: each row lists them in table order, and the
+    small-batch kernel pairs the k-th of one row with the k-th of the other when it solves a constraint once for both
+    endpoints."""
+    sp = wl.make_sheet(24, 1.0, 1.0, "corners", seed=71)
+    rng = np.random.default_rng(72)
+    pick = rng.choice(sp.num_constraints, 40, replace=False)
+    extra_i = sp.constraint_i[pick].copy()
+    extra_j = sp.constraint_j[pick].copy()
+    flip = rng.random(40) < 0.5
+    extra_i[flip], extra_j[flip] = sp.constraint_j[pick][flip], sp.constraint_i[pick][flip]
+    # a particle of row 1 joined twice more to one of row 20 (different CTAs of the cluster)
+    extra_i = np.concatenate([extra_i, np.array([30, 485], np.uint32)])
+    extra_j = np.concatenate([extra_j, np.array([485, 30], np.uint32)])
+    n_extra = len(extra_i)
+    sp.constraint_i = np.concatenate([sp.constraint_i, extra_i]).astype(np.uint32)
+    sp.constraint_j = np.concatenate([sp.constraint_j, extra_j]).astype(np.uint32)
+    rest = np.linalg.norm(sp.rest_positions[extra_i].astype(np.float64) - sp.rest_positions[extra_j], axis=1)
+    sp.rest_len = np.concatenate([sp.rest_len, (rest * rng.uniform(0.9, 1.1, n_extra)).astype(np.float32)])
+    sp.compliance = np.concatenate([sp.compliance, (10.0 ** rng.uniform(-8, -4, n_extra)).astype(np.float32)])
+    sp.constraint_type = np.concatenate([sp.constraint_type, np.zeros(n_extra, np.uint32)])
+    prm = params_for(10, 10, 1.0)
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10, jacobi_kernel=kernel)
+    plug = gpu_sim(sp, prm, cfg)
+    assert plug.stats()["solver_kernel"] == (SMALL if kernel == 5 else ROWS)
+    plug.step(frames=2)
+    o = oracle_sim(sp, prm, cfg)
+    o.substeps(20)
+    xo, vo = o.state()
+    assert max_abs(plug.positions(), xo) == 0.0
+    assert max_abs(plug.velocities(), vo) == 0.0
