@@ -2518,7 +2518,7 @@ extern "C" int xpbd_mlp_train(xpbd_ctx* ctx, uint32_t steps, uint32_t batch, flo
         ++ctx->adam_step;
         CK(cudaMemsetAsync(ctx->d_grads, 0, XPBD_MLP_PARAMS * 4, st), "memset");
         CK(launch_mlp_train(ctx->d_mlp, ctx->d_feat, ctx->d_target, ctx->d_idx + (size_t)s * batch, batch,
-                            ctx->d_grads, ctx->d_loss + s, st), "train");
+                            ctx->d_grads, ctx->d_loss + s, ctx->W.status, st), "train");
         const float bc1 = 1.f - powf(b1, (float)ctx->adam_step), bc2 = 1.f - powf(b2, (float)ctx->adam_step);
         CK(launch_mlp_adam(ctx->d_master, ctx->d_m1, ctx->d_m2, ctx->d_grads, 1.0f, lr, b1, b2, eps, bc1, bc2, ctx->d_mlp,
                            st), "adam");
@@ -2555,7 +2555,8 @@ extern "C" int xpbd_mlp_minibatch_gradients(xpbd_ctx* ctx, uint32_t batch, uint6
     CK(cudaMemcpyAsync(ctx->d_idx, idx.data(), (size_t)batch * 4, cudaMemcpyHostToDevice, st), "indices");
     CK(cudaMemsetAsync(grads, 0, XPBD_MLP_PARAMS * 4, st), "memset");
     CK(cudaMemsetAsync(loss, 0, 4, st), "memset");
-    CK(launch_mlp_train(ctx->d_mlp, ctx->d_feat, ctx->d_target, ctx->d_idx, batch, grads, loss, st), "train");
+    CK(launch_mlp_train(ctx->d_mlp, ctx->d_feat, ctx->d_target, ctx->d_idx, batch, grads, loss, ctx->W.status, st),
+       "train");
     ctx->stats.kernel_launches += 1;
     return XPBD_OK;
 }
@@ -2610,7 +2611,7 @@ extern "C" int xpbd_mlp_gradients(xpbd_ctx* ctx, const float* features, const fl
     if (e == cudaSuccess) e = cudaMemcpyAsync(di, idx.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, XPBD_MLP_PARAMS * 4, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(dl, 0, 4, st);
-    if (e == cudaSuccess) e = launch_mlp_train(ctx->d_mlp, df, dt, di, n, dg, dl, st);
+    if (e == cudaSuccess) e = launch_mlp_train(ctx->d_mlp, df, dt, di, n, dg, dl, ctx->W.status, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(grads, dg, XPBD_MLP_PARAMS * 4, cudaMemcpyDeviceToHost, st);
     float lsum = 0.f;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&lsum, dl, 4, cudaMemcpyDeviceToHost, st);

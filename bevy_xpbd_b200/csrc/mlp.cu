@@ -1,11 +1,10 @@
 // Learned λ warm start: a 9→64→64→1 MLP (SiLU) predicting each constraint's initial Lagrange multiplier from local
 // features. Inference, training (forward, backward) and the Adam update are hand-written kernels; every matrix
-// product runs on the tensor cores as BF16 tiles with FP32 accumulation. Inference uses the sm_100a tcgen05 path:
-// 128-constraint tiles, tcgen05.mma issued by one thread on shared-memory operands, accumulators in tensor memory
-// read back with tcgen05.ld. Training uses warp-level mma.sync.m16n8k16 tiles of 16 constraints (its backward keeps
-// the forward's accumulators in registers): layer 1 = [16 x 16(9 padded)] x [16 x 64], layer 2 = [16 x 64] x
-// [64 x 64] (the layer-1 accumulator registers are repacked as layer-2 A fragments), layer 3 a 64-wide dot product;
-// weight gradients are the same tiles with the batch as the reduction dimension. No reference counterpart: the reference has no learned component.
+// product runs on the sm_100a tcgen05 tensor cores as BF16 operands with FP32 accumulation: 128-row tiles,
+// tcgen05.mma issued by one thread on shared-memory operands, accumulators in tensor memory read back with
+// tcgen05.ld — inference: layer 1 [128 x 16 (9 padded)] x [16 x 64], layer 2 [128 x 64] x [64 x 64], layer 3 a
+// 64-wide dot product; training: the same forward, then dh1 = dz2 · W2 and the weight gradients with the batch rows
+// as the reduction dimension. No reference counterpart: the reference has no learned component.
 //
 // Features of constraint e = (i, j) at the predicted positions of the substep, before any iteration:
 //   f0 strain (|xi-xj| - rest)/rest      f1 previous-substep λ · (wi + wj + α̃)/rest
@@ -26,27 +25,7 @@
 namespace xpbd {
 
 namespace {
-constexpr unsigned kAll = 0xFFFFFFFFu;
-
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<uint32_t*>(&v);
-}
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-__device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
-__device__ __forceinline__ uint32_t two(const __nv_bfloat16 a, const __nv_bfloat16 b) {
-    __nv_bfloat162 v;
-    v.x = a;
-    v.y = b;
-    return *reinterpret_cast<uint32_t*>(&v);
-}
-__device__ __forceinline__ void mma16816(float* d, const uint32_t a[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
 // σ(z) = (1 + tanh(z/2)) / 2 on the hardware tanh approximation (tanh.approx.f32, one instruction): its error (about
 // 2^-11 relative to tanh) stays well below the BF16 rounding of the activations that follows, and it replaces an
 // exponential and an IEEE division in the SiLU that every hidden unit of every constraint evaluates.
@@ -60,99 +39,6 @@ __device__ __forceinline__ float silu(float z) { return z * sigm(z); }
 __device__ __forceinline__ float dsilu(float z) {
     const float s = sigm(z);
     return s * (1.0f + z * (1.0f - s));
-}
-
-// Shared-memory copy of the working weights (bf16, [out][in]) and biases.
-struct SmemMlp {
-    __nv_bfloat16 w1[64 * 16];
-    __nv_bfloat16 w2[64 * 64];
-    __nv_bfloat16 w3[64];
-    float b1[64], b2[64], b3;
-    float fmean[XPBD_MLP_IN], fstd[XPBD_MLP_IN], tmean, tstd;
-};
-__device__ void load_mlp(SmemMlp& s, const XpbdMlp& m) {
-    const __nv_bfloat16* w1 = reinterpret_cast<const __nv_bfloat16*>(m.w1);
-    const __nv_bfloat16* w2 = reinterpret_cast<const __nv_bfloat16*>(m.w2);
-    const __nv_bfloat16* w3 = reinterpret_cast<const __nv_bfloat16*>(m.w3);
-    for (uint32_t k = threadIdx.x; k < 64 * 16; k += blockDim.x) s.w1[k] = w1[k];
-    for (uint32_t k = threadIdx.x; k < 64 * 64; k += blockDim.x) s.w2[k] = w2[k];
-    for (uint32_t k = threadIdx.x; k < 64; k += blockDim.x) {
-        s.w3[k] = w3[k];
-        s.b1[k] = m.b1[k];
-        s.b2[k] = m.b2[k];
-    }
-    if (threadIdx.x < XPBD_MLP_IN) {
-        s.fmean[threadIdx.x] = m.fmean[threadIdx.x];
-        s.fstd[threadIdx.x] = m.fstd[threadIdx.x];
-    }
-    if (threadIdx.x == 0) {
-        s.b3 = m.b3;
-        s.tmean = m.tmean;
-        s.tstd = m.tstd;
-    }
-}
-
-// Forward of one 16-row tile. xs: the tile's standardised features [16][16] (bf16). Keeps z1, z2 (pre-activations,
-// fp32, accumulator layout: per n-tile j the thread holds rows g and g+8, cols 8j+2t, 8j+2t+1) and the bf16 h2 values
-// for the backward pass; returns y for rows g (y_lo) and g+8 (y_hi) in every lane of the row's quad.
-struct TileFwd {
-    float z1[8][4], z2[8][4];
-    float y_lo, y_hi;
-};
-__device__ __forceinline__ void tile_forward(const SmemMlp& S, const __nv_bfloat16* xs, TileFwd& F) {
-    const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
-    uint32_t a[4];
-    a[0] = ld_pair(xs + g * 16 + 2 * t);
-    a[1] = ld_pair(xs + (g + 8) * 16 + 2 * t);
-    a[2] = ld_pair(xs + g * 16 + 8 + 2 * t);
-    a[3] = ld_pair(xs + (g + 8) * 16 + 8 + 2 * t);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        float* d = F.z1[j];
-        d[0] = d[1] = d[2] = d[3] = 0.0f;
-        const __nv_bfloat16* wb = S.w1 + (8 * j + g) * 16;
-        mma16816(d, a, ld_pair(wb + 2 * t), ld_pair(wb + 8 + 2 * t));
-        const float b0 = S.b1[8 * j + 2 * t], b1 = S.b1[8 * j + 2 * t + 1];
-        d[0] += b0;
-        d[1] += b1;
-        d[2] += b0;
-        d[3] += b1;
-    }
-    uint32_t a2[4][4];
-#pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
-        const float* c0 = F.z1[2 * kk];
-        const float* c1 = F.z1[2 * kk + 1];
-        a2[kk][0] = pack_bf16(silu(c0[0]), silu(c0[1]));
-        a2[kk][1] = pack_bf16(silu(c0[2]), silu(c0[3]));
-        a2[kk][2] = pack_bf16(silu(c1[0]), silu(c1[1]));
-        a2[kk][3] = pack_bf16(silu(c1[2]), silu(c1[3]));
-    }
-    float ylo = 0.0f, yhi = 0.0f;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        float* d = F.z2[j];
-        d[0] = d[1] = d[2] = d[3] = 0.0f;
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            const __nv_bfloat16* wb = S.w2 + (8 * j + g) * 64 + 16 * kk;
-            mma16816(d, a2[kk], ld_pair(wb + 2 * t), ld_pair(wb + 8 + 2 * t));
-        }
-        const int c = 8 * j + 2 * t;
-        d[0] += S.b2[c];
-        d[1] += S.b2[c + 1];
-        d[2] += S.b2[c];
-        d[3] += S.b2[c + 1];
-        const float w3a = __bfloat162float(S.w3[c]), w3b = __bfloat162float(S.w3[c + 1]);
-        ylo += bf16r(silu(d[0])) * w3a + bf16r(silu(d[1])) * w3b;
-        yhi += bf16r(silu(d[2])) * w3a + bf16r(silu(d[3])) * w3b;
-    }
-    ylo += __shfl_xor_sync(kAll, ylo, 1);
-    ylo += __shfl_xor_sync(kAll, ylo, 2);
-    yhi += __shfl_xor_sync(kAll, yhi, 1);
-    yhi += __shfl_xor_sync(kAll, yhi, 2);
-    F.y_lo = ylo + S.b3;
-    F.y_hi = yhi + S.b3;
 }
 
 // Raw (unstandardised) features of packed constraint e at the predicted positions jac[0]; `scale` = rest/(wi+wj+α̃).
@@ -181,15 +67,6 @@ __device__ __forceinline__ void raw_features(const XpbdWorld& W, const XpbdDevPa
     f[7] = ty == 2 ? 1.0f : 0.0f;
     f[8] = (pi.w <= 0.0f || pj.w <= 0.0f) ? 1.0f : 0.0f;
     scale = denom > 0.0f ? rest / denom : 0.0f;
-}
-__device__ __forceinline__ void store_row(const SmemMlp& S, const float f[9], __nv_bfloat16* row) {
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        const float v = k < 5 ? (f[k] - S.fmean[k]) / S.fstd[k] : f[k];
-        row[k] = __float2bfloat16_rn(v);
-    }
-#pragma unroll
-    for (int k = 9; k < 16; ++k) row[k] = __float2bfloat16_rn(0.0f);
 }
 }  // namespace
 
@@ -405,196 +282,6 @@ __global__ void mlp_collect_targets_kernel(XpbdWorld W, uint32_t stride, uint32_
 
 // ---- training: gradients of mean((y - (t - f1 - tmean)/tstd)^2) over the rows listed in idx
 // grads layout (fp32): w1[64][9], b1[64], w2[64][64], b2[64], w3[64], b3; loss (sum of squares) at loss[0].
-struct TrainSmem {
-    SmemMlp S;
-    __nv_bfloat16 xs[4][16 * 16];
-    __nv_bfloat16 hs[4][16 * 64];   // h1 (bf16)
-    __nv_bfloat16 ds[4][16 * 64];   // dz2, then dz1 (bf16)
-    float gw1[64 * 16], gw2[64 * 64], gb1[64], gb2[64], gw3[64], gb3;
-};
-
-__global__ void __launch_bounds__(128) mlp_train_kernel(const XpbdMlp* __restrict__ mlp, const float* __restrict__ feat,
-                                                        const float* __restrict__ target,
-                                                        const uint32_t* __restrict__ idx, uint32_t nrows,
-                                                        float* __restrict__ grads, float* __restrict__ loss) {
-    extern __shared__ __align__(16) unsigned char t_smem[];
-    TrainSmem& T = *reinterpret_cast<TrainSmem*>(t_smem);
-    load_mlp(T.S, *mlp);
-    for (uint32_t k = threadIdx.x; k < 64 * 16; k += blockDim.x) T.gw1[k] = 0.0f;
-    for (uint32_t k = threadIdx.x; k < 64 * 64; k += blockDim.x) T.gw2[k] = 0.0f;
-    for (uint32_t k = threadIdx.x; k < 64; k += blockDim.x) T.gb1[k] = T.gb2[k] = T.gw3[k] = 0.0f;
-    if (threadIdx.x == 0) T.gb3 = 0.0f;
-    __syncthreads();
-    const SmemMlp& S = T.S;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3u;
-    __nv_bfloat16* xs = T.xs[warp];
-    __nv_bfloat16* hs = T.hs[warp];
-    __nv_bfloat16* ds = T.ds[warp];
-    const float inv_b = 1.0f / (float)nrows;
-    float loss_acc = 0.0f;
-    for (uint32_t tile = blockIdx.x * 4 + warp; tile < (nrows + 15) / 16; tile += gridDim.x * 4) {
-        float tgt = 0.0f;
-        bool valid = false;
-        if (lane < 16) {
-            const uint32_t r = tile * 16 + lane;
-            float f[9];
-            valid = r < nrows;
-            const uint32_t s = valid ? idx[r] : 0u;
-            for (int k = 0; k < 9; ++k) f[k] = valid ? feat[(size_t)s * 9 + k] : 0.0f;
-            store_row(S, f, xs + lane * 16);
-            tgt = valid ? (target[s] - f[1] - S.tmean) / S.tstd : 0.0f;
-        }
-        __syncwarp();
-        TileFwd F;
-        tile_forward(S, xs, F);
-        // dy per row (rows g and g+8), zero for padding rows
-        const float t_lo = __shfl_sync(kAll, tgt, g), t_hi = __shfl_sync(kAll, tgt, g + 8);
-        const bool v_lo = tile * 16 + g < nrows, v_hi = tile * 16 + g + 8 < nrows;
-        const float e_lo = v_lo ? F.y_lo - t_lo : 0.0f, e_hi = v_hi ? F.y_hi - t_hi : 0.0f;
-        if (t == 0) loss_acc += e_lo * e_lo + e_hi * e_hi;
-        const float dy_lo = 2.0f * e_lo * inv_b, dy_hi = 2.0f * e_hi * inv_b;
-        // layer 3 and dz2 (fp32), h1 / dz2 staged as bf16 for the tensor-core weight gradients
-        float dz2[8][4];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int c = 8 * j + 2 * t;
-            const float* z = F.z2[j];
-            const float h00 = bf16r(silu(z[0])), h01 = bf16r(silu(z[1])), h10 = bf16r(silu(z[2])),
-                        h11 = bf16r(silu(z[3]));
-            float gw3a = dy_lo * h00 + dy_hi * h10, gw3b = dy_lo * h01 + dy_hi * h11;
-            const float w3a = __bfloat162float(S.w3[c]), w3b = __bfloat162float(S.w3[c + 1]);
-            dz2[j][0] = dy_lo * w3a * dsilu(z[0]);
-            dz2[j][1] = dy_lo * w3b * dsilu(z[1]);
-            dz2[j][2] = dy_hi * w3a * dsilu(z[2]);
-            dz2[j][3] = dy_hi * w3b * dsilu(z[3]);
-            float gb2a = dz2[j][0] + dz2[j][2], gb2b = dz2[j][1] + dz2[j][3];
-#pragma unroll
-            for (int o = 4; o < 32; o <<= 1) {
-                gw3a += __shfl_xor_sync(kAll, gw3a, o);
-                gw3b += __shfl_xor_sync(kAll, gw3b, o);
-                gb2a += __shfl_xor_sync(kAll, gb2a, o);
-                gb2b += __shfl_xor_sync(kAll, gb2b, o);
-            }
-            if (g == 0) {
-                atomicAdd(&T.gw3[c], gw3a);
-                atomicAdd(&T.gw3[c + 1], gw3b);
-                atomicAdd(&T.gb2[c], gb2a);
-                atomicAdd(&T.gb2[c + 1], gb2b);
-            }
-            const float* z1 = F.z1[j];
-            hs[g * 64 + c] = __float2bfloat16_rn(silu(z1[0]));
-            hs[g * 64 + c + 1] = __float2bfloat16_rn(silu(z1[1]));
-            hs[(g + 8) * 64 + c] = __float2bfloat16_rn(silu(z1[2]));
-            hs[(g + 8) * 64 + c + 1] = __float2bfloat16_rn(silu(z1[3]));
-            ds[g * 64 + c] = __float2bfloat16_rn(dz2[j][0]);
-            ds[g * 64 + c + 1] = __float2bfloat16_rn(dz2[j][1]);
-            ds[(g + 8) * 64 + c] = __float2bfloat16_rn(dz2[j][2]);
-            ds[(g + 8) * 64 + c + 1] = __float2bfloat16_rn(dz2[j][3]);
-        }
-        if (t == 0) atomicAdd(&T.gb3, dy_lo + dy_hi);
-        __syncwarp();
-        // dW2[out][in] = sum_rows dz2[row][out] * h1[row][in]   (M = out, N = in, K = 16 rows)
-#pragma unroll 1
-        for (int mt = 0; mt < 4; ++mt) {
-            uint32_t a[4];
-            const int mo = 16 * mt;
-            a[0] = two(ds[(2 * t) * 64 + mo + g], ds[(2 * t + 1) * 64 + mo + g]);
-            a[1] = two(ds[(2 * t) * 64 + mo + g + 8], ds[(2 * t + 1) * 64 + mo + g + 8]);
-            a[2] = two(ds[(2 * t + 8) * 64 + mo + g], ds[(2 * t + 9) * 64 + mo + g]);
-            a[3] = two(ds[(2 * t + 8) * 64 + mo + g + 8], ds[(2 * t + 9) * 64 + mo + g + 8]);
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                float d[4] = {0.f, 0.f, 0.f, 0.f};
-                const int ni = 8 * nt + g;
-                mma16816(d, a, two(hs[(2 * t) * 64 + ni], hs[(2 * t + 1) * 64 + ni]),
-                         two(hs[(2 * t + 8) * 64 + ni], hs[(2 * t + 9) * 64 + ni]));
-                const int col = 8 * nt + 2 * t;
-                atomicAdd(&T.gw2[(mo + g) * 64 + col], d[0]);
-                atomicAdd(&T.gw2[(mo + g) * 64 + col + 1], d[1]);
-                atomicAdd(&T.gw2[(mo + g + 8) * 64 + col], d[2]);
-                atomicAdd(&T.gw2[(mo + g + 8) * 64 + col + 1], d[3]);
-            }
-        }
-        // dh1 = dz2 x W2 (M = 16 rows, K = 64 out, N = 64 in); A from the dz2 registers, B[k=out][n=in] = W2[out][in]
-        uint32_t ad[4][4];
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            ad[kk][0] = pack_bf16(dz2[2 * kk][0], dz2[2 * kk][1]);
-            ad[kk][1] = pack_bf16(dz2[2 * kk][2], dz2[2 * kk][3]);
-            ad[kk][2] = pack_bf16(dz2[2 * kk + 1][0], dz2[2 * kk + 1][1]);
-            ad[kk][3] = pack_bf16(dz2[2 * kk + 1][2], dz2[2 * kk + 1][3]);
-        }
-        __syncwarp();
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            float d[4] = {0.f, 0.f, 0.f, 0.f};
-            const int ni = 8 * nt + g;
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-                const int ko = 16 * kk;
-                mma16816(d, ad[kk], two(S.w2[(ko + 2 * t) * 64 + ni], S.w2[(ko + 2 * t + 1) * 64 + ni]),
-                         two(S.w2[(ko + 2 * t + 8) * 64 + ni], S.w2[(ko + 2 * t + 9) * 64 + ni]));
-            }
-            // dz1 = dh1 * silu'(z1), staged (bf16) over dz2's buffer; db1
-            const int c = 8 * nt + 2 * t;
-            const float* z1 = F.z1[nt];
-            const float q0 = d[0] * dsilu(z1[0]), q1 = d[1] * dsilu(z1[1]), q2 = d[2] * dsilu(z1[2]),
-                        q3 = d[3] * dsilu(z1[3]);
-            float gb1a = q0 + q2, gb1b = q1 + q3;
-#pragma unroll
-            for (int o = 4; o < 32; o <<= 1) {
-                gb1a += __shfl_xor_sync(kAll, gb1a, o);
-                gb1b += __shfl_xor_sync(kAll, gb1b, o);
-            }
-            if (g == 0) {
-                atomicAdd(&T.gb1[c], gb1a);
-                atomicAdd(&T.gb1[c + 1], gb1b);
-            }
-            __syncwarp();
-            ds[g * 64 + c] = __float2bfloat16_rn(q0);
-            ds[g * 64 + c + 1] = __float2bfloat16_rn(q1);
-            ds[(g + 8) * 64 + c] = __float2bfloat16_rn(q2);
-            ds[(g + 8) * 64 + c + 1] = __float2bfloat16_rn(q3);
-        }
-        __syncwarp();
-        // dW1[out][in] = sum_rows dz1[row][out] * x[row][in]   (M = out, N = in (16), K = 16 rows)
-#pragma unroll 1
-        for (int mt = 0; mt < 4; ++mt) {
-            uint32_t a[4];
-            const int mo = 16 * mt;
-            a[0] = two(ds[(2 * t) * 64 + mo + g], ds[(2 * t + 1) * 64 + mo + g]);
-            a[1] = two(ds[(2 * t) * 64 + mo + g + 8], ds[(2 * t + 1) * 64 + mo + g + 8]);
-            a[2] = two(ds[(2 * t + 8) * 64 + mo + g], ds[(2 * t + 9) * 64 + mo + g]);
-            a[3] = two(ds[(2 * t + 8) * 64 + mo + g + 8], ds[(2 * t + 9) * 64 + mo + g + 8]);
-#pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                float d[4] = {0.f, 0.f, 0.f, 0.f};
-                const int ni = 8 * nt + g;
-                mma16816(d, a, two(xs[(2 * t) * 16 + ni], xs[(2 * t + 1) * 16 + ni]),
-                         two(xs[(2 * t + 8) * 16 + ni], xs[(2 * t + 9) * 16 + ni]));
-                const int col = 8 * nt + 2 * t;
-                atomicAdd(&T.gw1[(mo + g) * 16 + col], d[0]);
-                atomicAdd(&T.gw1[(mo + g) * 16 + col + 1], d[1]);
-                atomicAdd(&T.gw1[(mo + g + 8) * 16 + col], d[2]);
-                atomicAdd(&T.gw1[(mo + g + 8) * 16 + col + 1], d[3]);
-            }
-        }
-        __syncwarp();
-    }
-    for (int o = 16; o > 0; o >>= 1) loss_acc += __shfl_xor_sync(kAll, loss_acc, o);
-    if (lane == 0) atomicAdd(loss, loss_acc);
-    __syncthreads();
-    // block partial gradients → global (fp32)
-    for (uint32_t k = threadIdx.x; k < 64 * 9; k += blockDim.x) atomicAdd(&grads[k], T.gw1[(k / 9) * 16 + k % 9]);
-    for (uint32_t k = threadIdx.x; k < 64; k += blockDim.x) {
-        atomicAdd(&grads[576 + k], T.gb1[k]);
-        atomicAdd(&grads[576 + 64 + 4096 + k], T.gb2[k]);
-        atomicAdd(&grads[576 + 64 + 4096 + 64 + k], T.gw3[k]);
-    }
-    for (uint32_t k = threadIdx.x; k < 64 * 64; k += blockDim.x) atomicAdd(&grads[576 + 64 + k], T.gw2[k]);
-    if (threadIdx.x == 0) atomicAdd(&grads[XPBD_MLP_PARAMS - 1], T.gb3);
-}
-
 // ---- Adam on the fp32 master parameters, then the bf16 working copy
 __global__ void mlp_adam_kernel(float* __restrict__ master, float* __restrict__ m1, float* __restrict__ m2,
                                 const float* __restrict__ grads, float gscale, float lr, float beta1, float beta2,
@@ -626,6 +313,242 @@ __global__ void mlp_publish_kernel(const float* __restrict__ master, XpbdMlp* __
     }
     for (uint32_t k = threadIdx.x; k < 64 * 64; k += blockDim.x) w2[k] = __float2bfloat16_rn(master[576 + 64 + k]);
     if (threadIdx.x == 0) mlp->b3 = master[XPBD_MLP_PARAMS - 1];
+}
+
+// ---- training step on the tcgen05 tensor cores: 128 sampled rows per tile, one thread per row.
+// Forward as in inference (layer 1: M 128, N 64, K 16; layer 2: K 64), then the backward products, each one
+// tcgen05.mma chain on K-major BF16 operands in shared memory with FP32 accumulation in tensor memory:
+//   dh1 = dz2 · W2         M 128 rows,  N 64 (in),  K 64 (out)   A = dz2, B = W2ᵀ (a transposed copy)
+//   dW2 += dz2ᵀ · h1       M 128 (out, rows 64..127 zero), N 64 (in), K 128 rows   A = dz2ᵀ, B = h1ᵀ
+//   dW1 += dz1ᵀ · x        M 128 (out, rows 64..127 zero), N 16 (features), K 128 rows   A = dz1ᵀ, B = xᵀ
+// The epilogues write each row's values both row-major and transposed (the transposed copies are the K-major
+// operands of the weight gradients), and dW2 and dW1 accumulate in tensor memory over all the CTA's tiles. The
+// rounding points are those of the forward and of the reference-checked gradient: BF16 operands (x, h1, dz2, dz1,
+// weights), FP32 accumulation, FP32 bias and output-layer gradients. Tensor-memory columns: z1 0-63, z2 then dh1
+// 64-127, dW2 128-191, dW1 192-207.
+struct TcTrainSmem {
+    __nv_bfloat16 w1[64 * 16];     // B of layer 1
+    __nv_bfloat16 w2[64 * 64];     // B of layer 2: [out][in]
+    __nv_bfloat16 w2t[64 * 64];    // B of dh1: [in][out]
+    __nv_bfloat16 a1[128 * 16];    // x  (A of layer 1)
+    __nv_bfloat16 xt[16 * 128];    // xᵀ (B of dW1)
+    __nv_bfloat16 a2[128 * 64];    // h1 (A of layer 2)
+    __nv_bfloat16 h1t[64 * 128];   // h1ᵀ (B of dW2)
+    __nv_bfloat16 dz2[128 * 64];   // dz2 (A of dh1)
+    __nv_bfloat16 dz2t[128 * 128]; // dz2ᵀ, rows 64..127 zero (A of dW2)
+    __nv_bfloat16 dz1t[128 * 128]; // dz1ᵀ, rows 64..127 zero (A of dW1)
+    float b1[64], b2[64], w3[64];
+    float fmean[XPBD_MLP_IN], fstd[XPBD_MLP_IN], b3, tmean, tstd;
+    float gb1[64], gb2[64], gw3[64], gb3, loss;
+    uint64_t bar;
+    uint32_t tmem;
+};
+constexpr size_t kTcTrainSmemBytes = (sizeof(TcTrainSmem) + 1023) / 1024 * 1024;
+constexpr uint32_t kTcTrainCols = 256;
+
+// Sum over the warp's 32 rows of v; lane 0 adds it to *dst (shared memory).
+__device__ __forceinline__ void warp_sum_to(float v, float* dst) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31u) == 0) atomicAdd(dst, v);
+}
+
+// One MMA chain issued by thread 0 and completed through the mbarrier: D (+)= A·Bᵀ over `ksteps` K-steps of 16;
+// `ra` / `rb` are the rows (M / N) of the K-major A and B tiles.
+__device__ __forceinline__ void tc_chain(uint32_t tmem_d, const __nv_bfloat16* a, uint32_t ra, const __nv_bfloat16* b,
+                                         uint32_t rb, uint32_t ksteps, uint32_t idesc, bool accumulate) {
+    for (uint32_t q = 0; q < ksteps; ++q)
+        tc_mma(tmem_d, tc_desc(tc_smem_addr(a) + q * 2u * ra * 16u, ra * 16u, 128u),
+               tc_desc(tc_smem_addr(b) + q * 2u * rb * 16u, rb * 16u, 128u), idesc, accumulate || q > 0);
+}
+
+__global__ void __launch_bounds__(128) mlp_train_tc_kernel(const XpbdMlp* __restrict__ mlp,
+                                                           const float* __restrict__ feat,
+                                                           const float* __restrict__ target,
+                                                           const uint32_t* __restrict__ idx, uint32_t nrows,
+                                                           float* __restrict__ grads, float* __restrict__ loss,
+                                                           int* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char tt_raw[];
+    TcTrainSmem& T = *reinterpret_cast<TcTrainSmem*>(tt_raw);
+    const uint32_t r = threadIdx.x, warp = r >> 5;
+    const __nv_bfloat16* w1 = reinterpret_cast<const __nv_bfloat16*>(mlp->w1);
+    const __nv_bfloat16* w2 = reinterpret_cast<const __nv_bfloat16*>(mlp->w2);
+    for (uint32_t q = r; q < 64 * 16; q += blockDim.x) T.w1[tc_index(q >> 4, q & 15u, 64)] = w1[q];
+    for (uint32_t q = r; q < 64 * 64; q += blockDim.x) {
+        const uint32_t o = q >> 6, i = q & 63u;
+        T.w2[tc_index(o, i, 64)] = w2[q];
+        T.w2t[tc_index(i, o, 64)] = w2[q];
+    }
+    for (uint32_t k = r; k < 64; k += blockDim.x) {
+        T.b1[k] = mlp->b1[k];
+        T.b2[k] = mlp->b2[k];
+        T.w3[k] = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(mlp->w3)[k]);
+        T.gb1[k] = T.gb2[k] = T.gw3[k] = 0.0f;
+    }
+    if (r < XPBD_MLP_IN) {
+        T.fmean[r] = mlp->fmean[r];
+        T.fstd[r] = mlp->fstd[r];
+    }
+    // rows 64..127 of the padded transposed operands stay zero
+    for (uint32_t q = r; q < 64 * 128; q += blockDim.x) {
+        T.dz2t[tc_index(64 + (q >> 7), q & 127u, 128)] = __float2bfloat16_rn(0.0f);
+        T.dz1t[tc_index(64 + (q >> 7), q & 127u, 128)] = __float2bfloat16_rn(0.0f);
+    }
+    if (r == 0) {
+        T.b3 = mlp->b3;
+        T.tmean = mlp->tmean;
+        T.tstd = mlp->tstd;
+        T.gb3 = 0.0f;
+        T.loss = 0.0f;
+        tc_mbar_init(&T.bar, 1);
+    }
+    if (warp == 0) tc_alloc(&T.tmem, kTcTrainCols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t lane_base = T.tmem + ((32u * warp) << 16);
+    constexpr uint32_t kId64 = tc_idesc_bf16(128, 64), kId16 = tc_idesc_bf16(128, 16);
+    const float inv_b = 1.0f / (float)nrows;
+    const uint32_t tiles = (nrows + 127) / 128;
+    uint32_t phase = 0;
+    bool ok = true, first = true;
+    float loss_acc = 0.0f;
+    auto issue_and_wait = [&](auto&& issue) {
+        tc_fence_proxy();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (r == 0) {
+            issue();
+            tc_commit(&T.bar);
+        }
+        ok = tc_mbar_wait(&T.bar, phase) && ok;
+        phase ^= 1u;
+        tc_fence_after();
+    };
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t row = tile * 128 + r;
+        const bool valid = row < nrows;
+        const uint32_t sample = valid ? idx[row] : 0u;
+        float f[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) f[k] = valid ? feat[(size_t)sample * 9 + k] : 0.0f;
+        const float tgt = valid ? (target[sample] - f[1] - T.tmean) / T.tstd : 0.0f;
+        {  // x: standardised features, BF16, row-major (layer 1) and transposed (dW1)
+            __nv_bfloat16 xv[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                xv[k] = __float2bfloat16_rn(k < 5 ? (f[k] - T.fmean[k]) / T.fstd[k] : (k < 9 ? f[k] : 0.0f));
+                T.xt[tc_index(k, r, 16)] = xv[k];
+            }
+            *reinterpret_cast<uint4*>(T.a1 + tc_index(r, 0, 128)) = *reinterpret_cast<const uint4*>(xv);
+            *reinterpret_cast<uint4*>(T.a1 + tc_index(r, 8, 128)) = *reinterpret_cast<const uint4*>(xv + 8);
+        }
+        issue_and_wait([&] { tc_chain(T.tmem, T.a1, 128, T.w1, 64, 1, kId64, false); });
+        // h1 = BF16(SiLU(z1 + b1)): row-major (layer 2) and transposed (dW2)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float z[16];
+            tc_ld16(lane_base + 16u * c, z);
+            __nv_bfloat16 h[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                h[k] = __float2bfloat16_rn(silu(z[k] + T.b1[16 * c + k]));
+                T.h1t[tc_index(16 * c + k, r, 64)] = h[k];
+            }
+            *reinterpret_cast<uint4*>(T.a2 + tc_index(r, 16 * c, 128)) = *reinterpret_cast<const uint4*>(h);
+            *reinterpret_cast<uint4*>(T.a2 + tc_index(r, 16 * c + 8, 128)) = *reinterpret_cast<const uint4*>(h + 8);
+        }
+        issue_and_wait([&] { tc_chain(T.tmem + 64u, T.a2, 128, T.w2, 64, 4, kId64, false); });
+        // output, error and dz2 = dy · w3 · SiLU'(z2 + b2) (two reads of z2: dy needs the whole row first)
+        float y = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float z[16];
+            tc_ld16(lane_base + 64u + 16u * c, z);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) y += bf16r(silu(z[k] + T.b2[16 * c + k])) * T.w3[16 * c + k];
+        }
+        y += T.b3;
+        const float e = valid ? y - tgt : 0.0f;
+        loss_acc += e * e;
+        const float dy = 2.0f * e * inv_b;
+        warp_sum_to(dy, &T.gb3);
+#pragma unroll 1
+        for (int c = 0; c < 4; ++c) {
+            float z[16];
+            tc_ld16(lane_base + 64u + 16u * c, z);
+            __nv_bfloat16 d[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const int u = 16 * c + k;
+                const float zz = z[k] + T.b2[u];
+                warp_sum_to(dy * bf16r(silu(zz)), &T.gw3[u]);
+                const float dz = dy * T.w3[u] * dsilu(zz);
+                warp_sum_to(dz, &T.gb2[u]);
+                d[k] = __float2bfloat16_rn(dz);
+                T.dz2t[tc_index(u, r, 128)] = d[k];
+            }
+            *reinterpret_cast<uint4*>(T.dz2 + tc_index(r, 16 * c, 128)) = *reinterpret_cast<const uint4*>(d);
+            *reinterpret_cast<uint4*>(T.dz2 + tc_index(r, 16 * c + 8, 128)) = *reinterpret_cast<const uint4*>(d + 8);
+        }
+        const bool acc = !first;
+        issue_and_wait([&] {
+            tc_chain(T.tmem + 64u, T.dz2, 128, T.w2t, 64, 4, kId64, false);  // dh1 (over z2's columns)
+            tc_chain(T.tmem + 128u, T.dz2t, 128, T.h1t, 64, 8, kId64, acc);  // dW2
+        });
+        // dz1 = dh1 · SiLU'(z1 + b1), transposed (dW1)
+#pragma unroll 1
+        for (int c = 0; c < 4; ++c) {
+            float dh[16], z[16];
+            tc_ld16(lane_base + 64u + 16u * c, dh);
+            tc_ld16(lane_base + 16u * c, z);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                const int u = 16 * c + k;
+                const float dz = dh[k] * dsilu(z[k] + T.b1[u]);
+                warp_sum_to(dz, &T.gb1[u]);
+                T.dz1t[tc_index(u, r, 128)] = __float2bfloat16_rn(dz);
+            }
+        }
+        issue_and_wait([&] { tc_chain(T.tmem + 192u, T.dz1t, 128, T.xt, 16, 8, kId16, acc); });
+        first = false;
+        // every MMA of this tile has completed: the next tile may overwrite the operands
+        tc_fence_before();
+        if (!__syncthreads_and(ok)) break;
+        tc_fence_after();
+    }
+    warp_sum_to(loss_acc, &T.loss);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (!first && warp < 2) {  // dW2 and dW1: tensor-memory lanes 0..63 are the 64 hidden units
+#pragma unroll 1
+        for (int c = 0; c < 4; ++c) {
+            float g[16];
+            tc_ld16(lane_base + 128u + 16u * c, g);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) atomicAdd(&grads[576 + 64 + r * 64 + 16 * c + k], g[k]);
+        }
+        float g1[16];
+        tc_ld16(lane_base + 192u, g1);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) atomicAdd(&grads[r * 9 + k], g1[k]);
+    }
+    for (uint32_t k = r; k < 64; k += blockDim.x) {
+        atomicAdd(&grads[576 + k], T.gb1[k]);
+        atomicAdd(&grads[576 + 64 + 4096 + k], T.gb2[k]);
+        atomicAdd(&grads[576 + 64 + 4096 + 64 + k], T.gw3[k]);
+    }
+    if (r == 0) {
+        atomicAdd(&grads[XPBD_MLP_PARAMS - 1], T.gb3);
+        atomicAdd(loss, T.loss);
+        if (!ok) atomicOr(status, XPBD_DEV_BARRIER_TIMEOUT);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tc_dealloc(T.tmem, kTcTrainCols);
 }
 
 // ---------------------------------------------------------------------------------------------- launchers
@@ -672,15 +595,16 @@ cudaError_t launch_mlp_collect_targets(const XpbdWorld& W, uint32_t stride, uint
     return cudaGetLastError();
 }
 cudaError_t launch_mlp_train(const XpbdMlp* mlp, const float* feat, const float* target, const uint32_t* idx,
-                             uint32_t nrows, float* grads, float* loss, cudaStream_t st) {
+                             uint32_t nrows, float* grads, float* loss, int* status, cudaStream_t st) {
     // the attribute is per device; setting it again is cheap and idempotent
-    const size_t smem = sizeof(TrainSmem);
-    if (cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    static_assert(sizeof(TcTrainSmem) <= kTcTrainSmemBytes, "tensor-core training shared memory");
+    if (cudaFuncSetAttribute(mlp_train_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kTcTrainSmemBytes) != cudaSuccess)
         return cudaErrorInvalidValue;
-    uint32_t grid = ((nrows + 15) / 16 + 3) / 4;
-    if (grid > 296) grid = 296;
+    uint32_t grid = (nrows + 127) / 128;  // one 128-row tile per CTA; one CTA per SM (shared memory)
+    if (grid > 148) grid = 148;
     if (grid == 0) grid = 1;
-    mlp_train_kernel<<<grid, 128, smem, st>>>(mlp, feat, target, idx, nrows, grads, loss);
+    mlp_train_tc_kernel<<<grid, 128, kTcTrainSmemBytes, st>>>(mlp, feat, target, idx, nrows, grads, loss, status);
     return cudaGetLastError();
 }
 cudaError_t launch_mlp_adam(float* master, float* m1, float* m2, const float* grads, float gscale, float lr,

@@ -32,8 +32,10 @@ cudaError_t launch_mlp_collect_features(const XpbdWorld& W, uint32_t stride, uin
                                         float* scale, uint32_t base, uint32_t cap, cudaStream_t st);
 cudaError_t launch_mlp_collect_targets(const XpbdWorld& W, uint32_t stride, uint32_t offset, const float* scale,
                                        float* target, uint32_t base, uint32_t cap, cudaStream_t st);
+// One training step's gradient (tcgen05 tensor cores): grads += d loss / d params over rows idx[0..nrows), loss += Σ e²;
+// a tensor-core wait that gives up sets XPBD_DEV_BARRIER_TIMEOUT in *status.
 cudaError_t launch_mlp_train(const XpbdMlp* mlp, const float* feat, const float* target, const uint32_t* idx,
-                             uint32_t nrows, float* grads, float* loss, cudaStream_t st);
+                             uint32_t nrows, float* grads, float* loss, int* status, cudaStream_t st);
 cudaError_t launch_mlp_adam(float* master, float* m1, float* m2, const float* grads, float gscale, float lr,
                             float beta1, float beta2, float eps, float bc1, float bc2, XpbdMlp* mlp, cudaStream_t st);
 cudaError_t launch_mlp_publish(const float* master, XpbdMlp* mlp, cudaStream_t st);
