@@ -319,8 +319,9 @@ __global__ void mlp_publish_kernel(const float* __restrict__ master, XpbdMlp* __
 // Forward as in inference (layer 1: M 128, N 64, K 16; layer 2: K 64), then the backward products, each one
 // tcgen05.mma chain on K-major BF16 operands in shared memory with FP32 accumulation in tensor memory:
 //   dh1 = dz2 · W2         M 128 rows,  N 64 (in),  K 64 (out)   A = dz2, B = W2ᵀ (a transposed copy)
-//   dW2 += dz2ᵀ · h1       M 128 (out, rows 64..127 zero), N 64 (in), K 128 rows   A = dz2ᵀ, B = h1ᵀ
-//   dW1 += dz1ᵀ · x        M 128 (out, rows 64..127 zero), N 16 (features), K 128 rows   A = dz1ᵀ, B = xᵀ
+//   dW2 += dz2ᵀ · h1       M 128 (out in rows 0..63), N 64 (in), K 128 rows   A = dz2ᵀ, B = h1ᵀ
+//   dW1 += dz1ᵀ · x        M 128 (out in rows 0..63), N 16 (features), K 128 rows   A = dz1ᵀ, B = xᵀ
+// (rows 64..127 of those A operands are never written: they only produce accumulator rows 64..127, never read)
 // The epilogues write each row's values both row-major and transposed (the transposed copies are the K-major
 // operands of the weight gradients), and dW2 and dW1 accumulate in tensor memory over all the CTA's tiles. The
 // rounding points are those of the forward and of the reference-checked gradient: BF16 operands (x, h1, dz2, dz1,
@@ -335,8 +336,8 @@ struct TcTrainSmem {
     __nv_bfloat16 a2[128 * 64];    // h1 (A of layer 2)
     __nv_bfloat16 h1t[64 * 128];   // h1ᵀ (B of dW2)
     __nv_bfloat16 dz2[128 * 64];   // dz2 (A of dh1)
-    __nv_bfloat16 dz2t[128 * 128]; // dz2ᵀ, rows 64..127 zero (A of dW2)
-    __nv_bfloat16 dz1t[128 * 128]; // dz1ᵀ, rows 64..127 zero (A of dW1)
+    __nv_bfloat16 dz2t[128 * 128]; // dz2ᵀ (A of dW2; rows 64..127 unwritten: they only reach D rows never read)
+    __nv_bfloat16 dz1t[128 * 128]; // dz1ᵀ (A of dW1; the same)
     float b1[64], b2[64], w3[64];
     float fmean[XPBD_MLP_IN], fstd[XPBD_MLP_IN], b3, tmean, tstd;
     float gb1[64], gb2[64], gw3[64], gb3, loss;
@@ -388,11 +389,6 @@ __global__ void __launch_bounds__(128) mlp_train_tc_kernel(const XpbdMlp* __rest
     if (r < XPBD_MLP_IN) {
         T.fmean[r] = mlp->fmean[r];
         T.fstd[r] = mlp->fstd[r];
-    }
-    // rows 64..127 of the padded transposed operands stay zero
-    for (uint32_t q = r; q < 64 * 128; q += blockDim.x) {
-        T.dz2t[tc_index(64 + (q >> 7), q & 127u, 128)] = __float2bfloat16_rn(0.0f);
-        T.dz1t[tc_index(64 + (q >> 7), q & 127u, 128)] = __float2bfloat16_rn(0.0f);
     }
     if (r == 0) {
         T.b3 = mlp->b3;
