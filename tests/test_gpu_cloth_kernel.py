@@ -206,3 +206,21 @@ def test_repeated_constraints_between_one_pair_bit_exact(kernel):
     xo, vo = o.state()
     assert max_abs(plug.positions(), xo) == 0.0
     assert max_abs(plug.velocities(), vo) == 0.0
+
+
+def test_small_batch_kernel_eight_cta_cluster_bit_exact():
+    """The small-batch kernel on a cluster of 8 CTAs (128 particles per CTA here): the same records, pairing of
+    rank-internal constraints and row updates as on 16, with a different split of the sheet."""
+    sp = wl.make_sheet(32, 1.0, 1.0, "corners", seed=73)
+    prm = params_for(10, 10, 1.0, drag=0.2)
+    cfg = _cfg(solver=P.SOLVER_JACOBI, relaxation=P.RELAX_AVERAGE, solve_substeps=10, jacobi_kernel=5,
+               cluster_ctas=8)
+    plug = gpu_sim(sp, prm, cfg)
+    st = plug.stats()
+    assert st["solver_kernel"] == SMALL and st["cluster_ctas"] == 8
+    plug.step(frames=3)
+    o = oracle_sim(sp, prm, cfg)
+    o.substeps(30)
+    xo, vo = o.state()
+    assert max_abs(plug.positions(), xo) == 0.0
+    assert max_abs(plug.velocities(), vo) == 0.0
